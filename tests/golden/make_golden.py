@@ -1,0 +1,175 @@
+"""Generate the golden fixtures of the stepping path by running the reference itself.
+
+Run once in a container where the reference is importable:
+
+    python tests/golden/make_golden.py /root/reference
+
+Writes (all small, committed):
+  rhs_cases.npz          f(t, y) and the 36 accumulator rates of TVSAModel.rhs for seeded,
+                         non-trivial states: every step type, every end-condition kind,
+                         alternative closures (core/residual.py:211-417)
+  colouring.npz          greedy colouring (numerics/sparsity.py:88-107): full arrays for small
+                         grids, sha256 + colour count for the benchmark and ensemble grids
+  jacobian_3x4x6.npz     coloured FD Jacobian values (core/jacobian.py:71-86)
+  trajectory_c0.npz      TR-BDF2 integration of a 4x4x16 bed: 200 s adsorption from the seeded
+                         constant-pressure state, then 10 s blowdown and 100 s heating; accepted
+                         step sequence, end states, accumulators and solver counters
+                         (core/solver.py:370-511)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def main(ref_root):
+    sys.path.insert(0, ref_root)
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.jacobian import FDJacobian
+    from core.residual import TVSAModel
+    from core.solver import TRBDF2
+    from core.state import initial_state
+    from numerics.sparsity import build_pattern, color_columns
+    from properties import R_GAS, get_backend
+
+    def seeded(cfg, grid, props, seed=0):
+        st = initial_state(cfg, grid, props)
+        rng = np.random.default_rng(seed)
+        T = 288.0 * (1.0 + 0.01 * (2.0 * rng.random(grid.shape) - 1.0))
+        y = st.c / st.c.sum(axis=0)
+        st.c = y * (101325.0 / (R_GAS * T))[None]
+        st.T = T
+        st.Tw = np.full(grid.wall_shape, 288.0)
+        return st
+
+    # ------------------------------------------------------------ rhs cases
+    base = {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6, "jacket.theta_coverage_deg": [0.0, 180.0],
+            "feed.profile": "cosine_theta", "feed.profile_amplitude": 0.3}
+    cases = []
+    for s in range(4):
+        cases.append((f"step{s}", base, s))
+    cases += [
+        ("ramp_ports_ads", {**base, "operation.vent_model": "ramp", "operation.vacuum_model": "ramp"}, 0),
+        ("ramp_ports_blow", {**base, "operation.vent_model": "ramp", "operation.vacuum_model": "ramp",
+                             "operation.vacuum_check_valve": False}, 1),
+        ("pump_no_check", {**base, "operation.vacuum_check_valve": False}, 2),
+        ("mech_hx_jacket_ramp", {**base, "isotherm.coadsorption.model": "mechanistic",
+                                 "internal_hx.enabled": True, "jacket.ramp_time": 50.0}, 2),
+        ("no_wall", {**base, "wall.enabled": False}, 0),
+        ("no_wall_lumped", {**base, "wall.enabled": False, "transport.heat_transfer_mode": "lumped"}, 2),
+        ("sb_wk_krish", {**base, "isotherm.coadsorption.model": "stampi_bombelli",
+                         "transport.dispersion_model": "wakao_kagei",
+                         "energy.vacuum_efficiency_model": "krishnamurthy"}, 2),
+        ("minmod_parallel_const", {**base, "solver.limiter": "minmod",
+                                   "transport.bed_conductivity_model": "parallel",
+                                   "transport.wall_htc_model": "constant"}, 0),
+        ("vanleer_young_none", {**base, "solver.limiter": "van_leer", "transport.dispersion_model": "young2021",
+                                "isotherm.coadsorption.model": "none", "feed.profile": "linear_r"}, 0),
+        ("tvd_equilibrium_basis", {**base, "solver.limiter": "van_albada_tvd",
+                                   "isotherm.coadsorption.water_loading_basis": "equilibrium",
+                                   "feed.profile": "sector"}, 0),
+        ("upwind_disc_pump_water", {**base, "solver.limiter": "upwind", "feed.profile": "central_disc",
+                                    "energy.pump_handles_water": True, "wall.enabled": False}, 1),
+        ("axisym_2x1x4", {"grid.Nr": 2, "grid.Ntheta": 1, "grid.Nz": 4}, 1),
+        ("line_1x1x30", {"grid.Nr": 1, "grid.Ntheta": 1, "grid.Nz": 30}, 0),
+        ("equal_area_4x3x5", {"grid.Nr": 4, "grid.Ntheta": 3, "grid.Nz": 5, "grid.radial_spacing": "equal_area",
+                              "jacket.z_coverage": [0.2, 0.7]}, 3),
+        ("nz2_3x4x2", {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 2}, 0),
+    ]
+    rhs = {}
+    meta = []
+    for i, (name, over, step_i) in enumerate(cases):
+        cfg = rp.load_config(override_dict=over)
+        g = Grid.from_config(cfg)
+        props = get_backend(cfg)
+        st = initial_state(cfg, g, props)
+        rng = np.random.default_rng(100 + i)
+        st.T = st.T + 5.0 * rng.random(st.T.shape)
+        st.q = st.q + 0.5 * rng.random(st.q.shape)
+        st.c = st.c * (1.0 + 0.05 * rng.random(st.c.shape))
+        st.Tw = st.Tw + 3.0 * rng.random(st.Tw.shape)
+        m = TVSAModel(cfg, g, props, cfg.cycle[step_i], st, T_jacket_prev=300.0 if "ramp" in name else None)
+        y = m.pack(st)
+        t = 3.0
+        f, acc = m.rhs(t, y)
+        d = m.rhs(t, y, diag=True)
+        rhs[f"{name}__y"] = y
+        rhs[f"{name}__f"] = f
+        rhs[f"{name}__acc"] = acc
+        rhs[f"{name}__T"] = d["T"]
+        rhs[f"{name}__P"] = d["P"]
+        rhs[f"{name}__P0"] = st.P
+        meta.append({"name": name, "over": over, "step": step_i, "t": t,
+                     "T_jacket_prev": 300.0 if "ramp" in name else None})
+    rhs["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "rhs_cases.npz"), **rhs)
+
+    # ------------------------------------------------------------ colouring
+    col = {}
+    small = [(3, 4, 6), (4, 4, 16), (2, 1, 4), (1, 1, 30), (8, 8, 12), (3, 1, 8), (4, 3, 5)]
+    for d in small:
+        c = color_columns(build_pattern(*d, 3, 2, True))
+        col["full_%dx%dx%d" % d] = c.astype(np.uint8)
+    big = [(8, 8, 32), (16, 16, 64)] + [(a, b, c) for a in (4, 8, 16) for b in (4, 8, 16) for c in (16, 32, 64)]
+    hashes = {}
+    for d in sorted(set(big)):
+        c = color_columns(build_pattern(*d, 3, 2, True)).astype(np.int64)
+        hashes["%dx%dx%d" % d] = [hashlib.sha256(c.tobytes()).hexdigest(), int(c.max()) + 1]
+    col["hashes"] = np.array(json.dumps(hashes))
+    np.savez_compressed(os.path.join(HERE, "colouring.npz"), **col)
+
+    # ------------------------------------------------------------ jacobian
+    cfg = rp.load_config(override_dict={"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6})
+    g = Grid.from_config(cfg)
+    props = get_backend(cfg)
+    st = initial_state(cfg, g, props)
+    st.T = st.T + np.random.default_rng(0).random(st.T.shape)
+    m = TVSAModel(cfg, g, props, cfg.cycle[0], st)
+    y = m.pack(st)
+    J = FDJacobian(m)(5.0, y)
+    np.savez_compressed(os.path.join(HERE, "jacobian_3x4x6.npz"), y=y, t=5.0, data=J.data, indices=J.indices,
+                        indptr=J.indptr, P0=st.P)
+
+    # ------------------------------------------------------------ trajectory (4x4x16)
+    over = {"grid.Nr": 4, "grid.Ntheta": 4, "grid.Nz": 16, "solver.scheme": "trbdf2",
+            "operation.T_adsorption_jacket": 288.0, "operation.T_cool": 288.0, "operation.T_heat": 373.0,
+            "operation.P_vacuum": 1e4, "feed.T": 288.0, "feed.RH": 0.5, "ambient.T": 288.0}
+    cfg = rp.load_config(override_dict=over)
+    g = Grid.from_config(cfg)
+    props = get_backend(cfg)
+    st = seeded(cfg, g, props)
+    out = {"over": np.array(json.dumps(over))}
+    T_jac_prev = None
+    for k, (si, dur) in enumerate(((0, 200.0), (1, 10.0), (2, 100.0))):
+        step = dict(cfg.cycle[si])
+        step["duration"] = dur
+        m = TVSAModel(cfg, g, props, step, st, T_jac_prev)
+        y0 = m.pack(st)
+        integ = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur)
+        hs = []
+        res = integ.integrate(y0, dur, np.linspace(0.0, dur, 12), on_step=lambda t, y, a: hs.append(t))
+        out[f"s{k}_y0"] = y0
+        out[f"s{k}_P0"] = st.P
+        out[f"s{k}_y"] = res.y
+        out[f"s{k}_acc"] = res.acc
+        out[f"s{k}_t_accepted"] = np.array(hs)
+        out[f"s{k}_stats"] = np.array([res.n_steps, res.n_reject, res.n_newton_fail, res.n_jac, res.n_lu,
+                                       res.nfev, integ.stats["gmres_iters"]])
+        out[f"s{k}_snap_t"] = np.array([s[0] for s in res.snapshots])
+        out[f"s{k}_snap_y"] = np.array([s[1] for s in res.snapshots])
+        out[f"s{k}_meta"] = np.array(json.dumps({"step": si, "duration": dur, "T_jacket_prev": T_jac_prev}))
+        st = m.to_state(res.y, st, st.t + res.t, step["name"])
+        T_jac_prev = m.T_jacket(res.t) if m.jacket_on else T_jac_prev
+    np.savez_compressed(os.path.join(HERE, "trajectory_c0.npz"), **out)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
