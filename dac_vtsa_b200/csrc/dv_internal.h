@@ -1,0 +1,83 @@
+// dv_internal.h -- model handle and launchers shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include "dacvtsa.h"
+
+namespace dv {
+
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define DV_CUDA(call)                                      \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return dv::cuda_fail(e_, #call); \
+    } while (0)
+
+struct Work {
+    int64_t n = 0;
+    int kdim = 0;
+    double *V = nullptr, *w = nullptr, *u = nullptr, *x = nullptr, *r = nullptr, *b = nullptr, *s = nullptr;
+    double *z = nullptr, *f = nullptr, *R = nullptr, *dz = nullptr, *zt = nullptr, *ft = nullptr, *Rt = nullptr;
+    double *tmp = nullptr, *best = nullptr;
+    double *part = nullptr, *scal = nullptr, *hbuf = nullptr, *ybuf = nullptr;
+    double* hpin = nullptr;       // pinned host mirror of small results
+    double* J = nullptr;          // Jacobian storage used by in-stage refreshes
+    int nparts = 0;
+};
+int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
+void work_free(Work& W);
+
+struct DevAux {
+    const double* feed_flux;
+    const double* n_nom;
+    const double* cov;
+};
+
+// Diagnostics / record layout offsets (doubles) within one record buffer.
+struct RecLayout {
+    int64_t T, P, y, qstar, uz, ur, uth, bnd, Qj, Qa, Qw, Rb, Qhx, total;
+};
+RecLayout rec_layout(const dv_step_params& p);
+
+}  // namespace dv
+
+struct dv_model {
+    dv_step_params p;
+    int64_t nc, nw, n;              // cells, wall unknowns, n_core
+    double* d_aux;                  // feed_flux | n_nom | cov
+    dv::DevAux aux;
+    dv::RecLayout rl;
+    double* d_rec;                  // internal record scratch (accumulators)
+    double* d_acc;                  // DV_NACC
+    int64_t nfev;
+    int64_t jac_doubles;
+    // preconditioner: block-pentadiagonal LU along z per partition
+    int pc_mode, pc_nparts, pc_nb, pc_ready;
+    int pc_cap_nb, pc_cap_parts;
+    double* d_pc;                   // [parts][Nz][5][nb*nb]
+    double* d_pc_work;              // [parts][2][nb*nb] factorisation scratch
+    int* d_pc_piv;                  // [parts][nb] pivot work
+    int* d_pc_info;                 // [parts] singular-pivot flags
+    dv::Work* W;                    // Krylov / Newton workspace (allocated at creation)
+    double* d_atol7;                // per-block absolute tolerances (device)
+    int ncolours;                   // colours of the Jacobian pattern (counts RHS-equivalents)
+};
+
+namespace dv {
+// residual family (dv_kernels.cu, -fmad=false)
+int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, cudaStream_t s);
+int launch_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known,
+                          double* R, cudaStream_t s);
+int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream_t s);
+// out = (v - dh (f(z + sig v) - f0)/sig)/s with v = u*s, sig = SQRT_EPS*scal[1]/scal[0] (scal on device)
+int launch_matvec(dv_model* m, double t, const double* z, const double* u, const double* sc, const double* f0,
+                  double dh, const double* scal, double* out, cudaStream_t s);
+int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s);
+// linear algebra (dv_linalg.cu)
+int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s);
+// x = diag(1/sc) M^-1 diag(sc) b  (sc may be NULL: plain solve)
+int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);
+}  // namespace dv

@@ -1,0 +1,313 @@
+// dv_kernels.cu -- residual, matvec, diagnostics, accumulator and FD-Jacobian kernels.
+// Compiled with -fmad=false (see dv_physics.cuh).
+#include "dv_internal.h"
+#include "dv_residual.cuh"
+
+namespace dv {
+
+RecLayout rec_layout(const dv_step_params& p) {
+    RecLayout r;
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz, nf = (int64_t)p.Nr * p.Nth, nw = (int64_t)p.Nth * p.Nz;
+    int64_t o = 0;
+    r.T = o; o += nc;
+    r.P = o; o += nc;
+    r.y = o; o += 3 * nc;
+    r.qstar = o; o += 2 * nc;
+    r.uz = o; o += nf * (p.Nz - 1);
+    r.ur = o; o += (int64_t)(p.Nr - 1) * p.Nth * p.Nz;
+    r.uth = o; o += nc;
+    r.bnd = o; o += 2 * BR_N * nf;
+    r.Qj = o; o += nw;
+    r.Qa = o; o += nw;
+    r.Qw = o; o += nw;
+    r.Rb = o; o += nw;
+    r.Qhx = o; o += nc;
+    r.total = o;
+    return r;
+}
+
+static Rec make_rec(const RecLayout& l, double* base) {
+    Rec r;
+    r.T = base + l.T;
+    r.P = base + l.P;
+    r.y = base + l.y;
+    r.qstar = base + l.qstar;
+    r.uz = base + l.uz;
+    r.ur = base + l.ur;
+    r.uth = base + l.uth;
+    r.bnd = base + l.bnd;
+    r.Qj = base + l.Qj;
+    r.Qa = base + l.Qa;
+    r.Qw = base + l.Qw;
+    r.Rb = base + l.Rb;
+    r.Qhx = base + l.Qhx;
+    return r;
+}
+
+static __device__ __forceinline__ void cell_ijk(const dv_step_params& p, int64_t c, int& i, int& j, int& k) {
+    k = (int)(c % p.Nz);
+    int64_t r = c / p.Nz;
+    j = (int)(r % p.Nth);
+    i = (int)(r / p.Nth);
+}
+
+enum { M_RHS = 0, M_STAGE = 1, M_MATVEC = 2 };
+
+// One thread per cell.  MODE selects the epilogue:
+//  M_RHS    out = f                                   (core/residual.py:361-365)
+//  M_STAGE  out = y - gh f - rhs_known                (core/residual.py:420-423)
+//  M_MATVEC out = (v - dh (f(z+sig v) - f0)/sig)/s    (core/solver.py:196-203)
+template <int MODE, bool REC>
+__global__ void __launch_bounds__(128) k_cells(dv_step_params p, Aux aux, Rec rec, double t, const double* __restrict__ y,
+                                               const double* __restrict__ u, const double* __restrict__ sc,
+                                               const double* __restrict__ f0, const double* __restrict__ scal,
+                                               double gh, double* __restrict__ out) {
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    int i, j, k;
+    cell_ijk(p, c, i, j, k);
+    double f[DV_NV], fw = 0.0;
+    const bool outer_wall = (i == p.Nr - 1) && p.wall_on;
+    const int64_t iw = (int64_t)DV_NV * nc + (int64_t)j * p.Nz + k;
+    if (MODE == M_MATVEC) {
+        const double un = scal[0];
+        if (un == 0.0) {            // matvec of a zero direction is zero
+#pragma unroll
+            for (int v = 0; v < DV_NV; ++v) out[v * nc + c] = 0.0;
+            if (outer_wall) out[iw] = 0.0;
+            return;
+        }
+        const double sig = 1.4901161193847656e-08 * scal[1] / un;
+        LoadDir ld{y, u, sc, sig};
+        cell_eval(p, aux, ld, t, i, j, k, f, outer_wall ? &fw : nullptr, REC ? &rec : nullptr);
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) {
+            const int64_t ix = v * nc + c;
+            const double vv = u[ix] * sc[ix];
+            out[ix] = (vv - gh * (f[v] - f0[ix]) / sig) / sc[ix];
+        }
+        if (outer_wall) {
+            const double vv = u[iw] * sc[iw];
+            out[iw] = (vv - gh * (fw - f0[iw]) / sig) / sc[iw];
+        }
+        return;
+    }
+    LoadPlain ld{y};
+    cell_eval(p, aux, ld, t, i, j, k, f, outer_wall ? &fw : nullptr, REC ? &rec : nullptr);
+    if (MODE == M_RHS) {
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) out[v * nc + c] = f[v];
+        if (outer_wall) out[iw] = fw;
+    } else {
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) {
+            const int64_t ix = v * nc + c;
+            out[ix] = y[ix] - gh * f[v] - u[ix];
+        }
+        if (outer_wall) out[iw] = y[iw] - gh * fw - u[iw];
+    }
+}
+
+// Deterministic block sum (fixed blockDim = 256).
+__device__ double block_sum(double v, double* sh) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (t < s) sh[t] = sh[t] + sh[t + s];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// The 36 accumulator rates from the end-face and wall records (core/residual.py:371-417).
+__global__ void __launch_bounds__(256) k_accumulators(dv_step_params p, const double* __restrict__ rec_bnd,
+                                                      const double* __restrict__ Qj, const double* __restrict__ Qa,
+                                                      const double* __restrict__ Qw, const double* __restrict__ Qhx,
+                                                      double* __restrict__ acc) {
+    __shared__ double sh[256];
+    const int t = threadIdx.x;
+    const int nf = p.Nr * p.Nth, nw = p.Nth * p.Nz;
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz;
+    double a[DV_NACC];
+    for (int q = 0; q < DV_NACC; ++q) a[q] = 0.0;
+    const double ex = (p.gam - 1.0) / p.gam;
+    const double pre = p.gam / (p.gam - 1.0) * DV_R;
+    for (int e = 0; e < 2; ++e) {
+        const dv_end& E = p.ends[e];
+        if (E.valve < 0) continue;
+        const double* b = rec_bnd + (int64_t)e * BR_N * nf;
+        const bool parts = (E.kind == DV_END_VALVE);
+        const int base = E.valve * (2 * DV_NG + 4);
+        double s_in[DV_NG] = {0, 0, 0}, s_out[DV_NG] = {0, 0, 0}, h_in = 0, h_out = 0, wp = 0, wf = 0;
+        for (int f = t; f < nf; f += blockDim.x) {
+            const bool inflow = b[BR_UOUT * nf + f] < 0.0;
+            double Fin[DV_NG];
+            for (int q = 0; q < DV_NG; ++q) {
+                Fin[q] = b[(BR_FIN + q) * nf + f];
+                s_in[q] += parts ? b[(BR_FINP + q) * nf + f] : (inflow ? Fin[q] : 0.0);
+                s_out[q] += parts ? b[(BR_FOUTP + q) * nf + f] : (inflow ? 0.0 : -Fin[q]);
+            }
+            const double H = b[BR_HIN * nf + f];
+            h_in += parts ? b[BR_HINP * nf + f] : (inflow ? H : 0.0);
+            h_out += parts ? b[BR_HOUTP * nf + f] : (inflow ? 0.0 : -H);
+            const double Pf = b[BR_PFACE * nf + f];
+            if (E.is_vacuum) {
+                double Fo[DV_NG];
+                for (int q = 0; q < DV_NG; ++q) Fo[q] = inflow ? 0.0 : -Fin[q];
+                double Ft = p.pump_water ? (Fo[0] + Fo[1] + Fo[2]) : (Fo[0] + Fo[2]);
+                double ratio = npmax(p.P_amb / npmax(Pf, 1.0), 1.0);
+                double eta = p.eta_vac;
+                if (p.vac_krishnamurthy) {
+                    double pb = Pf / 1e5;
+                    eta = npmax(0.8 * 19.55 * pb / (1.0 + 19.55 * pb), 1e-3);
+                }
+                wp += pre * b[BR_TLAY * nf + f] * Ft * (pow(ratio, ex) - 1.0) / eta;
+            }
+            if (E.is_feed) {
+                double Ft;
+                if (parts) Ft = b[(BR_FINP + 0) * nf + f] + b[(BR_FINP + 1) * nf + f] + b[(BR_FINP + 2) * nf + f];
+                else Ft = (inflow ? Fin[0] : 0.0) + (inflow ? Fin[1] : 0.0) + (inflow ? Fin[2] : 0.0);
+                double ratio = npmax(Pf / p.P_amb, 1.0);
+                wf += pre * E.T_ext * Ft * (pow(ratio, ex) - 1.0) / p.eta_bl;
+            }
+        }
+        for (int q = 0; q < DV_NG; ++q) {
+            a[base + q] = block_sum(s_in[q], sh);
+            a[base + DV_NG + q] = block_sum(s_out[q], sh);
+        }
+        a[base + 6] = block_sum(h_in, sh);
+        a[base + 7] = block_sum(h_out, sh);
+        if (E.is_vacuum) a[base + 8] = block_sum(wp, sh);
+        if (E.is_feed) a[base + 9] = block_sum(wf, sh);
+    }
+    double jp = 0, jn = 0, qa = 0, qw = 0;
+    for (int w = t; w < nw; w += blockDim.x) {
+        jp += npmax(Qj[w], 0.0);
+        jn += npmin(Qj[w], 0.0);
+        qa += Qa[w];
+        qw += Qw[w];
+    }
+    a[30] = block_sum(jp, sh);
+    a[31] = block_sum(jn, sh);
+    a[32] = block_sum(qa, sh);
+    a[33] = block_sum(qw, sh);
+    if (p.hx_on) {
+        double hp = 0, hn = 0;
+        for (int64_t c = t; c < nc; c += blockDim.x) {
+            hp += npmax(Qhx[c], 0.0);
+            hn += npmin(Qhx[c], 0.0);
+        }
+        a[34] = block_sum(hp, sh);
+        a[35] = block_sum(hn, sh);
+    }
+    if (t == 0)
+        for (int q = 0; q < DV_NACC; ++q) acc[q] = a[q];
+}
+
+// All colour perturbations of the forward-difference Jacobian in one launch.
+// blockIdx.y = slot * 7 + col_var: the perturbed column is unknown `col_var` of neighbour `slot`
+// of the row cell.  With a distance-2 colouring every row sees exactly one perturbed column of
+// each colour, so evaluating the row cell with that single column perturbed reproduces the
+// coloured evaluation of core/jacobian.py:78-84 (colour = colour[column]).
+__global__ void __launch_bounds__(128) k_fd_jacobian(dv_step_params p, Aux aux, double t, const double* __restrict__ y,
+                                                     const double* __restrict__ f0, double* __restrict__ J) {
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int slot = blockIdx.y / DV_NB, cv = blockIdx.y % DV_NB;
+    int i, j, k;
+    cell_ijk(p, c, i, j, k);
+    int ni = i, nj = j, nk = k;
+    bool ok = true;
+    switch (slot) {
+        case 0: break;
+        case 1: nk = k - 1; ok = nk >= 0; break;
+        case 2: nk = k + 1; ok = nk < p.Nz; break;
+        case 3: nk = k - 2; ok = nk >= 0; break;
+        case 4: nk = k + 2; ok = nk < p.Nz; break;
+        case 5: ni = i - 1; ok = ni >= 0; break;
+        case 6: ni = i + 1; ok = ni < p.Nr; break;
+        case 7: ok = p.Nth > 1; nj = (j == 0) ? p.Nth - 1 : j - 1; break;
+        default: ok = p.Nth > 1; nj = (j == p.Nth - 1) ? 0 : j + 1; break;
+    }
+    if (cv == DV_NV) ok = ok && p.wall_on && (ni == p.Nr - 1);
+    double* Jb = J + ((int64_t)slot * DV_NB * DV_NB + cv) * nc + c;     // row stride DV_NB*nc
+    if (!ok) {
+#pragma unroll
+        for (int rv = 0; rv < DV_NB; ++rv) Jb[(int64_t)rv * DV_NB * nc] = 0.0;
+        return;
+    }
+    const int64_t ncell_n = ((int64_t)ni * p.Nth + nj) * p.Nz + nk;
+    const int64_t col = (cv < DV_NV) ? (int64_t)cv * nc + ncell_n : (int64_t)DV_NV * nc + (int64_t)nj * p.Nz + nk;
+    const double yv = y[col];
+    double h = 1.5e-8 * npmax(fabs(yv), p.typ[cv]);
+    h = (yv + h) - yv;                                   // core/jacobian.py:75-76
+    LoadPert ld{y, col, h};
+    double f[DV_NV], fw = 0.0;
+    const bool outer_wall = (i == p.Nr - 1) && p.wall_on;
+    cell_eval(p, aux, ld, t, i, j, k, f, outer_wall ? &fw : nullptr, (const Rec*)nullptr);
+#pragma unroll
+    for (int rv = 0; rv < DV_NV; ++rv) Jb[(int64_t)rv * DV_NB * nc] = (f[rv] - f0[rv * nc + c]) / h;
+    Jb[(int64_t)DV_NV * DV_NB * nc] =
+        outer_wall ? (fw - f0[(int64_t)DV_NV * nc + (int64_t)j * p.Nz + k]) / h : 0.0;
+}
+
+static Aux aux_of(const dv_model* m) { return Aux{m->aux.feed_flux, m->aux.n_nom, m->aux.cov}; }
+
+static unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, cudaStream_t s) {
+    Rec rec = make_rec(m->rl, m->d_rec);
+    if (acc) {
+        k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
+                                                              nullptr, 0.0, f);
+        k_accumulators<<<1, 256, 0, s>>>(m->p, rec.bnd, rec.Qj, rec.Qa, rec.Qw, rec.Qhx, acc);
+    } else {
+        k_cells<M_RHS, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
+                                                               nullptr, 0.0, f);
+    }
+    m->nfev += 1;
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+int launch_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known,
+                          double* R, cudaStream_t s) {
+    Rec rec = make_rec(m->rl, m->d_rec);
+    k_cells<M_STAGE, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, rhs_known, nullptr, nullptr,
+                                                             nullptr, gamma_h, R);
+    m->nfev += 1;
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream_t s) {
+    Rec rec = make_rec(m->rl, diag);
+    k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
+                                                          nullptr, 0.0, m->d_rec);   // f discarded into scratch
+    m->nfev += 1;
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+int launch_matvec(dv_model* m, double t, const double* z, const double* u, const double* sc, const double* f0,
+                  double dh, const double* scal, double* out, cudaStream_t s) {
+    Rec rec = make_rec(m->rl, m->d_rec);
+    k_cells<M_MATVEC, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, z, u, sc, f0, scal, dh, out);
+    m->nfev += 1;
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s) {
+    dim3 grid(nblk(m->nc, 128), DV_NSLOT * DV_NB);
+    k_fd_jacobian<<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J);
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+}  // namespace dv

@@ -1,0 +1,1089 @@
+// dv_solver.cu -- Newton-Krylov stage solve, adaptive 2-stage implicit RK integrator, C ABI.
+//
+// Control flow mirrors the reference exactly (core/solver.py); the arithmetic runs on the GPU
+// (dv_kernels.cu, dv_linalg.cu and the vector kernels below) and the host reads back a few
+// scalars per Krylov iteration to take the same branch decisions.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+#include "dv_internal.h"
+#include "dv_physics.cuh"
+
+namespace dv {
+
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+int cuda_fail(cudaError_t e, const char* what) {
+    g_err = std::string("CUDA error ") + cudaGetErrorString(e) + " in " + what;
+    return DV_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------- vector kernels
+#define VB 256
+static unsigned vgrid(int64_t n) {
+    int64_t b = (n + VB - 1) / VB;
+    return (unsigned)(b < 1024 ? (b < 1 ? 1 : b) : 1024);
+}
+
+__global__ void k_scale(int64_t nc, int64_t n, const double* __restrict__ z, const double* __restrict__ atol7,
+                        double rtol, double* __restrict__ s) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int v = (int)(i / nc);
+        if (v > DV_NV) v = DV_NV;
+        s[i] = atol7[v] + rtol * fabs(z[i]);
+    }
+}
+
+// out = a*x + b*y   (y may be null)
+__global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
+                        double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = y ? a * x[i] + b * y[i] : a * x[i];
+}
+
+// out = x + a*y  (numpy  x + a * y)
+__global__ void k_xpay(int64_t n, const double* __restrict__ x, double a, const double* __restrict__ y,
+                       double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = x[i] + a * y[i];
+}
+
+// out = num / den (den may be null), with an optional sign: out = sgn * num / den
+__global__ void k_div(int64_t n, double sgn, const double* __restrict__ num, const double* __restrict__ den,
+                      double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (sgn < 0 ? -num[i] : num[i]) / den[i];
+}
+
+__global__ void k_mul(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] * b[i];
+}
+
+// positivity truncation of gas concentrations and loadings (core/solver.py:99-108): i < npos
+__global__ void k_truncate(int64_t n, int64_t npos, const double* __restrict__ z, double lam, const double* __restrict__ dz,
+                           double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = z[i] + lam * dz[i];
+        if (i < npos) v = npmax(v, 0.1 * npmax(z[i], 0.0));
+        out[i] = v;
+    }
+}
+
+// truncation of a prediction: out = max(x, 0.1 max(y, 0)) on i < npos, else x
+__global__ void k_truncate_to(int64_t n, int64_t npos, const double* __restrict__ x, const double* __restrict__ y,
+                              double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = x[i];
+        if (i < npos) v = npmax(v, 0.1 * npmax(y[i], 0.0));
+        out[i] = v;
+    }
+}
+
+// partial sums of (a/b)^2 (b null: a^2); non-finite terms propagate
+__global__ void k_sumsq(int64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ part) {
+    __shared__ double sh[VB];
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = b ? a[i] / b[i] : a[i];
+        acc += v * v;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = VB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+// out[slot] = mode 0: sqrt(sum/n); 1: max(1, sqrt(sum/n)); 2: sqrt(sum) ; 3: sum
+__global__ void k_finish(int nparts, const double* __restrict__ part, double n, int mode, double* __restrict__ out) {
+    __shared__ double sh[VB];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += part[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = VB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double v = sh[0];
+        if (mode == 0) v = sqrt(v / n);
+        else if (mode == 1) v = fmax(1.0, sqrt(v / n));
+        else if (mode == 2) v = sqrt(v);
+        out[0] = v;
+    }
+}
+
+// partial dots: part[blk][q] = sum_i V[q][i] w[i] (q < m), part[blk][m] = sum w^2
+__global__ void k_dots(int64_t n, int m, const double* __restrict__ V, int64_t ldv, const double* __restrict__ w,
+                       double* __restrict__ part) {
+    __shared__ double sh[VB];
+    for (int q = 0; q <= m; ++q) {
+        const double* a = (q < m) ? V + q * ldv : w;
+        double acc = 0.0;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            acc += a[i] * w[i];
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s = VB / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(int64_t)blockIdx.x * (m + 1) + q] = sh[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_dots_finish(int nblk, int m1, const double* __restrict__ part, double* __restrict__ out) {
+    int q = blockIdx.x;
+    __shared__ double sh[VB];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[(int64_t)b * m1 + q];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = VB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = sh[0];
+}
+
+// w -= sum_q h[q] V[q]
+__global__ void k_orth_update(int64_t n, int m, const double* __restrict__ V, int64_t ldv, const double* __restrict__ h,
+                              double* __restrict__ w) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int q = 0; q < m; ++q) acc += h[q] * V[q * ldv + i];
+        w[i] -= acc;
+    }
+}
+
+// x = sum_q y[q] V[q]  (y from host, passed by value through a small device buffer)
+__global__ void k_combine(int64_t n, int m, const double* __restrict__ V, int64_t ldv, const double* __restrict__ y,
+                          double* __restrict__ x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int q = 0; q < m; ++q) acc += y[q] * V[q * ldv + i];
+        x[i] = acc;
+    }
+}
+
+// conservation sums: out[0..3] = W R (species moles + energy), out[4..7] = W s (core/residual.py:146-168)
+__global__ void k_cons(dv_step_params p, const double* __restrict__ R, const double* __restrict__ s,
+                       double* __restrict__ out) {
+    __shared__ double sh[VB];
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz, nw = p.wall_on ? (int64_t)p.Nth * p.Nz : 0;
+    for (int which = 0; which < 2; ++which) {
+        const double* x = which ? s : R;
+        for (int m = 0; m <= DV_NG; ++m) {
+            double acc = 0.0;
+            for (int64_t c = threadIdx.x; c < nc; c += blockDim.x) {
+                const int i = (int)(c / ((int64_t)p.Nth * p.Nz));
+                const double V = p.V[i];
+                if (m < DV_NG) {
+                    acc += p.eps_t * V * x[m * nc + c];
+                    if (m < DV_NA) acc += p.rho_b * V * x[(DV_NG + m) * nc + c];
+                } else {
+                    acc += V * x[(int64_t)DV_NV * nc + c];
+                }
+            }
+            if (m == DV_NG)
+                for (int64_t w = threadIdx.x; w < nw; w += blockDim.x) acc += p.wall_C * x[(int64_t)DV_NV * nc + w];
+            sh[threadIdx.x] = acc;
+            __syncthreads();
+            for (int st = VB / 2; st > 0; st >>= 1) {
+                if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) out[which * 4 + m] = sh[0];
+            __syncthreads();
+        }
+    }
+}
+
+// err scale: sc = atol + rtol max(|y|, |z|)  (core/solver.py:461)
+__global__ void k_err_scale(int64_t nc, int64_t n, const double* __restrict__ y, const double* __restrict__ z,
+                            const double* __restrict__ atol7, double rtol, double* __restrict__ sc) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int v = (int)(i / nc);
+        if (v > DV_NV) v = DV_NV;
+        sc[i] = atol7[v] + rtol * npmax(fabs(y[i]), fabs(z[i]));
+    }
+}
+
+// y3 = y + h (w1 f_n + w2 f1 + w3 f2);  out = z2 - y3   (core/solver.py:456-460)
+__global__ void k_err_vec(int64_t n, const double* __restrict__ y, const double* __restrict__ z2, double h, double w1,
+                          const double* __restrict__ fn, double w2, const double* __restrict__ f1, double w3,
+                          const double* __restrict__ f2, double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double y3 = y[i] + h * (w1 * fn[i] + w2 * f1[i] + w3 * f2[i]);
+        out[i] = z2[i] - y3;
+    }
+}
+
+// ---------------------------------------------------------------- workspace
+int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
+    W.n = n;
+    W.kdim = kdim;
+    W.nparts = 1024;
+    auto A = [&](double** p, int64_t cnt) { return cudaMalloc((void**)p, sizeof(double) * (size_t)cnt); };
+    if (A(&W.V, (kdim + 1) * n) || A(&W.w, n) || A(&W.u, n) || A(&W.x, n) || A(&W.r, n) || A(&W.b, n) ||
+        A(&W.s, n) || A(&W.z, n) || A(&W.f, n) || A(&W.R, n) || A(&W.dz, n) || A(&W.zt, n) || A(&W.ft, n) ||
+        A(&W.Rt, n) || A(&W.tmp, n) || A(&W.best, n) || A(&W.part, (int64_t)W.nparts * (kdim + 2)) ||
+        A(&W.scal, 16) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles))
+        return cuda_fail(cudaGetLastError(), "cudaMalloc(Krylov workspace)");
+    if (cudaMallocHost((void**)&W.hpin, sizeof(double) * 4 * (kdim + 8)) != cudaSuccess)
+        return cuda_fail(cudaGetLastError(), "cudaMallocHost");
+    return DV_OK;
+}
+
+void work_free(Work& W) {
+    double* ptrs[] = {W.V, W.w, W.u, W.x, W.r, W.b, W.s, W.z, W.f, W.R, W.dz, W.zt, W.ft, W.Rt, W.tmp, W.best,
+                      W.part, W.scal, W.hbuf, W.ybuf, W.J};
+    for (double* p : ptrs)
+        if (p) cudaFree(p);
+    if (W.hpin) cudaFreeHost(W.hpin);
+    W = Work();
+}
+
+// reductions returning host values (synchronise)
+static int rms_ratio_dev(Work& W, int64_t n, const double* a, const double* b, int mode, double* dst, cudaStream_t s) {
+    unsigned g = vgrid(n);
+    k_sumsq<<<g, VB, 0, s>>>(n, a, b, W.part);
+    k_finish<<<1, VB, 0, s>>>((int)g, W.part, (double)n, mode, dst);
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+static int fetch(Work& W, const double* dev, int cnt, double* host, cudaStream_t s) {
+    DV_CUDA(cudaMemcpyAsync(W.hpin, dev, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s));
+    DV_CUDA(cudaStreamSynchronize(s));
+    memcpy(host, W.hpin, sizeof(double) * cnt);
+    return DV_OK;
+}
+
+static int rms_ratio(Work& W, int64_t n, const double* a, const double* b, double* out, cudaStream_t s) {
+    int rc = rms_ratio_dev(W, n, a, b, 0, W.scal + 8, s);
+    if (rc) return rc;
+    return fetch(W, W.scal + 8, 1, out, s);
+}
+
+#define DV_TRY(x)                 \
+    do {                          \
+        int rc_ = (x);            \
+        if (rc_ != DV_OK) return rc_; \
+    } while (0)
+
+
+
+// LAPACK dlartg (3.10+): c, s, r with [c s; -s c] [f; g] = [r; 0]
+static void lartg(double f, double g, double& c, double& s, double& r) {
+    const double safmin = std::numeric_limits<double>::min();
+    const double safmax = 1.0 / safmin;
+    const double rtmin = std::sqrt(safmin), rtmax = std::sqrt(safmax / 2);
+    double f1 = std::fabs(f), g1 = std::fabs(g);
+    if (g == 0.0) {
+        c = 1.0; s = 0.0; r = f;
+    } else if (f == 0.0) {
+        c = 0.0; s = std::copysign(1.0, g); r = g1;
+    } else if (f1 > rtmin && f1 < rtmax && g1 > rtmin && g1 < rtmax) {
+        double d = std::sqrt(f * f + g * g);
+        c = f1 / d;
+        r = std::copysign(d, f);
+        s = g / r;
+    } else {
+        double u = std::min(safmax, std::max(safmin, std::max(f1, g1)));
+        double fs = f / u, gs = g / u;
+        double d = std::sqrt(fs * fs + gs * gs);
+        c = std::fabs(fs) / d;
+        r = std::copysign(d, f);
+        s = gs / r;
+        r *= u;
+    }
+}
+
+// Operator of the Newton linear system in scaled variables, right-preconditioned:
+// AP(w) = matvec(prec(w)), prec(r) = M^-1 (r s) / s, matvec(u) = (v - dh (f(z + sig v) - f)/sig)/s.
+struct Op {
+    dv_model* m;
+    double t, dh;
+    const double* z;
+    const double* f;
+    const double* s;
+    int64_t n;
+};
+
+static int apply_AP(Work& W, const Op& op, const double* w, double* out, cudaStream_t st) {
+    DV_TRY(precond_apply(op.m, w, op.s, W.u, st));                      // u = prec(w)
+    DV_TRY(rms_ratio_dev(W, op.n, W.u, nullptr, 0, W.scal + 0, st));   // scal[0] = rms(u)
+    DV_TRY(launch_matvec(op.m, op.t, op.z, W.u, op.s, op.f, op.dh, W.scal, out, st));
+    return DV_OK;
+}
+
+// scipy.sparse.linalg.gmres(AP, b, rtol, atol, restart=kdim, maxiter=1) with M = identity
+// (scipy/sparse/linalg/_isolve/iterative.py); x written to W.x.  Returns info (0 = converged).
+static int gmres(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
+                 int64_t* inner, cudaStream_t st) {
+    const int64_t n = op.n;
+    double bn2;
+    DV_TRY(rms_ratio_dev(W, n, b, nullptr, 2, W.scal + 9, st));
+    DV_TRY(fetch(W, W.scal + 9, 1, &bn2, st));
+    const double atol_eff = std::max(atol, rtol * bn2);
+    *info = 0;
+    if (bn2 == 0.0) {
+        DV_CUDA(cudaMemsetAsync(W.x, 0, sizeof(double) * n, st));
+        return DV_OK;
+    }
+    double ptol = bn2 * std::min(1.0, atol_eff / bn2);
+    const double eps = std::numeric_limits<double>::epsilon();
+    if (bn2 < atol_eff) {       // ||r0|| < atol with x0 = 0
+        DV_CUDA(cudaMemsetAsync(W.x, 0, sizeof(double) * n, st));
+        return DV_OK;
+    }
+    const int64_t ldv = n;
+    k_axpby<<<vgrid(n), VB, 0, st>>>(n, 1.0 / bn2, b, 0.0, nullptr, W.V);      // v0 = r / ||r||
+    std::vector<double> H((size_t)kdim * (kdim + 1), 0.0), S(kdim + 1, 0.0), gc(kdim), gs(kdim);
+    auto h = [&](int col, int k) -> double& { return H[(size_t)col * (kdim + 1) + k]; };
+    S[0] = bn2;
+    bool breakdown = false;
+    int col = 0;
+    double presid = 0.0;
+    const unsigned g = vgrid(n);
+    for (col = 0; col < kdim; ++col) {
+        double* w = W.V + (col + 1) * ldv;
+        DV_TRY(apply_AP(W, op, W.V + col * ldv, w, st));
+        // classical Gram-Schmidt, twice (orthogonality equivalent to scipy's modified GS)
+        const int m = col + 1;
+        k_dots<<<g, VB, 0, st>>>(n, m, W.V, ldv, w, W.part);
+        k_dots_finish<<<m + 1, VB, 0, st>>>((int)g, m + 1, W.part, W.hbuf);
+        k_orth_update<<<g, VB, 0, st>>>(n, m, W.V, ldv, W.hbuf, w);
+        k_dots<<<g, VB, 0, st>>>(n, m, W.V, ldv, w, W.part);
+        k_dots_finish<<<m + 1, VB, 0, st>>>((int)g, m + 1, W.part, W.hbuf + (kdim + 2));
+        k_orth_update<<<g, VB, 0, st>>>(n, m, W.V, ldv, W.hbuf + (kdim + 2), w);
+        DV_TRY(rms_ratio_dev(W, n, w, nullptr, 2, W.hbuf + 2 * (kdim + 2), st));
+        DV_CUDA(cudaGetLastError());
+        std::vector<double> hh(2 * (kdim + 2) + 1);
+        DV_CUDA(cudaMemcpyAsync(W.hpin, W.hbuf, sizeof(double) * (2 * (kdim + 2) + 1), cudaMemcpyDeviceToHost, st));
+        DV_CUDA(cudaStreamSynchronize(st));
+        memcpy(hh.data(), W.hpin, sizeof(double) * hh.size());
+        const double h0 = std::sqrt(hh[m]);          // ||w|| before orthogonalisation
+        for (int k = 0; k <= col; ++k) h(col, k) = hh[k] + hh[(kdim + 2) + k];
+        const double h1 = hh[2 * (kdim + 2)];
+        h(col, col + 1) = h1;
+        if (h1 <= eps * h0 || !(h1 == h1)) {
+            h(col, col + 1) = 0.0;
+            breakdown = true;
+        } else {
+            k_axpby<<<g, VB, 0, st>>>(n, 1.0 / h1, w, 0.0, nullptr, w);
+        }
+        for (int k = 0; k < col; ++k) {
+            double c = gc[k], s = gs[k];
+            double n0 = h(col, k), n1 = h(col, k + 1);
+            h(col, k) = c * n0 + s * n1;
+            h(col, k + 1) = -s * n0 + c * n1;
+        }
+        double c, s, mag;
+        lartg(h(col, col), h(col, col + 1), c, s, mag);
+        gc[col] = c;
+        gs[col] = s;
+        h(col, col) = mag;
+        h(col, col + 1) = 0.0;
+        double tmp = -s * S[col];
+        S[col] = c * S[col];
+        S[col + 1] = tmp;
+        presid = std::fabs(tmp);
+        *inner += 1;
+        if (!(presid == presid)) break;
+        if (presid <= ptol || breakdown) break;
+    }
+    if (col == kdim) col = kdim - 1;
+    if (h(col, col) == 0.0) S[col] = 0.0;
+    std::vector<double> y(col + 1);
+    for (int k = 0; k <= col; ++k) y[k] = S[k];
+    for (int k = col; k > 0; --k) {
+        if (y[k] != 0.0) {
+            y[k] /= h(k, k);
+            double tmp = y[k];
+            for (int q = 0; q < k; ++q) y[q] -= tmp * h(k, q);
+        }
+    }
+    if (y[0] != 0.0) y[0] /= h(0, 0);
+    memcpy(W.hpin, y.data(), sizeof(double) * (col + 1));
+    DV_CUDA(cudaMemcpyAsync(W.ybuf, W.hpin, sizeof(double) * (col + 1), cudaMemcpyHostToDevice, st));
+    k_combine<<<g, VB, 0, st>>>(n, col + 1, W.V, ldv, W.ybuf, W.x);
+    // true residual r = b - AP x
+    DV_TRY(apply_AP(W, op, W.x, W.r, st));
+    k_axpby<<<g, VB, 0, st>>>(n, 1.0, b, -1.0, W.r, W.r);
+    double rnorm;
+    DV_TRY(rms_ratio_dev(W, n, W.r, nullptr, 2, W.scal + 10, st));
+    DV_TRY(fetch(W, W.scal + 10, 1, &rnorm, st));
+    *info = (rnorm <= atol_eff) ? 0 : 1;
+    return DV_OK;
+}
+
+}  // namespace dv
+// ================================================================== Newton-Krylov stage solve
+namespace dv {
+
+struct NewtonCtx {
+    dv_model* m;
+    Work* W;
+    const double* atol7;
+    int64_t n, npos;
+    dv_newton_opts o;
+    dv_newton_result* res;
+    int64_t* gm_counter;      // GMRES iterations counted towards the Jacobian-refresh rule
+};
+
+static int refresh_J(NewtonCtx& C, double t, const double* z, double dh, cudaStream_t st) {
+    // fc = rhs(t, zc); J = jac(t, zc, fc); factor(J, h) with h = dh / D (core/solver.py:350-356)
+    Work& W = *C.W;
+    DV_TRY(launch_rhs(C.m, t, z, W.tmp, nullptr, st));
+    DV_TRY(launch_fd_jacobian(C.m, t, z, W.tmp, W.J, st));
+    C.m->nfev += C.m->ncolours;
+    const double D = (2.0 - std::sqrt(2.0)) / 2.0;
+    const double h = dh / D;
+    DV_TRY(precond_factor(C.m, W.J, D * h, C.o.precond_mode, st));
+    return DV_OK;
+}
+
+// newton_krylov (core/solver.py:154-294) on the GPU.  z written to `zout`.
+static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double* rhs_known, double dh, double* zout,
+                         cudaStream_t st) {
+    Work& W = *C.W;
+    dv_model* m = C.m;
+    const int64_t n = C.n;
+    const unsigned g = vgrid(n);
+    dv_newton_result& r = *C.res;
+    r.ok = 0;
+    r.iters = 0;
+    r.rate = 0.0;
+    r.refreshed = 0;
+    const double kappa = C.o.kappa, rtol = C.o.rtol;
+    auto scale = [&](const double* z, double* s) { k_scale<<<g, VB, 0, st>>>(m->nc, n, z, C.atol7, rtol, s); };
+    auto stage = [&](const double* z, double* f, double* R) -> int {
+        // f = rhs(z); R = z - dh f - rhs_known
+        DV_TRY(launch_rhs(m, t, z, f, nullptr, st));
+        k_axpby<<<g, VB, 0, st>>>(n, 1.0, z, -dh, f, R);
+        k_axpby<<<g, VB, 0, st>>>(n, 1.0, R, -1.0, rhs_known, R);
+        return DV_OK;
+    };
+    auto pnorm = [&](const double* RR, const double* ss, double* out) -> int {
+        DV_TRY(precond_apply(m, RR, nullptr, W.tmp, st));
+        return rms_ratio(W, n, W.tmp, ss, out, st);
+    };
+    auto copy = [&](const double* a, double* b) { DV_CUDA(cudaMemcpyAsync(b, a, sizeof(double) * n, cudaMemcpyDeviceToDevice, st)); return DV_OK; };
+    auto cons_ok = [&](const double* R, const double* z, bool* ok) -> int {
+        if (C.o.cons_tol <= 0.0) { *ok = true; return DV_OK; }
+        scale(z, W.tmp);
+        k_cons<<<1, VB, 0, st>>>(m->p, R, W.tmp, W.scal);
+        DV_CUDA(cudaGetLastError());
+        double v[8];
+        DV_TRY(fetch(W, W.scal, 8, v, st));
+        *ok = true;
+        for (int q = 0; q < 4; ++q)
+            if (!(std::fabs(v[q]) <= C.o.cons_tol * v[4 + q])) *ok = false;
+        return DV_OK;
+    };
+
+    DV_TRY(copy(z0, W.z));
+    DV_TRY(stage(W.z, W.f, W.R));
+    scale(W.z, W.s);
+    double rn;
+    DV_TRY(rms_ratio(W, n, W.R, W.s, &rn, st));
+    if (!std::isfinite(rn)) {
+        DV_TRY(copy(z0, zout));
+        r.rate = INFINITY;
+        return DV_OK;
+    }
+    double pn;
+    DV_TRY(pnorm(W.R, W.s, &pn));
+    double step_prev = -1.0;     // < 0 : None
+    int polish = 0;
+    bool have_best = false;
+    double best_rn = 0.0;
+    bool new_lu = false;
+    int it = -1;
+    const double sqrt_n = std::sqrt((double)n);
+    while (it + 1 < C.o.max_iter + polish) {
+        ++it;
+        scale(W.z, W.s);
+        k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.b);                    // b = -R/s
+        DV_TRY(rms_ratio_dev(W, n, W.z, W.s, 1, W.scal + 1, st));           // zs = max(1, rms(z/s))
+        Op op{m, t, dh, W.z, W.f, W.s, n};
+        const double floor_ = (polish ? 1e-4 : 0.1 * kappa) * sqrt_n;
+        int info = 0;
+        int64_t inner = 0;
+        DV_TRY(gmres(W, op, W.b, polish ? 1e-3 : C.o.eta, floor_, C.o.krylov_dim, &info, &inner, st));
+        if (polish) r.gmres_polish += inner;
+        else { r.gmres_iters += inner; if (C.gm_counter) *C.gm_counter += inner; }
+        if (info != 0 && C.o.allow_refresh && !new_lu && !polish) {
+            DV_TRY(refresh_J(C, t, W.z, dh, st));
+            new_lu = true;
+            r.refreshed = 1;
+            r.jac_refresh_in_newton += 1;
+            DV_TRY(pnorm(W.R, W.s, &pn));
+            int64_t inner2 = 0;
+            DV_TRY(gmres(W, op, W.b, C.o.eta, floor_, C.o.krylov_dim, &info, &inner2, st));
+            r.gmres_iters += inner2;
+            if (C.gm_counter) *C.gm_counter += inner2;
+        }
+        // dz = prec(w) * s
+        DV_TRY(precond_apply(m, W.x, W.s, W.u, st));
+        k_mul<<<g, VB, 0, st>>>(n, W.u, W.s, W.dz);
+        double dzn;
+        DV_TRY(rms_ratio(W, n, W.dz, nullptr, &dzn, st));
+        if (!std::isfinite(dzn)) {
+            DV_TRY(copy(z0, zout));
+            r.iters = it + 1;
+            r.rate = INFINITY;
+            return DV_OK;
+        }
+        double lam = 1.0, rn_try = 0.0, pn_try = INFINITY;
+        for (int ls = 0; ls < 4; ++ls) {
+            k_truncate<<<g, VB, 0, st>>>(n, C.npos, W.z, lam, W.dz, W.zt);
+            DV_TRY(stage(W.zt, W.ft, W.Rt));
+            DV_TRY(rms_ratio(W, n, W.Rt, W.s, &rn_try, st));
+            if (std::isfinite(rn_try)) DV_TRY(pnorm(W.Rt, W.s, &pn_try));
+            else pn_try = INFINITY;
+            if (std::isfinite(pn_try) && (pn_try <= (1.0 - 1e-4 * lam) * pn || ls == 3)) break;
+            lam *= 0.5;
+        }
+        if (!std::isfinite(pn_try)) {
+            DV_TRY(copy(z0, zout));
+            r.iters = it + 1;
+            r.rate = INFINITY;
+            return DV_OK;
+        }
+        // step = rms((z_try - z)/s)
+        k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.tmp);
+        double step;
+        DV_TRY(rms_ratio(W, n, W.tmp, W.s, &step, st));
+        std::swap(W.z, W.zt);
+        std::swap(W.f, W.ft);
+        std::swap(W.R, W.Rt);
+        rn = rn_try;
+        pn = pn_try;
+        const double rate = (step_prev < 0.0) ? 0.0 : step / std::max(step_prev, 1e-300);
+        const bool sp = step_prev >= 0.0;
+        const bool converged = (lam == 1.0 && step <= kappa && (info == 0 || sp)) ||
+                               (sp && lam == 1.0 && info == 0 && rate < 1.0 && rate / (1.0 - rate) * step <= kappa) ||
+                               pn <= kappa;
+        if (converged) {
+            if (!have_best || rn < best_rn) {
+                have_best = true;
+                best_rn = rn;
+                DV_TRY(copy(W.z, W.best));
+            }
+            bool ok;
+            DV_TRY(cons_ok(W.R, W.z, &ok));
+            if (ok) {
+                DV_TRY(copy(W.z, zout));
+                r.ok = 1; r.iters = it + 1; r.rate = rate;
+                return DV_OK;
+            }
+            if (polish < 2) {
+                polish += 1;
+                step_prev = -1.0;
+                continue;
+            }
+            r.balance_unclosed += 1;
+            DV_TRY(copy(W.best, zout));
+            r.ok = 1; r.iters = it + 1; r.rate = rate;
+            return DV_OK;
+        }
+        if (have_best) {
+            r.balance_unclosed += 1;
+            DV_TRY(copy(W.best, zout));
+            r.ok = 1; r.iters = it + 1; r.rate = rate;
+            return DV_OK;
+        }
+        if (sp && lam == 1.0 && info == 0) {
+            const int left = C.o.max_iter - it - 1;
+            if (it >= 2 && (rate >= 1.0 || std::pow(rate, left) / (1.0 - rate) * step > kappa * 1e3)) {
+                DV_TRY(copy(W.z, zout));
+                r.ok = 0; r.iters = it + 1; r.rate = rate;
+                return DV_OK;
+            }
+        }
+        step_prev = step;
+    }
+    DV_TRY(copy(W.z, zout));
+    r.ok = 0;
+    r.iters = it + 1;
+    r.rate = 1.0;
+    return DV_OK;
+}
+
+}  // namespace dv
+
+// ================================================================== integrator (TRBDF2, core/solver.py:297-511)
+namespace dv {
+
+static const double GAMMA_ = 2.0 - 1.4142135623730951;        // 2 - sqrt 2 (np.sqrt(2.0))
+static const double D_ = GAMMA_ / 2.0;
+static const double C1_ = 1.0 / (GAMMA_ * (2.0 - GAMMA_));
+static const double C2_ = (1.0 - GAMMA_) * (1.0 - GAMMA_) / (GAMMA_ * (2.0 - GAMMA_));
+static const double W1_ = (3.0 * GAMMA_ - 1.0) / (6.0 * GAMMA_);
+static const double W2_ = 1.0 / (6.0 * GAMMA_ * (1.0 - GAMMA_));
+static const double W3_ = (2.0 - 3.0 * GAMMA_) / (6.0 * (1.0 - GAMMA_));
+static const double G_SD_ = 1.0 - 1.0 / 1.4142135623730951;
+static const double SW1_ = (3.0 * G_SD_ - 1.0) / (6.0 * G_SD_);
+static const double SW2_ = 1.0 / (6.0 * G_SD_ * (1.0 - G_SD_));
+static const double SW3_ = (2.0 - 3.0 * G_SD_) / (6.0 * (1.0 - G_SD_));
+
+// out = y + a * ((z1 - y) / dh)       (SDIRK2 stage-2 right-hand side, core/solver.py:430-431)
+__global__ void k_sd_rhs2(int64_t n, const double* __restrict__ y, const double* __restrict__ z1, double dh, double a,
+                          double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = y[i] + a * ((z1[i] - y[i]) / dh);
+}
+// out = truncate(y + (z1 - y)/c, y)    (stage-2 predictor, core/solver.py:432,435)
+__global__ void k_pred2(int64_t n, int64_t npos, const double* __restrict__ y, const double* __restrict__ z1, double c,
+                        double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = y[i] + (z1[i] - y[i]) / c;
+        if (i < npos) v = npmax(v, 0.1 * npmax(y[i], 0.0));
+        out[i] = v;
+    }
+}
+// out = (z2 - y) / h
+__global__ void k_slope(int64_t n, const double* __restrict__ y, const double* __restrict__ z2, double h,
+                        double* __restrict__ out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (z2[i] - y[i]) / h;
+}
+
+}  // namespace dv
+
+struct dv_integrator {
+    dv_model* m;
+    dv_solver_opts o;
+    int64_t n;
+    double *y, *fn, *slope, *z1, *z2, *f1, *f2, *rhs1, *rhs2, *pred, *ev, *es, *d_g;   // device vectors
+    double* h_g;                  // pinned: 3 x DV_NACC accumulator rates
+    double acc[DV_NACC], gn[DV_NACC];
+    double t, t_end, h, h_cap, h_lu, log_refactor;
+    bool have_J, have_lu, fresh, have_slope, started;
+    int jac_age;
+    int64_t gm;                   // GMRES iterations (non-polish) since start
+    dv_step_report rep;
+};
+
+using namespace dv;
+
+extern "C" {
+
+int dv_abi_version(void) { return DV_ABI_VERSION; }
+size_t dv_step_params_size(void) { return sizeof(dv_step_params); }
+const char* dv_last_error(void) { return g_err.c_str(); }
+
+int dv_device_count(int* n) {
+    if (!n) return DV_ERR_ARG;
+    cudaError_t e = cudaGetDeviceCount(n);
+    if (e != cudaSuccess) {
+        *n = 0;
+        cudaGetLastError();
+    }
+    return DV_OK;
+}
+
+int dv_model_destroy(dv_model* m) {
+    if (!m) return DV_OK;
+    void* ptrs[] = {m->d_aux, m->d_rec, m->d_acc, m->d_pc, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (m->W) {
+        work_free(*m->W);
+        delete m->W;
+    }
+    delete m;
+    return DV_OK;
+}
+
+int dv_model_create(const dv_step_params* p, const double* feed_flux, const double* n_nom, const double* coverage,
+                    dv_model** out) {
+    if (!p || !out || !feed_flux || !n_nom || !coverage) { set_error("null argument"); return DV_ERR_ARG; }
+    if (p->Nr < 1 || p->Nth < 1 || p->Nz < 1 || p->Nr > DV_MAX_NR || p->Nth == 2) {
+        set_error("grid dimensions outside the supported range (1 <= Nr <= 64, Ntheta != 2)");
+        return DV_ERR_ARG;
+    }
+    dv_model* m = new dv_model();
+    memset(m, 0, sizeof(dv_model));
+    m->p = *p;
+    m->nc = (int64_t)p->Nr * p->Nth * p->Nz;
+    m->nw = p->wall_on ? (int64_t)p->Nth * p->Nz : 0;
+    m->n = DV_NV * m->nc + m->nw;
+    m->rl = rec_layout(*p);
+    m->jac_doubles = (int64_t)DV_NSLOT * DV_NB * DV_NB * m->nc;
+    const int64_t nf = (int64_t)p->Nr * p->Nth, nwall = (int64_t)p->Nth * p->Nz;
+    int nb_sector = DV_NV * p->Nr + (p->wall_on ? 1 : 0);
+    int nb_full = DV_NV * p->Nr * p->Nth + (p->wall_on ? p->Nth : 0);
+    bool full_ok = nb_full <= 512;
+    m->pc_cap_nb = full_ok ? std::max(nb_full, nb_sector) : nb_sector;
+    m->pc_cap_parts = p->Nth;
+    int64_t pc_need = std::max((int64_t)p->Nth * p->Nz * 5 * (int64_t)nb_sector * nb_sector,
+                               full_ok ? (int64_t)p->Nz * 5 * (int64_t)nb_full * nb_full : (int64_t)0);
+    int64_t work_need = (int64_t)m->pc_cap_parts * 4 * (int64_t)m->pc_cap_nb * m->pc_cap_nb;
+    const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
+    bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_atol7, sizeof(double) * DV_NB) != cudaSuccess;
+    if (fail) {
+        int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(model workspace)");
+        dv_model_destroy(m);
+        return rc;
+    }
+    m->W = new Work();
+    int rc = work_alloc(*m->W, m->n, 30, m->jac_doubles);
+    if (rc != DV_OK) {
+        dv_model_destroy(m);
+        return rc;
+    }
+    cudaMemcpy(m->d_aux, feed_flux, sizeof(double) * nf, cudaMemcpyHostToDevice);
+    cudaMemcpy(m->d_aux + nf, n_nom, sizeof(double) * nf, cudaMemcpyHostToDevice);
+    cudaMemcpy(m->d_aux + 2 * nf, coverage, sizeof(double) * nwall, cudaMemcpyHostToDevice);
+    cudaMemcpy(m->d_atol7, p->atol, sizeof(double) * DV_NB, cudaMemcpyHostToDevice);
+    m->aux.feed_flux = m->d_aux;
+    m->aux.n_nom = m->d_aux + nf;
+    m->aux.cov = m->d_aux + 2 * nf;
+    cudaMemset(m->d_rec, 0, sizeof(double) * rec_n);
+    int32_t ncol = 0;
+    std::vector<int64_t> colour((size_t)m->n);
+    rc = dv_colour_columns(p->Nr, p->Nth, p->Nz, p->wall_on, colour.data(), &ncol);
+    if (rc != DV_OK) {
+        dv_model_destroy(m);
+        return rc;
+    }
+    m->ncolours = ncol;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        dv_model_destroy(m);
+        return cuda_fail(e, "dv_model_create");
+    }
+    *out = m;
+    return DV_OK;
+}
+
+int dv_model_sizes(const dv_model* m, int64_t* n_core, int64_t* ncell, int64_t* n_wall, int64_t* jac_doubles,
+                   int64_t* diag_doubles) {
+    if (!m) return DV_ERR_ARG;
+    if (n_core) *n_core = m->n;
+    if (ncell) *ncell = m->nc;
+    if (n_wall) *n_wall = m->nw;
+    if (jac_doubles) *jac_doubles = m->jac_doubles;
+    if (diag_doubles) *diag_doubles = m->rl.total;
+    return DV_OK;
+}
+
+int64_t dv_model_nfev(const dv_model* m) { return m ? m->nfev : -1; }
+
+int dv_rhs(dv_model* m, double t, const double* y, double* f, double* acc, void* stream) {
+    if (!m || !y || !f) { set_error("null argument"); return DV_ERR_ARG; }
+    return launch_rhs(m, t, y, f, acc, (cudaStream_t)stream);
+}
+
+int dv_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known, double* R,
+                      void* stream) {
+    if (!m || !y || !rhs_known || !R) { set_error("null argument"); return DV_ERR_ARG; }
+    return launch_stage_residual(m, t, y, gamma_h, rhs_known, R, (cudaStream_t)stream);
+}
+
+int dv_rhs_diag(dv_model* m, double t, const double* y, double* diag, void* stream) {
+    if (!m || !y || !diag) { set_error("null argument"); return DV_ERR_ARG; }
+    return launch_diag(m, t, y, diag, (cudaStream_t)stream);
+}
+
+int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, void* stream) {
+    if (!m || !y || !f0 || !J) { set_error("null argument"); return DV_ERR_ARG; }
+    m->nfev += m->ncolours;
+    return launch_fd_jacobian(m, t, y, f0, J, (cudaStream_t)stream);
+}
+
+int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, void* stream) {
+    if (!m || !J) { set_error("null argument"); return DV_ERR_ARG; }
+    return precond_factor(m, J, dh, mode, (cudaStream_t)stream);
+}
+
+int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream) {
+    if (!m || !b || !x) { set_error("null argument"); return DV_ERR_ARG; }
+    return precond_apply(m, b, nullptr, x, (cudaStream_t)stream);
+}
+
+int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_known, double dh, const dv_newton_opts* o,
+                    double* z_out, dv_newton_result* r, void* stream) {
+    if (!m || !z0 || !rhs_known || !o || !z_out || !r) { set_error("null argument"); return DV_ERR_ARG; }
+    if (!m->pc_ready) { set_error("dv_newton_stage needs a factorised preconditioner"); return DV_ERR_ARG; }
+    if (o->krylov_dim < 1 || o->krylov_dim > m->W->kdim) { set_error("krylov_dim outside 1..30"); return DV_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    memset(r, 0, sizeof(*r));
+    NewtonCtx C{m, m->W, m->d_atol7, m->n, DV_NG * m->nc + DV_NA * m->nc, *o, r, nullptr};
+    int rc = newton_krylov(C, t, z0, rhs_known, dh, z_out, st);
+    cudaStreamSynchronize(st);
+    return rc;
+}
+
+// ------------------------------------------------------------------ integrator
+int dv_integrator_destroy(dv_integrator* g) {
+    if (!g) return DV_OK;
+    double* ptrs[] = {g->y, g->fn, g->slope, g->z1, g->z2, g->f1, g->f2, g->rhs1, g->rhs2, g->pred, g->ev, g->es, g->d_g};
+    for (double* q : ptrs)
+        if (q) cudaFree(q);
+    if (g->h_g) cudaFreeHost(g->h_g);
+    delete g;
+    return DV_OK;
+}
+
+int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** out) {
+    if (!m || !o || !out) { set_error("null argument"); return DV_ERR_ARG; }
+    if (o->scheme != 0 && o->scheme != 1) { set_error("scheme must be 0 (sdirk2) or 1 (trbdf2)"); return DV_ERR_ARG; }
+    dv_integrator* g = new dv_integrator();
+    memset(g, 0, sizeof(dv_integrator));
+    g->m = m;
+    g->o = *o;
+    g->n = m->n;
+    g->log_refactor = std::log(o->refactor_ratio);
+    double** vecs[] = {&g->y, &g->fn, &g->slope, &g->z1, &g->z2, &g->f1, &g->f2, &g->rhs1, &g->rhs2, &g->pred, &g->ev, &g->es};
+    for (double** v : vecs) {
+        if (cudaMalloc((void**)v, sizeof(double) * g->n) != cudaSuccess) {
+            int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(integrator)");
+            dv_integrator_destroy(g);
+            return rc;
+        }
+    }
+    if (cudaMalloc((void**)&g->d_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
+        cudaMallocHost((void**)&g->h_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess) {
+        int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(integrator)");
+        dv_integrator_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return DV_OK;
+}
+
+int dv_integrator_start(dv_integrator* g, const double* y0, double t_end, void* stream) {
+    if (!g || !y0) { set_error("null argument"); return DV_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    g->t = 0.0;
+    g->t_end = t_end;
+    DV_CUDA(cudaMemcpyAsync(g->y, y0, sizeof(double) * g->n, cudaMemcpyDefault, st));
+    DV_TRY(launch_rhs(g->m, 0.0, g->y, g->fn, g->d_g, st));
+    DV_CUDA(cudaMemcpyAsync(g->h_g, g->d_g, sizeof(double) * DV_NACC, cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    memcpy(g->gn, g->h_g, sizeof(double) * DV_NACC);
+    memset(g->acc, 0, sizeof(g->acc));
+    g->h = std::min(std::min(g->o.h_init, g->o.h_max), t_end);
+    g->have_J = g->have_lu = g->fresh = g->have_slope = false;
+    g->jac_age = 0;
+    g->h_cap = INFINITY;
+    g->h_lu = 0.0;
+    g->gm = 0;
+    memset(&g->rep, 0, sizeof(g->rep));
+    g->rep.nfev = g->m->nfev;
+    g->started = true;
+    return DV_OK;
+}
+
+const double* dv_integrator_y(const dv_integrator* g) { return g ? g->y : nullptr; }
+
+int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream) {
+    if (!g || !dst) { set_error("null argument"); return DV_ERR_ARG; }
+    DV_CUDA(cudaMemcpyAsync(dst, g->y, sizeof(double) * g->n, cudaMemcpyDefault, (cudaStream_t)stream));
+    DV_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return DV_OK;
+}
+
+int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep, void* stream) {
+    if (!g || !rep) { set_error("null argument"); return DV_ERR_ARG; }
+    if (!g->started) { set_error("dv_integrator_advance before dv_integrator_start"); return DV_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    dv_model* m = g->m;
+    Work& W = *m->W;
+    const int64_t n = g->n;
+    const unsigned gr = vgrid(n);
+    const int64_t npos = (int64_t)(DV_NG + DV_NA) * m->nc;
+    const bool sd = g->o.scheme == 0;
+    const double c_mid = sd ? G_SD_ : GAMMA_;
+    dv_step_report& R = g->rep;
+    const int64_t nfev0 = m->nfev;
+    const int64_t nfev_base = R.nfev;
+    auto sync_nfev = [&]() { R.nfev = nfev_base + (m->nfev - nfev0); };
+    dv_newton_opts no;
+    no.max_iter = g->o.max_newton_iter;
+    no.krylov_dim = 30;
+    no.precond_mode = g->o.precond_mode;
+    no.kappa = g->o.newton_kappa;
+    no.eta = 1e-2;
+    no.rtol = g->o.rtol;
+    no.cons_tol = g->o.conservation_tol;
+    while (g->t < g->t_end * (1.0 - 1e-12)) {
+        const int64_t gm0 = g->gm;
+        if (R.n_steps + R.n_reject + R.n_newton_fail > g->o.max_steps) {
+            sync_nfev();
+            *rep = R;
+            char buf[160];
+            snprintf(buf, sizeof buf, "too many steps at t=%.4gs", g->t);
+            set_error(buf);
+            return DV_ERR_STEPS;
+        }
+        const double h_desired = g->h;
+        double h = std::min(std::min(g->h, g->o.h_max), t_target - g->t);
+        const bool truncated = h < h_desired * (1.0 - 1e-9);
+        if (h < 1e-10 * std::max(1.0, g->t_end)) {
+            sync_nfev();
+            *rep = R;
+            char buf[160];
+            snprintf(buf, sizeof buf, "step size underflow (h=%.3e) at t=%.6gs", h, g->t);
+            set_error(buf);
+            return DV_ERR_UNDERFLOW;
+        }
+        g->h = h;
+        if (!g->have_J || g->jac_age >= g->o.jacobian_max_age) {
+            DV_TRY(launch_fd_jacobian(m, g->t, g->y, g->fn, W.J, st));
+            m->nfev += m->ncolours;
+            R.n_jac += 1;
+            g->have_J = true;
+            g->jac_age = 0;
+            g->fresh = true;
+            g->have_lu = false;
+        }
+        if (!g->have_lu || std::fabs(std::log(h / g->h_lu)) > g->log_refactor) {
+            DV_TRY(precond_factor(m, W.J, D_ * h, g->o.precond_mode, st));
+            g->h_lu = h;
+            R.n_lu += 1;
+            g->have_lu = true;
+        }
+        const double dh = D_ * h;
+        // ---- stage 1
+        if (sd) DV_CUDA(cudaMemcpyAsync(g->rhs1, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        else k_xpay<<<gr, VB, 0, st>>>(n, g->y, dh, g->fn, g->rhs1);
+        if (g->have_slope) {
+            k_xpay<<<gr, VB, 0, st>>>(n, g->y, c_mid * h, g->slope, g->pred);
+            k_truncate_to<<<gr, VB, 0, st>>>(n, npos, g->pred, g->y, g->pred);
+        } else {
+            DV_CUDA(cudaMemcpyAsync(g->pred, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        no.allow_refresh = g->fresh ? 0 : 1;          // self._fresh = fresh (set before stage 1)
+        dv_newton_result r1;
+        memset(&r1, 0, sizeof r1);
+        NewtonCtx C1{m, &W, m->d_atol7, n, npos, no, &r1, &g->gm};
+        DV_TRY(newton_krylov(C1, g->t + c_mid * h, g->pred, g->rhs1, dh, g->z1, st));
+        R.n_krylov += 1;
+        R.gmres_iters += r1.gmres_iters;
+        R.gmres_polish += r1.gmres_polish;
+        R.balance_unclosed += r1.balance_unclosed;
+        R.jac_refresh_in_newton += r1.jac_refresh_in_newton;
+        if (r1.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+        if (r1.refreshed) {
+            R.n_jac += 1;
+            R.n_lu += 1;
+            g->h_lu = dh / D_;
+            g->jac_age = 0;
+            g->fresh = true;
+        }
+        bool ok = r1.ok != 0;
+        if (ok) {
+            if (sd) k_sd_rhs2<<<gr, VB, 0, st>>>(n, g->y, g->z1, dh, (1.0 - G_SD_) * h, g->rhs2);
+            else k_axpby<<<gr, VB, 0, st>>>(n, C1_, g->z1, -C2_, g->y, g->rhs2);
+            k_pred2<<<gr, VB, 0, st>>>(n, npos, g->y, g->z1, c_mid, g->pred);
+            dv_newton_result r2;
+            memset(&r2, 0, sizeof r2);
+            NewtonCtx C2{m, &W, m->d_atol7, n, npos, no, &r2, &g->gm};
+            DV_TRY(newton_krylov(C2, g->t + h, g->pred, g->rhs2, dh, g->z2, st));
+            R.n_krylov += 1;
+            R.gmres_iters += r2.gmres_iters;
+            R.gmres_polish += r2.gmres_polish;
+            R.balance_unclosed += r2.balance_unclosed;
+            R.jac_refresh_in_newton += r2.jac_refresh_in_newton;
+            if (r2.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+            if (r2.refreshed) {
+                R.n_jac += 1;
+                R.n_lu += 1;
+                g->h_lu = dh / D_;
+                g->jac_age = 0;
+                g->fresh = true;
+            }
+            ok = r2.ok != 0;
+        }
+        if (!ok) {
+            R.n_newton_fail += 1;
+            if (!g->fresh) {
+                g->have_J = false;
+            } else {
+                g->h_cap = std::min(g->h_cap, 0.5 * h);
+                g->h = h * 0.3;
+                g->have_lu = false;
+            }
+            continue;
+        }
+        // ---- error estimate filtered by M^-1 (core/solver.py:454-469)
+        DV_TRY(launch_rhs(m, g->t + c_mid * h, g->z1, g->f1, g->d_g + DV_NACC, st));
+        DV_TRY(launch_rhs(m, g->t + h, g->z2, g->f2, g->d_g + 2 * DV_NACC, st));
+        if (sd) k_err_vec<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, SW1_, g->fn, SW2_, g->f1, SW3_, g->f2, g->ev);
+        else k_err_vec<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, W1_, g->fn, W2_, g->f1, W3_, g->f2, g->ev);
+        DV_TRY(precond_apply(m, g->ev, nullptr, g->ev, st));
+        k_err_scale<<<gr, VB, 0, st>>>(m->nc, n, g->y, g->z2, m->d_atol7, g->o.rtol, g->es);
+        double en;
+        DV_TRY(rms_ratio(W, n, g->ev, g->es, &en, st));
+        if (!std::isfinite(en)) en = 1e6;
+        R.err_norm = en;
+        if (en > 1.0) {
+            R.n_reject += 1;
+            g->h = h * std::max(0.2, 0.9 * std::pow(en, -1.0 / 3.0));
+            continue;
+        }
+        // ---- accept
+        DV_CUDA(cudaMemcpyAsync(g->h_g + DV_NACC, g->d_g + DV_NACC, sizeof(double) * 2 * DV_NACC,
+                                cudaMemcpyDeviceToHost, st));
+        DV_CUDA(cudaStreamSynchronize(st));
+        const double* g1 = g->h_g + DV_NACC;
+        const double* g2 = g->h_g + 2 * DV_NACC;
+        for (int q = 0; q < DV_NACC; ++q) {
+            if (sd) {
+                g->acc[q] = g->acc[q] + h * ((1.0 - G_SD_) * g1[q] + G_SD_ * g2[q]);
+            } else {
+                double acc_g = g->acc[q] + D_ * h * (g->gn[q] + g1[q]);
+                g->acc[q] = C1_ * acc_g - C2_ * g->acc[q] + D_ * h * g2[q];
+            }
+        }
+        k_slope<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, g->slope);
+        g->have_slope = true;
+        std::swap(g->y, g->z2);
+        std::swap(g->fn, g->f2);
+        memcpy(g->gn, g2, sizeof(double) * DV_NACC);
+        g->t = g->t + h;
+        R.n_steps += 1;
+        g->jac_age += 1;
+        g->fresh = false;
+        if (g->gm - gm0 > g->o.gmres_refresh) g->jac_age = g->o.jacobian_max_age;
+        double fac = (en < 1e-8) ? 4.0 : std::min(4.0, std::max(0.2, 0.9 * std::pow(en, -1.0 / 3.0)));
+        if (1.0 <= fac && fac < 1.25) fac = 1.0;
+        double hn = truncated ? std::max(h * fac, h_desired) : h * fac;
+        g->h_cap *= 1.15;
+        g->h = std::min(hn, g->h_cap);
+        R.t = g->t;
+        R.h_used = h;
+        memcpy(R.acc, g->acc, sizeof(g->acc));
+        sync_nfev();
+        DV_CUDA(cudaStreamSynchronize(st));
+        *rep = R;
+        return DV_OK;
+    }
+    R.t = g->t;
+    sync_nfev();
+    *rep = R;
+    return DV_OK;
+}
+
+}  // extern "C"

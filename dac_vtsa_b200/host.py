@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import copy
 from dataclasses import dataclass, field
+from enum import Enum
 from typing import Dict, Optional, Tuple
 
 import numpy as np
@@ -185,12 +186,20 @@ class Grid:
 
 # ------------------------------------------------------------------ valves -> end conditions
 
+class ValveState(str, Enum):
+    """Valve states of a cycle step (valves/valve_logic.py:41-45)."""
+    CLOSED = "CLOSED"
+    OPEN = "OPEN"
+    OPEN_ATMOSPHERIC = "OPEN_ATMOSPHERIC"
+    OPEN_VACUUM = "OPEN_VACUUM"
+
+
 @dataclass
 class EndCondition:
     """Boundary condition of one column end for one step (valves/valve_logic.py:48-60)."""
     end: str
     valve: Optional[str]
-    state: str
+    state: ValveState
     kind: str                      # closed | feed | pump | valve | pressure
     P_target: float = 101325.0
     y_ext: Optional[np.ndarray] = None
@@ -227,13 +236,13 @@ def end_conditions(cfg, step: Dict, species, props) -> Dict[str, EndCondition]:
             if ports[v] == end and step["valves"][v] != "CLOSED":
                 valve = v
         if valve is None:
-            out[end] = EndCondition(end, None, "CLOSED", "closed")
+            out[end] = EndCondition(end, None, ValveState.CLOSED, "closed")
             continue
-        st = step["valves"][valve]
+        st = ValveState(step["valves"][valve])
         is_prod = step.get("product_port", "V3") == valve
-        if st == "OPEN":
+        if st == ValveState.OPEN:
             out[end] = EndCondition(end, valve, st, "feed", feed.P, y_feed, feed.T, is_feed=True)
-        elif st == "OPEN_ATMOSPHERIC":
+        elif st == ValveState.OPEN_ATMOSPHERIC:
             kind = "valve" if cfg.operation.vent_model == "valve" else "pressure"
             kv = cfg.operation.vent_conductance
             if valve == "V1":

@@ -1,0 +1,227 @@
+/*
+ * dacvtsa.h -- C ABI of the B200 implicit stepping path of the dac_vtsa TVSA simulator.
+ *
+ * The reference (Navneet07rkt/dac_vtsa) is pure Python; its "plugin interface" for this path
+ * is the object protocol the step runner drives (steps/_runner.py:87-153):
+ *   TVSAModel (core/residual.py:40-482)  -> dv_model_* , dv_rhs, dv_stage_residual, dv_rhs_diag
+ *   FDJacobian (core/jacobian.py:21-91), color_columns (numerics/sparsity.py:88-107)
+ *                                        -> dv_colour_columns, dv_fd_jacobian
+ *   TRBDF2._factor / splu (core/solver.py:334-337)
+ *                                        -> dv_precond_factor, dv_precond_solve
+ *   newton_krylov (core/solver.py:154-294) -> dv_newton_stage
+ *   TRBDF2.integrate (core/solver.py:370-511) -> dv_integrator_*
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Plain C types only.  Vectors are DEVICE pointers (FP64) unless stated; `stream` is a
+ *    cudaStream_t passed as void* (NULL = legacy default stream).  Calls are asynchronous on
+ *    `stream` unless they return host values (documented per call).
+ *  - State layout (variable-major, core/residual.py:110-118):
+ *      y = [c_CO2 | c_H2O | c_N2 | q_CO2 | q_H2O | e | Tw]
+ *    each cell block ncell long in C order (i_r*Ntheta + j_theta)*Nz + k_z, then Tw over
+ *    (Ntheta, Nz).  n_core = 6*ncell + Ntheta*Nz (wall enabled) or 6*ncell.
+ *  - Return value: 0 = success; < 0 = error (dv_last_error() gives the message):
+ *      DV_ERR_ARG (-1) bad argument / size, DV_ERR_CUDA (-2) CUDA runtime error,
+ *      DV_ERR_UNSUPPORTED (-3) configuration without a GPU implementation,
+ *      DV_ERR_STEPS (-10) too many steps (reference: SolverError "too many steps"),
+ *      DV_ERR_UNDERFLOW (-11) step size underflow (reference: SolverError "step size underflow").
+ *  - Handles are not thread-safe (the reference model/integrator are not either); one handle
+ *    per thread.  No entry point allocates device memory except *_create.
+ */
+#ifndef DACVTSA_H
+#define DACVTSA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DV_ABI_VERSION 1
+#define DV_MAX_NR 64          /* radial rings supported by the per-ring parameter arrays      */
+#define DV_NG 3               /* gas species CO2, H2O, N2 (components.water = true)            */
+#define DV_NA 2               /* adsorbed species CO2, H2O                                     */
+#define DV_NV 6               /* unknowns per cell: 3 c, 2 q, e                                */
+#define DV_NACC 36            /* accumulator rates (core/residual.py:126-133)                  */
+#define DV_NSLOT 9            /* Jacobian neighbour slots: self, z-1, z+1, z-2, z+2, r-1, r+1, th-1, th+1 */
+#define DV_NB 7               /* Jacobian block size: 6 cell unknowns + the wall unknown of the cell  */
+
+#define DV_OK 0
+#define DV_ERR_ARG (-1)
+#define DV_ERR_CUDA (-2)
+#define DV_ERR_UNSUPPORTED (-3)
+#define DV_ERR_STEPS (-10)
+#define DV_ERR_UNDERFLOW (-11)
+
+enum dv_end_kind { DV_END_CLOSED = 0, DV_END_FEED = 1, DV_END_PUMP = 2, DV_END_VALVE = 3, DV_END_PRESSURE = 4 };
+enum dv_limiter { DV_LIM_VAN_ALBADA = 0, DV_LIM_VAN_ALBADA_TVD = 1, DV_LIM_VAN_LEER = 2, DV_LIM_MINMOD = 3,
+                  DV_LIM_UPWIND = 4 };
+enum dv_coads { DV_COADS_NONE = 0, DV_COADS_WADST = 1, DV_COADS_MECHANISTIC = 2, DV_COADS_STAMPI = 3 };
+enum dv_disp { DV_DISP_EDWARDS_RICHARDSON = 0, DV_DISP_YOUNG2021 = 1, DV_DISP_WAKAO_KAGEI = 2 };
+enum dv_bedcond { DV_BED_ZEHNER_SCHLUNDER = 0, DV_BED_PARALLEL = 1, DV_BED_CONSTANT = 2 };
+enum dv_wallhtc { DV_HTC_MARTIN_NILLES = 0, DV_HTC_CONSTANT = 1 };
+
+/* One column end for one cycle step (valves/valve_logic.py:48-109, boundaries/conditions.py:75-160). */
+typedef struct dv_end {
+    int32_t kind;            /* dv_end_kind */
+    int32_t valve;           /* 0,1,2 = V1,V2,V3 open at this end; -1 = none */
+    int32_t check_valve, is_vacuum, is_feed, pad_;
+    double P_target, T_ext, speed, P_start;   /* P_start: mean layer pressure at step start */
+    double y_ext[DV_NG];
+} dv_end;
+
+/* Per-step constants of the residual (everything TVSAModel.__init__ derives, core/residual.py:41-123). */
+typedef struct dv_step_params {
+    int32_t Nr, Nth, Nz, wall_on;
+    /* geometry (core/grid.py:61-96); per-ring arrays have Nr entries, per-r-face arrays Nr-1 */
+    double dz, dth, half_dr_outer, A_wall_in, A_wall_out, wall_C, wall_kz, wall_kt;
+    double Az[DV_MAX_NR], V[DV_MAX_NR], Ath[DV_MAX_NR], arc[DV_MAX_NR], Ar[DV_MAX_NR], drc[DV_MAX_NR];
+    /* sorbent + thermodynamics (physics/energy.py:31-52) */
+    double eps_b, eps_t, rho_b, cp_s, dp, T_ref;
+    double cpg[DV_NG], cpa[DV_NA], dH[DV_NA];
+    /* gas data (properties/ideal_gas_backend.py): mu_s = sum_t mu_w*(mu_D*T + mu_E);
+       k_s = sum_t k_w*k_0*(T/300)^k_n ; nt = number of terms (air = N2/O2 blend) */
+    double M[DV_NG];
+    double mu_w[DV_NG][2], mu_D[DV_NG][2], mu_E[DV_NG][2];
+    double k_w[DV_NG][2], k_0[DV_NG][2], k_n[DV_NG][2];
+    int32_t mu_nt[DV_NG], k_nt[DV_NG];
+    double mass_q[DV_NG][DV_NG], wilke_den[DV_NG][DV_NG];
+    double fuller_sqrtM[2], fuller_s[2];       /* pairs CO2-AIR, CO2-H2O (utils/diffusion.py:19-26) */
+    /* isotherms (physics/isotherms.py) */
+    double co2_q_inf0, co2_chi, co2_b0, co2_dH0, co2_tau0, co2_alpha, co2_T0, p_reg;
+    double h2o_q_m, h2o_C, h2o_D, h2o_F, h2o_G, h2o_E10_slope, h2o_E10_intercept, rh_cap;
+    double wadst_b0, wadst_q_inf0, wadst_tau0, wadst_chi, wadst_alpha, wadst_dH, wadst_A;
+    double mech_f_blocked_max, mech_k, mech_phi_dry, mech_A, mech_dH_wet, mech_n;
+    double sb_gamma, sb_beta;
+    int32_t coads, basis_state;
+    /* LDF kinetics (physics/kinetics.py) */
+    double k_ldf[DV_NA], Ea[DV_NA], T_ref_kin;
+    int32_t ea_zero;
+    /* transport (physics/pressure.py, dispersion.py, heat_transfer.py) */
+    int32_t disp_model, bed_model, htc_model, lumped;
+    double ka, kb, g1, g2, er_beta, Pe_T, lam_const, zs_B, zs_s, lam_s, Pe_r, Pe_z, alpha_const, N_ratio, U_lumped;
+    double u_nom;
+    int32_t limiter, pad0_;
+    /* ends 0 = top (z = 0), 1 = bottom (z = L) */
+    dv_end ends[2];
+    double tau_valve;
+    /* jacket, wall, exchanger (core/residual.py:87-100,328-359) */
+    int32_t jacket_on, hx_on;
+    double T_jac_set, T_jac_prev, jac_tau, h_jac, h_amb, T_amb, P_amb, hA_v;
+    /* energy accounting (core/residual.py:102-108,395-409) */
+    double gam, eta_vac, eta_bl;
+    int32_t vac_krishnamurthy, pump_water;
+    /* solver constants per variable block (core/residual.py:135-144, core/jacobian.py:39-48);
+       index 0..5 = cell unknowns, 6 = wall */
+    double atol[DV_NB], typ[DV_NB];
+} dv_step_params;
+
+typedef struct dv_model dv_model;
+typedef struct dv_integrator dv_integrator;
+
+/* ------------------------------------------------------------------ library */
+int dv_abi_version(void);
+size_t dv_step_params_size(void);
+const char* dv_last_error(void);
+int dv_device_count(int* n);
+
+/* ------------------------------------------------------------------ model
+ * Replaces TVSAModel.__init__ (core/residual.py:41-123).  Host inputs: feed_flux and n_nom over
+ * (Nr, Ntheta) [mol/s per inlet face; mol/m2/s nominal column flux, zeros without feed],
+ * coverage over (Ntheta, Nz).  Allocates all device workspaces of the model. */
+int dv_model_create(const dv_step_params* p, const double* feed_flux, const double* n_nom,
+                    const double* coverage, dv_model** out);
+int dv_model_destroy(dv_model* m);
+/* host values: n_core, ncell, wall unknowns, Jacobian block doubles, diagnostics doubles */
+int dv_model_sizes(const dv_model* m, int64_t* n_core, int64_t* ncell, int64_t* n_wall,
+                   int64_t* jac_doubles, int64_t* diag_doubles);
+/* host value: right-hand-side evaluations issued so far (TVSAModel.nfev, core/residual.py:123,213) */
+int64_t dv_model_nfev(const dv_model* m);
+
+/* f = dy/dt (TVSAModel.rhs, core/residual.py:211-365); acc (36 accumulator rates,
+ * core/residual.py:371-417) is written when non-NULL. */
+int dv_rhs(dv_model* m, double t, const double* y, double* f, double* acc, void* stream);
+/* R = y - gamma_h f(t, y) - rhs_known (TVSAModel.stage_residual, core/residual.py:420-423) */
+int dv_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known,
+                      double* R, void* stream);
+/* Diagnostics of TVSAModel.rhs(diag=True) (core/residual.py:366-368) into `diag` (diag_doubles):
+ * T, P [ncell]; y [3 ncell]; qstar [2 ncell]; uz [Nr Nth (Nz-1)]; ur [(Nr-1) Nth Nz]; uth [ncell];
+ * boundary records [2 ends][16][Nr Nth] = F_in(3) H_in u_out P_face F_inpart(3) F_outpart(3)
+ * H_inpart H_outpart T_layer 0; Q_jac, Q_amb, Q_wb, R_bed [Nth Nz]; Q_hx [ncell]. */
+int dv_rhs_diag(dv_model* m, double t, const double* y, double* diag, void* stream);
+
+/* ------------------------------------------------------------------ Jacobian
+ * Greedy distance-2 column colouring of the stencil pattern, bit-identical to
+ * color_columns(build_pattern(...)) (numerics/sparsity.py:29-107).  Host call; colour has
+ * n_core entries. */
+int dv_colour_columns(int32_t Nr, int32_t Nth, int32_t Nz, int32_t wall, int64_t* colour, int32_t* ncolours);
+/* Forward-difference Jacobian df/dy at (t, y) with f0 = f(t, y) (FDJacobian.__call__,
+ * core/jacobian.py:71-86): every colour perturbation in one launch.  J is the block layout
+ * J[slot][row 0..6][col 0..6][cell] (jac_doubles): d f_row(cell) / d y_col(neighbour `slot`),
+ * row/col 6 = the wall unknown of an outer-ring cell.  Same step rule h = 1.5e-8 max(|y|, typ). */
+int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, void* stream);
+
+/* ------------------------------------------------------------------ preconditioner
+ * Factorise M = I - dh J restricted to theta sectors (theta_block) or whole cross-sections
+ * (full) as a block-pentadiagonal LU along z (replaces splu of TRBDF2._factor,
+ * core/solver.py:334-337); mode 0 = theta_block, 1 = full.  Stored in the model. */
+int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, void* stream);
+/* x = M^-1 b with the stored factors (lu.solve). b and x may alias. */
+int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream);
+
+/* ------------------------------------------------------------------ stage solve */
+typedef struct dv_newton_opts {
+    int32_t max_iter, krylov_dim, allow_refresh, precond_mode;
+    double kappa, eta, rtol, cons_tol;
+} dv_newton_opts;
+
+typedef struct dv_newton_result {
+    int32_t ok, iters, refreshed, pad_;
+    double rate;
+    int64_t gmres_iters, gmres_polish, balance_unclosed, jac_refresh_in_newton;
+} dv_newton_result;
+
+/* Inexact Newton for R(z) = z - dh f(t, z) - rhs_known = 0 from z0 (newton_krylov,
+ * core/solver.py:154-294): GMRES(krylov_dim, one cycle) on the finite-difference operator,
+ * right-preconditioned by the stored factors; Armijo backtracking on ||M^-1 R/s||; positivity
+ * truncation; conservation polish.  With allow_refresh, a stalled GMRES re-linearises at the
+ * current iterate (Jacobian + factors are replaced in the model).  Synchronises `stream`. */
+int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_known, double dh,
+                    const dv_newton_opts* o, double* z_out, dv_newton_result* r, void* stream);
+
+/* ------------------------------------------------------------------ integrator */
+typedef struct dv_solver_opts {
+    int32_t scheme;            /* 0 = sdirk2, 1 = trbdf2 (solver.scheme) */
+    int32_t max_newton_iter, jacobian_max_age, gmres_refresh, precond_mode;
+    int32_t pad_;
+    int64_t max_steps;
+    double rtol, newton_kappa, refactor_ratio, conservation_tol, h_max, h_init;
+} dv_solver_opts;
+
+typedef struct dv_step_report {
+    double t, h_used, err_norm;
+    int64_t n_steps, n_reject, n_newton_fail, n_krylov, n_jac, n_lu, nfev;
+    int64_t gmres_iters, gmres_polish, balance_unclosed, jac_refresh_in_newton, krylov_ok, krylov_fail;
+    double acc[DV_NACC];       /* accumulator integrals since start (host copy) */
+} dv_step_report;
+
+/* TRBDF2(model, cfg, h_max, h_init) (core/solver.py:298-329) */
+int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** out);
+int dv_integrator_destroy(dv_integrator* g);
+/* integrate() prologue (core/solver.py:374-393): t = 0, y = y0 (device, copied), f_n, g_n. */
+int dv_integrator_start(dv_integrator* g, const double* y0, double t_end, void* stream);
+/* Advance until ONE step is accepted without passing t_target (core/solver.py:394-506):
+ * step-size limiting, Jacobian/LU reuse policy, two implicit stages, M^-1-filtered error test,
+ * accumulator quadrature, step-size update.  Host report; synchronises.  Returns DV_ERR_STEPS /
+ * DV_ERR_UNDERFLOW like the reference's SolverError. */
+int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep, void* stream);
+/* Device pointer to the current state y (n_core, owned by the integrator). */
+const double* dv_integrator_y(const dv_integrator* g);
+/* Copy the current state into dst (device or host memory); synchronises `stream`. */
+int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DACVTSA_H */

@@ -399,3 +399,39 @@ def fixed_step_run(model, y0, hs, scheme="trbdf2", rtol=1e-4, tol=1e-12):
         t, y, f_n, g_n = t + h, z2, f2, g2
         out.append(y.copy())
     return out, acc
+
+
+def explicit_dt(model, y, safety=0.5):
+    """Explicit stability limit (restates numerics/cfl.py:26-56)."""
+    g, cfg = model.grid, model.cfg
+    d = model.rhs(0.0, y, diag=True)
+    P = d["P"]
+    eps = model.eps_b
+    dp = cfg.sorbent.particle_diameter
+    dx_min = min(g.dz, float(np.min(g.dr)), float(np.min(g.r_c * g.dth)) if g.Nth > 1 else np.inf)
+    v = float(np.max(np.abs(d["uz"]))) / eps if d["uz"].size else 0.0
+    v = max(v, cfg.feed.velocity / eps)
+    K = eps ** 3 * dp ** 2 / (150.0 * (1.0 - eps) ** 2)
+    D_P = K * float(np.max(P)) / (model.eps_t * 1.8e-5)
+    lim = [0.9 * dx_min / max(v, 1e-12), 0.5 * dx_min ** 2 / 1e-4,
+           0.5 * dx_min ** 2 * model.rho_b * cfg.sorbent.cp_solid / 0.3, 0.5 * dx_min ** 2 / D_P,
+           1.0 / max(cfg.kinetics.k_ldf_co2, cfg.kinetics.k_ldf_h2o)]
+    return safety * min(lim)
+
+
+def integrate_rk4(model, y0, t_end, dt):
+    """Classical RK4 with accumulators (restates core/ode_solver.py:19-43)."""
+    n = int(np.ceil(t_end / dt))
+    dt = t_end / n
+    y = y0.copy()
+    acc = np.zeros(model.n_acc)
+    t = 0.0
+    for _ in range(n):
+        k1, a1 = model.rhs(t, y)
+        k2, a2 = model.rhs(t + 0.5 * dt, y + 0.5 * dt * k1)
+        k3, a3 = model.rhs(t + 0.5 * dt, y + 0.5 * dt * k2)
+        k4, a4 = model.rhs(t + dt, y + dt * k3)
+        y = y + dt / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+        acc += dt / 6.0 * (a1 + 2 * a2 + 2 * a3 + a4)
+        t += dt
+    return y, acc, t, n

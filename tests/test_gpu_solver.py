@@ -1,0 +1,122 @@
+"""GPU preconditioner, Newton-Krylov stage solve and integrator vs the oracle / reference."""
+import json
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from cases import build, config0_overrides, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _sector_of(m):
+    g = m.grid
+    n = g.ncell
+    idx = np.arange(m.n_core)
+    cellpart = idx < 6 * n
+    return np.where(cellpart, ((idx % n) // g.Nz) % g.Nth, (idx - 6 * n) // g.Nz)
+
+
+@pytest.mark.parametrize("mode", ["theta_block", "full"])
+def test_preconditioner_solves_partition_system(mode):
+    """dv_precond_solve == exact sparse solve of I - dh J restricted to the partition couplings."""
+    from dac_vtsa_b200.jacobian import FDJacobian
+    from dac_vtsa_b200.model import TVSAModel
+    d = golden("jacobian_3x4x6.npz")
+    m, _ = build(TVSAModel, {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6}, 0, d["P0"])
+    jac = FDJacobian(m)
+    Jc = jac(5.0, d["y"])
+    dh = 0.3 * 7.0
+    m.precond_factor(jac.block(5.0, d["y"]), dh, mode)
+    Jc = Jc.tocoo()
+    keep = np.ones(Jc.nnz, dtype=bool)
+    if mode == "theta_block":
+        sec = _sector_of(m)
+        keep = sec[Jc.row] == sec[Jc.col]
+    Jk = sp.csc_matrix((Jc.data[keep], (Jc.row[keep], Jc.col[keep])), shape=Jc.shape)
+    M = (sp.identity(m.n_core, format="csc") - dh * Jk).tocsc()
+    b = np.random.default_rng(7).standard_normal(m.n_core) * m.atol
+    x_ref = spla.spsolve(M, b)
+    x = m.precond_solve(b)
+    assert np.abs(x - x_ref).max() <= 1e-9 * np.abs(x_ref).max()
+
+
+def test_implicit_solver_matches_rk4_on_short_transient():
+    """Reference integration test (tests/test_physics_and_numerics.py:182-200): SDIRK2 Newton-Krylov
+    on the GPU vs classical RK4 (oracle) on a 2x1x4 blowdown, 2 ms, scaled RMS error < 1."""
+    from dac_vtsa_b200 import host
+    from dac_vtsa_b200.config import load_config
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.solver import TRBDF2
+    from oracle.residual import OracleModel
+    from oracle.solver import explicit_dt, integrate_rk4
+    cfg = load_config(override_dict={"grid.Nr": 2, "grid.Ntheta": 1, "grid.Nz": 4, "solver.rtol": 1e-6,
+                                     "solver.newton_kappa": 1e-3})
+    g = host.Grid.from_config(cfg)
+    props = host.get_backend(cfg)
+    st = host.initial_state(cfg, g, props)
+    mo = OracleModel(cfg, g, props, cfg.cycle[1], st)
+    y0 = mo.pack(st)
+    t_end = 2e-3
+    y_rk = integrate_rk4(mo, y0, t_end, explicit_dt(mo, y0, safety=0.25))[0]
+    m = TVSAModel(cfg, g, props, cfg.cycle[1], st)
+    res = TRBDF2(m, cfg, h_max=t_end, h_init=1e-6).integrate(y0, t_end, np.array([t_end]))
+    sc = m.atol + 1e-4 * np.abs(y_rk)
+    err = np.sqrt(np.mean(((res.y - y_rk) / sc) ** 2))
+    assert err < 1.0, err
+
+
+def _c0_model(cls, k=0):
+    d = golden("trajectory_c0.npz")
+    over = json.loads(str(d["over"]))
+    meta = json.loads(str(d[f"s{k}_meta"]))
+    m, cfg = build(cls, over, meta["step"], d[f"s{k}_P0"], meta["T_jacket_prev"], duration=meta["duration"])
+    return d, m, cfg, meta
+
+
+def test_replay_step_end_states_within_1e8():
+    """Replay the reference's first accepted steps of the 4x4x16 adsorption: GPU and oracle solve the
+    same stage equations tightly; step-end states agree to 1e-8 relative."""
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.replay import fixed_step_run as gpu_run
+    from oracle.residual import OracleModel
+    from oracle.solver import fixed_step_run as cpu_run
+    d, m, cfg, meta = _c0_model(TVSAModel)
+    _, mo, _, _ = _c0_model(OracleModel)
+    ts = np.concatenate([[0.0], d["s0_t_accepted"]])
+    hs = np.diff(ts)[:12]
+    y0 = d["s0_y0"]
+    ys_gpu, acc_gpu = gpu_run(m, y0, hs, scheme="trbdf2")
+    ys_cpu, acc_cpu = cpu_run(mo, y0, hs, scheme="trbdf2", tol=1e-12)
+    worst = 0.0
+    for a, b in zip(ys_gpu, ys_cpu):
+        rel = np.abs(a - b) / (np.abs(b) + m.atol)
+        worst = max(worst, float(rel.max()))
+    assert worst <= 1e-8, worst
+    assert np.allclose(acc_gpu, acc_cpu, rtol=1e-8, atol=1e-20)
+
+
+def test_free_running_adsorption_matches_reference_to_tolerance():
+    """Adaptive 200 s adsorption of the 4x4x16 bed (TR-BDF2, reference defaults): the end state agrees
+    with the reference's within its own tolerance scale, and mass/energy balances close as tightly."""
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.solver import TRBDF2
+    d, m, cfg, meta = _c0_model(TVSAModel)
+    dur = meta["duration"]
+    res = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur).integrate(d["s0_y0"], dur, np.linspace(0, dur, 12))
+    y_ref = d["s0_y"]
+    sc = m.atol + cfg.solver.rtol * np.abs(y_ref)
+    err = np.sqrt(np.mean(((res.y - y_ref) / sc) ** 2))
+    assert res.t == pytest.approx(dur)
+    assert err < 5.0, err
+    # balances: inventory change == accumulated boundary flows
+    inv0, inv1 = m.inventories(d["s0_y0"]), m.inventories(res.y)
+    ai = m.acc_index
+    for s in m.species:
+        fin = sum(res.acc[ai[f"n_in_{v}_{s}"]] for v in ("V1", "V2", "V3"))
+        fout = sum(res.acc[ai[f"n_out_{v}_{s}"]] for v in ("V1", "V2", "V3"))
+        resid = (inv1[f"tot_{s}"] - inv0[f"tot_{s}"]) - (fin - fout)
+        scale = max(abs(fin), abs(fout), abs(inv0[f"tot_{s}"]), abs(inv1[f"tot_{s}"]))
+        assert abs(resid) / scale < 1e-4
