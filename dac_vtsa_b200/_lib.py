@@ -108,6 +108,9 @@ SIGNATURES = [
     ("dv_step_params_size", C.c_size_t, []),
     ("dv_last_error", C.c_char_p, []),
     ("dv_device_count", C.c_int, [C.POINTER(C.c_int)]),
+    ("dv_profile_enable", C.c_int, [I32]),
+    ("dv_profile_read", C.c_int, [I32, C.POINTER(I64), C.POINTER(I64), C.POINTER(D)]),
+    ("dv_launch_count", I64, []),
     ("dv_model_create", C.c_int, [C.POINTER(DvStepParams), P, P, P, C.POINTER(P)]),
     ("dv_model_destroy", C.c_int, [P]),
     ("dv_model_sizes", C.c_int, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)]),
@@ -164,6 +167,28 @@ def check(rc: int, what: str = ""):
     if rc == DV_ERR_UNSUPPORTED:
         raise NotImplementedError(f"{what}: {msg}")
     raise LibraryError(f"{what} failed ({rc}): {msg}")
+
+
+KERNEL_KINDS = ("residual", "matvec", "fd_jacobian", "precond_factor", "precond_apply", "vector")
+
+
+def profile_enable(on: bool = True):
+    check(load().dv_profile_enable(int(bool(on))), "dv_profile_enable")
+
+
+def profile_read():
+    """{kind: (launches, timed launches, device ms)} for the library's kernels since profile_enable."""
+    lib = load()
+    out = {}
+    for k, name in enumerate(KERNEL_KINDS):
+        a, b, ms = I64(0), I64(0), D(0.0)
+        check(lib.dv_profile_read(k, C.byref(a), C.byref(b), C.byref(ms)), "dv_profile_read")
+        out[name] = (a.value, b.value, ms.value)
+    return out
+
+
+def launch_count() -> int:
+    return int(load().dv_launch_count())
 
 
 def colour_columns(Nr: int, Nth: int, Nz: int, wall: bool = True):

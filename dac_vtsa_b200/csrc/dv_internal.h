@@ -10,6 +10,20 @@ namespace dv {
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
 
+// Launch accounting: every kernel launch of the library goes through DV_LAUNCH, which counts it per
+// kind and, when profiling is on (dv_profile_enable), brackets it with CUDA events on its stream.
+enum KernelKind { K_RESIDUAL = 0, K_MATVEC = 1, K_FDJAC = 2, K_PC_FACTOR = 3, K_PC_APPLY = 4, K_VECTOR = 5,
+                  K_NKIND = 6 };
+void prof_begin(int kind, cudaStream_t s);
+void prof_end(int kind, cudaStream_t s);
+void prof_flush();
+#define DV_LAUNCH(kind, stream, ...)      \
+    do {                                  \
+        dv::prof_begin(kind, stream);     \
+        __VA_ARGS__;                      \
+        dv::prof_end(kind, stream);       \
+    } while (0)
+
 #define DV_CUDA(call)                                      \
     do {                                                   \
         cudaError_t e_ = (call);                           \
@@ -61,6 +75,7 @@ struct dv_model {
     double* d_pc_work;              // [parts][2][nb*nb] factorisation scratch
     int* d_pc_piv;                  // [parts][nb] pivot work
     int* d_pc_info;                 // [parts] singular-pivot flags
+    int* d_err;                     // device error word (bounded waits that gave up)
     dv::Work* W;                    // Krylov / Newton workspace (allocated at creation)
     double* d_atol7;                // per-block absolute tolerances (device)
     int ncolours;                   // colours of the Jacobian pattern (counts RHS-equivalents)
@@ -78,6 +93,8 @@ int launch_matvec(dv_model* m, double t, const double* z, const double* u, const
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s);
 // linear algebra (dv_linalg.cu)
 int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s);
+int64_t precond_doubles(int nb, int nparts, int Nz);
+int64_t precond_work_doubles(int nb, int nparts, int Nz);
 // x = diag(1/sc) M^-1 diag(sc) b  (sc may be NULL: plain solve)
 int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);
 }  // namespace dv

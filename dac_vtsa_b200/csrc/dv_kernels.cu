@@ -263,12 +263,12 @@ static unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, cudaStream_t s) {
     Rec rec = make_rec(m->rl, m->d_rec);
     if (acc) {
-        k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
-                                                              nullptr, 0.0, f);
-        k_accumulators<<<1, 256, 0, s>>>(m->p, rec.bnd, rec.Qj, rec.Qa, rec.Qw, rec.Qhx, acc);
+        DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
+                                                              nullptr, 0.0, f));
+        DV_LAUNCH(dv::K_RESIDUAL, s, k_accumulators<<<1, 256, 0, s>>>(m->p, rec.bnd, rec.Qj, rec.Qa, rec.Qw, rec.Qhx, acc));
     } else {
-        k_cells<M_RHS, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
-                                                               nullptr, 0.0, f);
+        DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_RHS, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
+                                                               nullptr, 0.0, f));
     }
     m->nfev += 1;
     DV_CUDA(cudaGetLastError());
@@ -278,8 +278,8 @@ int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, c
 int launch_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known,
                           double* R, cudaStream_t s) {
     Rec rec = make_rec(m->rl, m->d_rec);
-    k_cells<M_STAGE, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, rhs_known, nullptr, nullptr,
-                                                             nullptr, gamma_h, R);
+    DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_STAGE, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, rhs_known, nullptr, nullptr,
+                                                             nullptr, gamma_h, R));
     m->nfev += 1;
     DV_CUDA(cudaGetLastError());
     return DV_OK;
@@ -287,8 +287,8 @@ int launch_stage_residual(dv_model* m, double t, const double* y, double gamma_h
 
 int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream_t s) {
     Rec rec = make_rec(m->rl, diag);
-    k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
-                                                          nullptr, 0.0, m->d_rec);   // f discarded into scratch
+    DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
+                                                          nullptr, 0.0, m->d_rec));   // f discarded into scratch
     m->nfev += 1;
     DV_CUDA(cudaGetLastError());
     return DV_OK;
@@ -297,7 +297,7 @@ int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream
 int launch_matvec(dv_model* m, double t, const double* z, const double* u, const double* sc, const double* f0,
                   double dh, const double* scal, double* out, cudaStream_t s) {
     Rec rec = make_rec(m->rl, m->d_rec);
-    k_cells<M_MATVEC, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, z, u, sc, f0, scal, dh, out);
+    DV_LAUNCH(dv::K_MATVEC, s, k_cells<M_MATVEC, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, z, u, sc, f0, scal, dh, out));
     m->nfev += 1;
     DV_CUDA(cudaGetLastError());
     return DV_OK;
@@ -305,7 +305,7 @@ int launch_matvec(dv_model* m, double t, const double* z, const double* u, const
 
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s) {
     dim3 grid(nblk(m->nc, 128), DV_NSLOT * DV_NB);
-    k_fd_jacobian<<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J);
+    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }

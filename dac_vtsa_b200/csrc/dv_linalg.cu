@@ -1,4 +1,4 @@
-// dv_linalg.cu -- preconditioner (block-pentadiagonal LU along z) and Krylov vector kernels.
+// dv_linalg.cu -- preconditioner: block-pentadiagonal LU of I - dh J along z, and its sweep.
 //
 // The reference preconditions GMRES with a SuperLU factorisation of M = I - d h J restricted to
 // theta sectors (+ the innermost rings fully coupled), core/solver.py:334-337 and
@@ -6,13 +6,16 @@
 // theta sector (mode theta_block: cells (i, j, k) for all rings i of sector j, plus the wall
 // node (j, k)) or a whole cross-section (mode full).  Inside a partition every coupling of the
 // stencil is kept: within a plane (r, and theta in full mode) and between planes k-2..k+2 (the
-// MUSCL z+-2 reach).  The partition matrix is block-pentadiagonal in z with dense nb x nb
-// blocks, factorised by block Gaussian elimination:
+// MUSCL z+-2 reach).  The partition matrix is block-pentadiagonal in z with dense nb x nb blocks
+// (row-major, leading dimension ld >= nb, zero padded), factorised by block Gaussian elimination:
 //   L2_k = A(k,k-2) Uinv_{k-2}
 //   L1_k = (A(k,k-1) - L2_k U1_{k-2}) Uinv_{k-1}
 //   D_k  = A(k,k) - L1_k U1_{k-1} - L2_k U2_{k-2},      Uinv_k = D_k^-1 (Gauss-Jordan, partial pivoting)
 //   U1_k = A(k,k+1) - L1_k U2_{k-1},                    U2_k = A(k,k+2)
-// and applied by one forward and one backward sweep along z (one CTA per partition).
+// Stored per plane k: slot 0 L2_k, slot 1 L1_k, slot 2 Uinv_k, slot 3 -Uinv_k U1_k, slot 4 -Uinv_k U2_k,
+// so that both sweeps are one fused GEMV per plane:
+//   forward  z_k = b_k - L1_k z_{k-1} - L2_k z_{k-2}
+//   backward x_k = Uinv_k z_k + (-Uinv_k U1_k) x_{k+1} + (-Uinv_k U2_k) x_{k+2}
 #include <algorithm>
 #include "dv_internal.h"
 #include "dv_physics.cuh"
@@ -20,9 +23,19 @@
 namespace dv {
 
 struct PcGeom {
-    int Nr, Nth, Nz, wall, mode, nb, nparts;
-    int64_t nc;
+    int Nr, Nth, Nz, wall, mode, nb, nparts, ld;
+    int64_t nc, bs;        // bs: block stride in doubles (nb*ld rounded up to even: 16-byte multiple)
 };
+
+#define PC_SMEM_NB 56      // largest block the shared-memory factorisation keeps resident (9 blocks)
+
+// leading dimension: nb rounded up to 8 and kept == 8 (mod 16) so the 4 rows a warp reads in the
+// sweep fall on alternating shared-memory bank halves
+static inline int pc_ld(int nb) {
+    int ld = (nb + 7) / 8 * 8;
+    if (ld % 16 == 0) ld += 8;
+    return ld;
+}
 
 static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int k, int l) {
     const int64_t offw = (int64_t)DV_NV * g.nc;
@@ -40,14 +53,22 @@ static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int
     return offw + (int64_t)(l - DV_NV * g.Nr * g.Nth) * g.Nz + k;
 }
 
-// local index of (cell (i, j), var v) / wall (j) inside its partition; part of column j
+// local index of (cell (i, j), var v) / wall (j) inside its partition
 static __device__ __forceinline__ int pc_local(const PcGeom& g, int i, int j, int v) {
     if (g.mode == 0) return (v < DV_NV) ? i * DV_NV + v : DV_NV * g.Nr;
     return (v < DV_NV) ? (i * g.Nth + j) * DV_NV + v : DV_NV * g.Nr * g.Nth + j;
 }
 
+// The z-couplings A(k, k+-1), A(k, k+-2) only connect a cell to itself in another plane: they are
+// block diagonal with 6x6 cell blocks (and 1x1 wall entries).  First index / size of the block of l:
+static __device__ __forceinline__ void pc_cellblock(const PcGeom& g, int l, int& b0, int& bsz) {
+    const int ncv = (g.mode == 0) ? DV_NV * g.Nr : DV_NV * g.Nr * g.Nth;
+    if (l < ncv) { b0 = (l / DV_NV) * DV_NV; bsz = DV_NV; }
+    else { b0 = l; bsz = 1; }
+}
+
 // ---------------------------------------------------------------- assembly of I - dh J
-// blocks: [part][Nz][5][nb*nb] column-major, slot d+2 holds A(k, k+d).
+// blocks: [part][Nz][5][bs] row-major (B[row*ld + col]); slot d+2 holds A(k, k+d).
 __global__ void k_pc_zero(double* __restrict__ A, int64_t n) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
         A[q] = 0.0;
@@ -76,8 +97,7 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
     if (!ok) return;
     const int part = (g.mode == 0) ? j : 0;
     const int d = nk - k;
-    const int nb = g.nb;
-    double* B = A + (((int64_t)part * g.Nz + k) * 5 + (d + 2)) * (int64_t)nb * nb;
+    double* B = A + (((int64_t)part * g.Nz + k) * 5 + (d + 2)) * g.bs;
     const bool row_wall_ok = g.wall && i == g.Nr - 1;
     const bool col_wall_ok = g.wall && ni == g.Nr - 1;
     for (int rv = 0; rv < DV_NB; ++rv) {
@@ -89,44 +109,273 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
             const double jv = J[((int64_t)(slot * DV_NB + rv) * DV_NB + cv) * g.nc + c];
             double val = -dh * jv;
             if (slot == 0 && rv == cv) val += 1.0;
-            B[(int64_t)lc * nb + lr] = val;
+            B[(int64_t)lr * g.ld + lc] = val;
         }
     }
 }
 
-// ---------------------------------------------------------------- CTA-level dense kernels
-// C = beta C + alpha A B  (nb x nb, column-major, generic pointers); 256 threads, 32x32 tiles.
-static __device__ void cta_gemm(int nb, double alpha, const double* A, const double* B, double beta, double* C,
-                                double* shA, double* shB) {
+// ---------------------------------------------------------------- shared-memory dense kernels (row-major)
+// 256 threads as a 16 x 16 grid; thread (ty, tx) owns rows ty + 16a and columns tx + 16b (a, b < 4),
+// i.e. a 4 x 4 register tile of any nb <= 64 matrix.  No integer division in the inner loops.
+#define SM_T 16
+#define SM_R 4
+
+// C = beta C + alpha A B (all row-major in shared memory, leading dimension ld, nb <= 64)
+static __device__ void sm_gemm(int nb, int ld, double alpha, const double* A, const double* B, double beta,
+                               double* C) {
+    const int tx = threadIdx.x % SM_T, ty = threadIdx.x / SM_T;
+    double acc[SM_R][SM_R];
+#pragma unroll
+    for (int a = 0; a < SM_R; ++a)
+#pragma unroll
+        for (int b = 0; b < SM_R; ++b) acc[a][b] = 0.0;
+    for (int q = 0; q < nb; ++q) {
+        double av[SM_R], bv[SM_R];
+#pragma unroll
+        for (int a = 0; a < SM_R; ++a) {
+            const int r = ty + SM_T * a;
+            av[a] = (r < nb) ? A[r * ld + q] : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < SM_R; ++b) {
+            const int c = tx + SM_T * b;
+            bv[b] = (c < nb) ? B[q * ld + c] : 0.0;
+        }
+#pragma unroll
+        for (int a = 0; a < SM_R; ++a)
+#pragma unroll
+            for (int b = 0; b < SM_R; ++b) acc[a][b] += av[a] * bv[b];
+    }
+#pragma unroll
+    for (int a = 0; a < SM_R; ++a) {
+        const int r = ty + SM_T * a;
+        if (r >= nb) continue;
+#pragma unroll
+        for (int b = 0; b < SM_R; ++b) {
+            const int c = tx + SM_T * b;
+            if (c >= nb) continue;
+            double* cp = C + r * ld + c;
+            *cp = (beta == 0.0) ? alpha * acc[a][b] : beta * (*cp) + alpha * acc[a][b];
+        }
+    }
+    __syncthreads();
+}
+
+// C = beta C + alpha Bd X with Bd block diagonal (cell blocks) in shared memory.
+static __device__ void sm_bd_left(const PcGeom& g, double alpha, const double* Bd, const double* X, double beta,
+                                  double* C) {
+    const int nb = g.nb, ld = g.ld;
+    const int tx = threadIdx.x % SM_T, ty = threadIdx.x / SM_T;
+#pragma unroll
+    for (int a = 0; a < SM_R; ++a) {
+        const int r = ty + SM_T * a;
+        if (r >= nb) continue;
+        int b0, bsz;
+        pc_cellblock(g, r, b0, bsz);
+#pragma unroll
+        for (int b = 0; b < SM_R; ++b) {
+            const int c = tx + SM_T * b;
+            if (c >= nb) continue;
+            double acc = 0.0;
+            for (int q = b0; q < b0 + bsz; ++q) acc += Bd[r * ld + q] * X[q * ld + c];
+            double* cp = C + r * ld + c;
+            *cp = (beta == 0.0) ? alpha * acc : beta * (*cp) + alpha * acc;
+        }
+    }
+    __syncthreads();
+}
+
+// C = beta C + alpha X Bd with Bd block diagonal (any memory space).
+static __device__ void sm_bd_right(const PcGeom& g, double alpha, const double* X, const double* Bd, double beta,
+                                   double* C) {
+    const int nb = g.nb, ld = g.ld;
+    const int tx = threadIdx.x % SM_T, ty = threadIdx.x / SM_T;
+#pragma unroll
+    for (int b = 0; b < SM_R; ++b) {
+        const int c = tx + SM_T * b;
+        if (c >= nb) continue;
+        int b0, bsz;
+        pc_cellblock(g, c, b0, bsz);
+#pragma unroll
+        for (int a = 0; a < SM_R; ++a) {
+            const int r = ty + SM_T * a;
+            if (r >= nb) continue;
+            double acc = 0.0;
+            for (int q = b0; q < b0 + bsz; ++q) acc += X[r * ld + q] * Bd[q * ld + c];
+            double* cp = C + r * ld + c;
+            *cp = (beta == 0.0) ? alpha * acc : beta * (*cp) + alpha * acc;
+        }
+    }
+    __syncthreads();
+}
+
+// In-place Gauss-Jordan inverse (row-major, nb <= 64) with partial pivoting; returns 1 on a zero /
+// non-finite pivot (replaced by 1 so the factors stay finite; reported through the info flag).
+static __device__ int sm_inverse(int nb, int ld, double* A, int* perm, double* fcol, double* prow, int* sp) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tx = tid % SM_T, ty = tid / SM_T;
+    int bad = 0;
+    for (int k = 0; k < nb; ++k) {
+        if (warp == 0) {                          // pivot row: largest |A[i][k]|, i >= k
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + lane; i < nb; i += 32) {
+                double v = fabs(A[i * ld + k]);
+                if (v > best) { best = v; bi = i; }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                double ov = __shfl_down_sync(0xffffffffu, best, off);
+                int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) { sp[0] = bi; perm[k] = bi; }
+        }
+        __syncthreads();
+        const int p = sp[0];
+        double piv = A[p * ld + k];
+        if (!(fabs(piv) > 0.0) || !isfinite(piv)) { bad = 1; piv = 1.0; }
+        const double inv = 1.0 / piv;
+        if (tid < nb) {                           // scaled pivot row and old column k (rows k, p exchanged)
+            const int c = tid;
+            prow[c] = ((c == k) ? 1.0 : A[p * ld + c]) * inv;
+            const int i = tid;
+            const int src = (i == k) ? p : ((i == p) ? k : i);
+            fcol[i] = (i == k) ? 0.0 : A[src * ld + k];
+        }
+        __syncthreads();
+        double keep[SM_R][SM_R];
+#pragma unroll
+        for (int a = 0; a < SM_R; ++a) {
+            const int i = ty + SM_T * a;
+            if (i >= nb) continue;
+            const int src = (i == k) ? p : ((i == p) ? k : i);
+#pragma unroll
+            for (int b = 0; b < SM_R; ++b) {
+                const int c = tx + SM_T * b;
+                if (c >= nb) continue;
+                if (i == k) keep[a][b] = prow[c];
+                else keep[a][b] = ((c == k) ? 0.0 : A[src * ld + c]) - fcol[i] * prow[c];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < SM_R; ++a) {
+            const int i = ty + SM_T * a;
+            if (i >= nb) continue;
+#pragma unroll
+            for (int b = 0; b < SM_R; ++b) {
+                const int c = tx + SM_T * b;
+                if (c < nb) A[i * ld + c] = keep[a][b];
+            }
+        }
+        __syncthreads();
+    }
+    for (int k = nb - 1; k >= 0; --k) {           // undo the row interchanges as column interchanges
+        const int p = perm[k];
+        if (p != k && tid < nb) {
+            double t = A[tid * ld + k];
+            A[tid * ld + k] = A[tid * ld + p];
+            A[tid * ld + p] = t;
+        }
+        __syncthreads();
+    }
+    return bad;
+}
+
+static __device__ void cp_block(int64_t n, const double* src, double* dst) {
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[q];
+}
+
+// One CTA per partition, every working block resident in shared memory (nb <= PC_SMEM_NB).
+__global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom g, double* __restrict__ A, int* __restrict__ info) {
+    extern __shared__ __align__(16) double dsm[];
+    __shared__ int perm[64];
+    __shared__ double fcol[64], prow[64];
+    __shared__ int sp[1];
+    const int nb = g.nb, ld = g.ld;
+    const int n2 = nb * ld;
+    double* buf[9];
+    for (int q = 0; q < 9; ++q) buf[q] = dsm + (int64_t)q * n2;
+    double *S0 = buf[0], *S1 = buf[1], *S2 = buf[2], *S3 = buf[3], *T = buf[4];
+    double *Ui1 = buf[5], *Ui2 = buf[6], *U11 = buf[7], *U12 = buf[8];
+    for (int64_t q = threadIdx.x; q < 9 * (int64_t)n2; q += blockDim.x) dsm[q] = 0.0;   // zero padding columns
+    __syncthreads();
+    double* base = A + (int64_t)blockIdx.x * g.Nz * 5 * g.bs;
+    int bad = 0;
+    for (int k = 0; k < g.Nz; ++k) {
+        double* Ak = base + (int64_t)k * 5 * g.bs;
+        if (k >= 2) cp_block(n2, Ak, S0);
+        if (k >= 1) cp_block(n2, Ak + g.bs, S1);
+        cp_block(n2, Ak + 2 * g.bs, S2);
+        cp_block(n2, Ak + 3 * g.bs, S3);
+        __syncthreads();
+        if (k >= 2) {
+            double* U2_2 = base + ((int64_t)(k - 2) * 5 + 4) * g.bs;        // A(k-2, k), block diagonal
+            sm_bd_left(g, 1.0, S0, Ui2, 0.0, T);                               // L2 = A(k,k-2) Uinv_{k-2}
+            double* t = S0; S0 = T; T = t;
+            sm_gemm(nb, ld, -1.0, S0, U12, 1.0, S1);                           // A(k,k-1) -= L2 U1_{k-2}
+            sm_bd_right(g, -1.0, S0, U2_2, 1.0, S2);                           // D -= L2 U2_{k-2}
+            sm_bd_right(g, -1.0, Ui2, U2_2, 0.0, T);                           // -Uinv_{k-2} U2_{k-2}
+            cp_block(n2, T, U2_2);                                             // (U2_{k-2} is not needed again)
+            __syncthreads();
+        }
+        if (k >= 1) {
+            const double* U2_1 = base + ((int64_t)(k - 1) * 5 + 4) * g.bs;   // A(k-1, k+1), block diagonal
+            if (k == 1) sm_bd_left(g, 1.0, S1, Ui1, 0.0, T);                  // L1 = A(1,0) Uinv_0
+            else sm_gemm(nb, ld, 1.0, S1, Ui1, 0.0, T);                        // L1 = (...) Uinv_{k-1}
+            double* t = S1; S1 = T; T = t;
+            sm_gemm(nb, ld, -1.0, S1, U11, 1.0, S2);                           // D -= L1 U1_{k-1}
+            sm_bd_right(g, -1.0, S1, U2_1, 1.0, S3);                           // U1 = A(k,k+1) - L1 U2_{k-1}
+        }
+        bad |= sm_inverse(nb, ld, S2, perm, fcol, prow, sp);
+        sm_gemm(nb, ld, -1.0, S2, S3, 0.0, T);                                 // -Uinv_k U1_k
+        if (k >= 2) cp_block(n2, S0, Ak);
+        if (k >= 1) cp_block(n2, S1, Ak + g.bs);
+        cp_block(n2, S2, Ak + 2 * g.bs);
+        cp_block(n2, T, Ak + 3 * g.bs);
+        __syncthreads();
+        // rotate: Uinv_{k-2} <- Uinv_{k-1} <- Uinv_k ; U1 likewise; freed blocks become S2 / S3
+        double* fi = Ui2; Ui2 = Ui1; Ui1 = S2; S2 = fi;
+        double* fu = U12; U12 = U11; U11 = S3; S3 = fu;
+    }
+    // slot 4 of the last two planes: U2_k = A(k, k+2) = 0 for k >= Nz-2 (zeroed at assembly)
+    if (threadIdx.x == 0) info[blockIdx.x] = bad;
+}
+
+// ---------------------------------------------------------------- global-memory fallback (large blocks)
+// C = beta C + alpha A B, row-major (leading dimension ld) in global memory; 256 threads, 32x32 tiles.
+static __device__ void cta_gemm(int nb, int ld, double alpha, const double* A, const double* B, double beta,
+                                double* C, double* shA, double* shB) {
     const int tid = threadIdx.x;
-    const int tr = tid % 32, tc4 = (tid / 32) * 4;
+    const int tc = tid % 32, tr4 = (tid / 32) * 4;
     for (int ti = 0; ti < nb; ti += 32) {
         for (int tj = 0; tj < nb; tj += 32) {
             double acc[4] = {0.0, 0.0, 0.0, 0.0};
             for (int kk = 0; kk < nb; kk += 32) {
                 for (int q = tid; q < 1024; q += blockDim.x) {
-                    int r = q % 32, cc = q / 32;
+                    int r = q / 32, cc = q % 32;
                     int gr = ti + r, gk = kk + cc;
-                    shA[cc * 32 + r] = (gr < nb && gk < nb) ? A[(int64_t)gk * nb + gr] : 0.0;
+                    shA[r * 32 + cc] = (gr < nb && gk < nb) ? A[(int64_t)gr * ld + gk] : 0.0;
                     int gk2 = kk + r, gc = tj + cc;
-                    shB[cc * 32 + r] = (gk2 < nb && gc < nb) ? B[(int64_t)gc * nb + gk2] : 0.0;
+                    shB[r * 32 + cc] = (gk2 < nb && gc < nb) ? B[(int64_t)gk2 * ld + gc] : 0.0;
                 }
                 __syncthreads();
 #pragma unroll 8
                 for (int q = 0; q < 32; ++q) {
-                    double a = shA[q * 32 + tr];
+                    double b = shB[q * 32 + tc];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) acc[u] += a * shB[(tc4 + u) * 32 + q];
+                    for (int u = 0; u < 4; ++u) acc[u] += shA[(tr4 + u) * 32 + q] * b;
                 }
                 __syncthreads();
             }
-            const int gr = ti + tr;
-            if (gr < nb) {
+            const int gc = tj + tc;
+            if (gc < nb) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
-                    int gc = tj + tc4 + u;
-                    if (gc < nb) {
-                        double* cp = C + (int64_t)gc * nb + gr;
+                    int gr = ti + tr4 + u;
+                    if (gr < nb) {
+                        double* cp = C + (int64_t)gr * ld + gc;
                         *cp = (beta == 0.0) ? alpha * acc[u] : beta * (*cp) + alpha * acc[u];
                     }
                 }
@@ -141,19 +390,20 @@ static __device__ void cta_copy(int64_t n, const double* src, double* dst) {
     __syncthreads();
 }
 
-// In-place inverse of D (nb x nb, column-major) using W (nb x 2nb scratch).  Returns 1 if a zero /
-// non-finite pivot was met (the pivot is then replaced by 1 so the factorisation stays finite).
-static __device__ int cta_inverse(int nb, double* D, double* W, double* red_v, int* red_i) {
+// Gauss-Jordan inverse of the row-major D (leading dimension ld) through an augmented scratch W
+// (nb x 2nb, column-major over the augmented matrix).  Reading D column-major inverts D^T; the
+// inverse of the transpose is the transpose of the inverse, so writing back the same way yields
+// the row-major inverse.
+static __device__ int cta_inverse(int nb, int ld, double* D, double* W, double* red_v, int* red_i) {
     const int tid = threadIdx.x;
     const int64_t n2 = (int64_t)nb * nb;
     for (int64_t q = tid; q < 2 * n2; q += blockDim.x) {
         int64_t col = q / nb, row = q % nb;
-        W[q] = (col < nb) ? D[q] : ((col - nb) == row ? 1.0 : 0.0);
+        W[q] = (col < nb) ? D[col * ld + row] : ((col - nb) == row ? 1.0 : 0.0);
     }
     __syncthreads();
     int bad = 0;
     for (int pc = 0; pc < nb; ++pc) {
-        // pivot search (rows pc..nb-1 of column pc)
         double best = -1.0;
         int bi = pc;
         for (int r = pc + tid; r < nb; r += blockDim.x) {
@@ -201,143 +451,260 @@ static __device__ int cta_inverse(int nb, double* D, double* W, double* red_v, i
         }
         __syncthreads();
     }
-    for (int64_t q = tid; q < n2; q += blockDim.x) D[q] = W[n2 + q];
+    for (int64_t q = tid; q < n2; q += blockDim.x) {
+        int64_t col = q / nb, row = q % nb;
+        D[col * ld + row] = W[n2 + q];
+    }
     __syncthreads();
     return bad;
 }
 
-// One CTA per partition: sequential block elimination along z.
-__global__ void __launch_bounds__(256) k_pc_factor(PcGeom g, double* __restrict__ A, double* __restrict__ work,
-                                                   int* __restrict__ info, int use_smem) {
+__global__ void __launch_bounds__(256) k_pc_factor_glob(PcGeom g, double* __restrict__ A, double* __restrict__ work,
+                                                        int* __restrict__ info, int use_smem) {
     extern __shared__ double dsm[];
     __shared__ double shA[1024], shB[1024];
     __shared__ double red_v[256];
     __shared__ int red_i[256];
     const int part = blockIdx.x;
-    const int nb = g.nb;
-    const int64_t n2 = (int64_t)nb * nb;
-    double* base = A + (int64_t)part * g.Nz * 5 * n2;
-    double* T = work + (int64_t)part * 4 * n2;          // temp block
-    double* W = use_smem ? dsm : (T + n2);             // 2*n2 Gauss-Jordan scratch
+    const int nb = g.nb, ld = g.ld;
+    const int64_t n2 = (int64_t)nb * ld;
+    const int64_t bs = g.bs;
+    double* base = A + (int64_t)part * g.Nz * 5 * bs;
+    double* T = work + (int64_t)part * 4 * n2;
+    double* W = use_smem ? dsm : (T + n2);
     int bad = 0;
     for (int k = 0; k < g.Nz; ++k) {
-        double* Ak = base + (int64_t)k * 5 * n2;
+        double* Ak = base + (int64_t)k * 5 * bs;
         double* Am2 = Ak;
-        double* Am1 = Ak + n2;
-        double* A0 = Ak + 2 * n2;
-        double* Ap1 = Ak + 3 * n2;
-        double* Uinv_1 = (k >= 1) ? base + ((int64_t)(k - 1) * 5 + 2) * n2 : nullptr;
-        double* U1_1 = (k >= 1) ? base + ((int64_t)(k - 1) * 5 + 3) * n2 : nullptr;
-        double* U2_1 = (k >= 1) ? base + ((int64_t)(k - 1) * 5 + 4) * n2 : nullptr;
-        double* Uinv_2 = (k >= 2) ? base + ((int64_t)(k - 2) * 5 + 2) * n2 : nullptr;
-        double* U1_2 = (k >= 2) ? base + ((int64_t)(k - 2) * 5 + 3) * n2 : nullptr;
-        double* U2_2 = (k >= 2) ? base + ((int64_t)(k - 2) * 5 + 4) * n2 : nullptr;
-        if (k >= 2) {                                   // L2 = A(k,k-2) Uinv_{k-2}
-            cta_gemm(nb, 1.0, Am2, Uinv_2, 0.0, T, shA, shB);
+        double* Am1 = Ak + bs;
+        double* A0 = Ak + 2 * bs;
+        double* Ap1 = Ak + 3 * bs;
+        double* Uinv_1 = (k >= 1) ? base + ((int64_t)(k - 1) * 5 + 2) * bs : nullptr;
+        double* U1_1 = (k >= 1) ? base + ((int64_t)(k - 1) * 5 + 3) * bs : nullptr;
+        double* U2_1 = (k >= 1) ? base + ((int64_t)(k - 1) * 5 + 4) * bs : nullptr;
+        double* Uinv_2 = (k >= 2) ? base + ((int64_t)(k - 2) * 5 + 2) * bs : nullptr;
+        double* U1_2 = (k >= 2) ? base + ((int64_t)(k - 2) * 5 + 3) * bs : nullptr;
+        double* U2_2 = (k >= 2) ? base + ((int64_t)(k - 2) * 5 + 4) * bs : nullptr;
+        if (k >= 2) {
+            cta_gemm(nb, ld, 1.0, Am2, Uinv_2, 0.0, T, shA, shB);
             cta_copy(n2, T, Am2);
-            cta_gemm(nb, -1.0, Am2, U1_2, 1.0, Am1, shA, shB);   // A(k,k-1) -= L2 U1_{k-2}
-            cta_gemm(nb, -1.0, Am2, U2_2, 1.0, A0, shA, shB);    // D -= L2 U2_{k-2}
+            cta_gemm(nb, ld, -1.0, Am2, U1_2, 1.0, Am1, shA, shB);
+            cta_gemm(nb, ld, -1.0, Am2, U2_2, 1.0, A0, shA, shB);
         }
-        if (k >= 1) {                                   // L1 = (...) Uinv_{k-1}
-            cta_gemm(nb, 1.0, Am1, Uinv_1, 0.0, T, shA, shB);
+        if (k >= 1) {
+            cta_gemm(nb, ld, 1.0, Am1, Uinv_1, 0.0, T, shA, shB);
             cta_copy(n2, T, Am1);
-            cta_gemm(nb, -1.0, Am1, U1_1, 1.0, A0, shA, shB);    // D -= L1 U1_{k-1}
-            cta_gemm(nb, -1.0, Am1, U2_1, 1.0, Ap1, shA, shB);   // U1 = A(k,k+1) - L1 U2_{k-1}
+            cta_gemm(nb, ld, -1.0, Am1, U1_1, 1.0, A0, shA, shB);
+            cta_gemm(nb, ld, -1.0, Am1, U2_1, 1.0, Ap1, shA, shB);
         }
-        bad |= cta_inverse(nb, A0, W, red_v, red_i);
+        bad |= cta_inverse(nb, ld, A0, W, red_v, red_i);
+    }
+    // fused-sweep form: slot 3 <- -Uinv_k U1_k, slot 4 <- -Uinv_k U2_k
+    for (int k = 0; k < g.Nz; ++k) {
+        double* Ak = base + (int64_t)k * 5 * bs;
+        for (int slot = 3; slot <= 4; ++slot) {
+            cta_gemm(nb, ld, -1.0, Ak + 2 * bs, Ak + slot * bs, 0.0, T, shA, shB);
+            cta_copy(n2, T, Ak + slot * bs);
+        }
     }
     if (threadIdx.x == 0) info[part] = bad;
 }
 
-// x = diag(1/sc) M^-1 diag(sc) b  for all partitions (one CTA each, 256 threads, 4 threads per row).
-__global__ void __launch_bounds__(256) k_pc_apply(PcGeom g, const double* __restrict__ A, const double* __restrict__ b,
-                                                  const double* __restrict__ sc, double* __restrict__ x) {
-    extern __shared__ double xs[];                  // [Nz][nb]
+// ---------------------------------------------------------------- sweeps
+static __device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+static __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+static __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+static __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+// bounded wait: false after ~2^22 polls (each poll may itself suspend briefly)
+static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+// x = diag(1/sc) M^-1 diag(sc) b for all partitions: one CTA (512 threads, 8 lanes per row) per
+// partition.  The factor blocks of the next plane stream into a second shared buffer (cp.async.bulk
+// with an mbarrier) while the current plane is swept.  NJ = ld / 8: each lane's columns lane + 8j,
+// j < NJ, are a fixed, fully unrolled batch of loads (padding columns hold zeros).
+#define PA_THREADS 512
+#define PA_LANES 8
+template <int NJ>
+__global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom g, const double* __restrict__ A,
+                                                         const double* __restrict__ b, const double* __restrict__ sc,
+                                                         double* __restrict__ x, int* __restrict__ err) {
+    extern __shared__ __align__(128) double dsm[];
+    __shared__ __align__(8) uint64_t bars[2];
+    constexpr int LD = NJ * PA_LANES;
     const int part = blockIdx.x;
     const int nb = g.nb;
-    const int64_t n2 = (int64_t)nb * nb;
-    const double* base = A + (int64_t)part * g.Nz * 5 * n2;
     const int tid = threadIdx.x;
-    const int lane4 = tid & 3;
-    const int rows_per_pass = blockDim.x / 4;
-    for (int64_t q = tid; q < (int64_t)g.Nz * nb; q += blockDim.x) {
-        int k = (int)(q / nb), l = (int)(q % nb);
-        int64_t gi = pc_glob(g, part, k, l);
-        xs[q] = sc ? b[gi] * sc[gi] : b[gi];
+    const int64_t bs = g.bs;
+    double* xs = dsm;                          // [Nz][LD]: b, then z, then x (padding zero)
+    double* tv = xs + (int64_t)g.Nz * LD;      // [LD]
+    double* buf0 = tv + LD;                    // [3 bs]
+    double* buf1 = buf0 + 3 * bs;
+    const double* base = A + (int64_t)part * g.Nz * 5 * bs;
+    const int S = 2 * g.Nz - 1;                // stages: forward 1..Nz-1, backward Nz-1..0
+    auto stage_src = [&](int s) -> const double* {
+        if (s < g.Nz - 1) return base + (int64_t)(s + 1) * 5 * bs;
+        const int k = g.Nz - 1 - (s - (g.Nz - 1));
+        return base + ((int64_t)k * 5 + 2) * bs;
+    };
+    auto stage_bytes = [&](int s) -> uint32_t {
+        return (uint32_t)(((s < g.Nz - 1) ? 2 : 3) * bs * sizeof(double));
+    };
+    if (tid == 0) {
+        mbar_init(smem_u32(&bars[0]), 1);
+        mbar_init(smem_u32(&bars[1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    // forward: z_k = b_k - L1_k z_{k-1} - L2_k z_{k-2}
-    for (int k = 1; k < g.Nz; ++k) {
-        const double* L1 = base + ((int64_t)k * 5 + 1) * n2;
-        const double* L2 = base + ((int64_t)k * 5 + 0) * n2;
-        const double* z1 = xs + (int64_t)(k - 1) * nb;
-        const double* z2 = (k >= 2) ? xs + (int64_t)(k - 2) * nb : nullptr;
-        for (int r0 = 0; r0 < nb; r0 += rows_per_pass) {
-            int r = r0 + tid / 4;
-            double acc = 0.0;
-            if (r < nb) {
-                for (int c = lane4; c < nb; c += 4) {
-                    acc += L1[(int64_t)c * nb + r] * z1[c];
-                    if (z2) acc += L2[(int64_t)c * nb + r] * z2[c];
+    if (tid == 0) {
+        bulk_load(smem_u32(buf0), stage_src(0), stage_bytes(0), smem_u32(&bars[0]));
+        if (S > 1) bulk_load(smem_u32(buf1), stage_src(1), stage_bytes(1), smem_u32(&bars[1]));
+    }
+    for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
+        const int k = q / LD, l = q - k * LD;
+        double v = 0.0;
+        if (l < nb) {
+            const int64_t gi = pc_glob(g, part, k, l);
+            v = sc ? b[gi] * sc[gi] : b[gi];
+        }
+        xs[q] = v;
+    }
+    if (tid < LD) tv[tid] = 0.0;
+    __syncthreads();
+    const int lane = tid % PA_LANES;
+    const int r = tid / PA_LANES;              // one row per 8 lanes: 64 rows (nb <= 64)
+    bool ok = true;
+    for (int s = 0; s < S; ++s) {
+        const int bi = s & 1;
+        const double* buf = bi ? buf1 : buf0;
+        const bool arrived = mbar_wait(smem_u32(&bars[bi]), (uint32_t)((s >> 1) & 1));
+        if (!__syncthreads_and(arrived)) {       // uniform decision: no thread is left at a barrier
+            ok = false;
+            if (tid == 0) atomicOr(err, 1);
+            break;
+        }
+        const bool fwd = s < g.Nz - 1;
+        const int k = fwd ? s + 1 : g.Nz - 1 - (s - (g.Nz - 1));
+        double acc = 0.0;
+        if (r < nb) {
+            if (fwd) {                           // [L1 | L2] . [z_{k-1} ; z_{k-2}]
+                const double* m1 = buf + bs + r * LD;
+                const double* v1 = xs + (int64_t)(k - 1) * LD;
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) acc += m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
+                if (k >= 2) {
+                    const double* m2 = buf + r * LD;
+                    const double* v2 = xs + (int64_t)(k - 2) * LD;
+#pragma unroll
+                    for (int j = 0; j < NJ; ++j) acc += m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
+                }
+            } else {                             // [Uinv | -W1 | -W2] . [z_k ; x_{k+1} ; x_{k+2}]
+                const double* m0 = buf + r * LD;
+                const double* v0 = xs + (int64_t)k * LD;
+#pragma unroll
+                for (int j = 0; j < NJ; ++j) acc += m0[lane + PA_LANES * j] * v0[lane + PA_LANES * j];
+                if (k + 1 < g.Nz) {
+                    const double* m1 = buf + bs + r * LD;
+                    const double* v1 = xs + (int64_t)(k + 1) * LD;
+#pragma unroll
+                    for (int j = 0; j < NJ; ++j) acc += m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
+                }
+                if (k + 2 < g.Nz) {
+                    const double* m2 = buf + 2 * bs + r * LD;
+                    const double* v2 = xs + (int64_t)(k + 2) * LD;
+#pragma unroll
+                    for (int j = 0; j < NJ; ++j) acc += m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
                 }
             }
-            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-            acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-            if (r < nb && lane4 == 0) xs[(int64_t)k * nb + r] -= acc;
+        }
+#pragma unroll
+        for (int off = PA_LANES / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, PA_LANES);
+        if (r < nb && lane == 0) tv[r] = fwd ? xs[(int64_t)k * LD + r] - acc : acc;
+        __syncthreads();                         // every thread is done with `buf` and with xs reads
+        if (tid < nb) xs[(int64_t)k * LD + tid] = tv[tid];
+        if (tid == 0 && s + 2 < S) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bulk_load(smem_u32(buf), stage_src(s + 2), stage_bytes(s + 2), smem_u32(&bars[bi]));
         }
         __syncthreads();
     }
-    // backward: x_k = Uinv_k (z_k - U1_k x_{k+1} - U2_k x_{k+2}); tmp held in registers then written
-    for (int k = g.Nz - 1; k >= 0; --k) {
-        const double* Ui = base + ((int64_t)k * 5 + 2) * n2;
-        const double* U1 = base + ((int64_t)k * 5 + 3) * n2;
-        const double* U2 = base + ((int64_t)k * 5 + 4) * n2;
-        const double* x1 = (k + 1 < g.Nz) ? xs + (int64_t)(k + 1) * nb : nullptr;
-        const double* x2 = (k + 2 < g.Nz) ? xs + (int64_t)(k + 2) * nb : nullptr;
-        double* zk = xs + (int64_t)k * nb;
-        if (x1) {
-            for (int r0 = 0; r0 < nb; r0 += rows_per_pass) {
-                int r = r0 + tid / 4;
-                double acc = 0.0;
-                if (r < nb) {
-                    for (int c = lane4; c < nb; c += 4) {
-                        acc += U1[(int64_t)c * nb + r] * x1[c];
-                        if (x2) acc += U2[(int64_t)c * nb + r] * x2[c];
-                    }
-                }
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                __syncthreads();
-                if (r < nb && lane4 == 0) zk[r] -= acc;
-            }
-            __syncthreads();
+    if (!ok) {                                   // drain copies still in flight (bounded) and leave x untouched
+        if (tid == 0) {
+            mbar_wait(smem_u32(&bars[0]), 0);
+            mbar_wait(smem_u32(&bars[1]), 0);
         }
-        // x_k = Uinv_k zk  (rows computed into registers, written after a barrier)
-        double outv[8];
-        int nout = 0;
-        for (int r0 = 0; r0 < nb; r0 += rows_per_pass) {
-            int r = r0 + tid / 4;
+        return;
+    }
+    for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
+        const int k = q / LD, l = q - k * LD;
+        if (l < nb) {
+            const int64_t gi = pc_glob(g, part, k, l);
+            x[gi] = sc ? xs[q] / sc[gi] : xs[q];
+        }
+    }
+}
+
+// Sweep for partitions too large for the shared-memory pipeline: same fused stages, operands read
+// from global memory (L2).
+__global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom g, const double* __restrict__ A,
+                                                       const double* __restrict__ b, const double* __restrict__ sc,
+                                                       double* __restrict__ x, double* __restrict__ xs_all) {
+    __shared__ double tv[512];
+    const int part = blockIdx.x;
+    const int nb = g.nb, ld = g.ld;
+    const int tid = threadIdx.x;
+    const int64_t bs = g.bs;
+    double* xs = xs_all + (int64_t)part * g.Nz * ld;
+    const double* base = A + (int64_t)part * g.Nz * 5 * bs;
+    for (int64_t q = tid; q < (int64_t)g.Nz * nb; q += blockDim.x) {
+        int k = (int)(q / nb), l = (int)(q % nb);
+        int64_t gi = pc_glob(g, part, k, l);
+        xs[(int64_t)k * ld + l] = sc ? b[gi] * sc[gi] : b[gi];
+    }
+    __syncthreads();
+    const int S = 2 * g.Nz - 1;
+    for (int s = 0; s < S; ++s) {
+        const bool fwd = s < g.Nz - 1;
+        const int k = fwd ? s + 1 : g.Nz - 1 - (s - (g.Nz - 1));
+        const double* Ak = base + (int64_t)k * 5 * bs;
+        const double* M0 = fwd ? Ak + bs : Ak + 2 * bs;
+        const double* v0 = fwd ? xs + (int64_t)(k - 1) * ld : xs + (int64_t)k * ld;
+        const double* M1 = fwd ? ((k >= 2) ? Ak : nullptr) : ((k + 1 < g.Nz) ? Ak + 3 * bs : nullptr);
+        const double* v1 = fwd ? ((k >= 2) ? xs + (int64_t)(k - 2) * ld : nullptr)
+                               : ((k + 1 < g.Nz) ? xs + (int64_t)(k + 1) * ld : nullptr);
+        const double* M2 = (!fwd && k + 2 < g.Nz) ? Ak + 4 * bs : nullptr;
+        const double* v2 = (!fwd && k + 2 < g.Nz) ? xs + (int64_t)(k + 2) * ld : nullptr;
+        for (int r = tid; r < nb; r += blockDim.x) {
             double acc = 0.0;
-            if (r < nb)
-                for (int c = lane4; c < nb; c += 4) acc += Ui[(int64_t)c * nb + r] * zk[c];
-            acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-            acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-            if (nout < 8) outv[nout] = acc;
-            ++nout;
+            for (int c = 0; c < nb; ++c) acc += M0[(int64_t)r * ld + c] * v0[c];
+            if (M1) for (int c = 0; c < nb; ++c) acc += M1[(int64_t)r * ld + c] * v1[c];
+            if (M2) for (int c = 0; c < nb; ++c) acc += M2[(int64_t)r * ld + c] * v2[c];
+            tv[r] = fwd ? xs[(int64_t)k * ld + r] - acc : acc;
         }
         __syncthreads();
-        nout = 0;
-        for (int r0 = 0; r0 < nb; r0 += rows_per_pass) {
-            int r = r0 + tid / 4;
-            if (r < nb && lane4 == 0 && nout < 8) zk[r] = outv[nout];
-            ++nout;
-        }
+        for (int r = tid; r < nb; r += blockDim.x) xs[(int64_t)k * ld + r] = tv[r];
         __syncthreads();
     }
     for (int64_t q = tid; q < (int64_t)g.Nz * nb; q += blockDim.x) {
         int k = (int)(q / nb), l = (int)(q % nb);
         int64_t gi = pc_glob(g, part, k, l);
-        x[gi] = sc ? xs[q] / sc[gi] : xs[q];
+        x[gi] = sc ? xs[(int64_t)k * ld + l] / sc[gi] : xs[(int64_t)k * ld + l];
     }
 }
 
@@ -356,6 +723,8 @@ static PcGeom geom_of(const dv_model* m, int mode) {
         g.nb = DV_NV * g.Nr * g.Nth + (g.wall ? g.Nth : 0);
         g.nparts = 1;
     }
+    g.ld = pc_ld(g.nb);
+    g.bs = (((int64_t)g.nb * g.ld + 1) / 2) * 2;
     return g;
 }
 
@@ -366,32 +735,59 @@ static int smem_optin() {
     return v;
 }
 
+int64_t precond_doubles(int nb, int nparts, int Nz) {
+    const int ld = pc_ld(nb);
+    return (int64_t)nparts * Nz * 5 * ((((int64_t)nb * ld + 1) / 2) * 2);
+}
+
+int64_t precond_work_doubles(int nb, int nparts, int Nz) {
+    const int ld = pc_ld(nb);
+    return std::max((int64_t)nparts * 4 * (int64_t)nb * ld, (int64_t)nparts * Nz * (int64_t)ld);
+}
+
 int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s) {
     PcGeom g = geom_of(m, mode);
     if (g.nb > m->pc_cap_nb || g.nparts > m->pc_cap_parts) {
         set_error("preconditioner partition larger than the workspace allocated at model creation");
         return DV_ERR_ARG;
     }
-    if (g.nb > 8 * 64) {
+    if (g.nb > 512) {
         set_error("preconditioner block size above the supported 512 (use theta_block)");
         return DV_ERR_UNSUPPORTED;
     }
-    const int64_t n2 = (int64_t)g.nb * g.nb;
-    const int64_t total = (int64_t)g.nparts * g.Nz * 5 * n2;
-    k_pc_zero<<<std::min<int64_t>((total + 255) / 256, 4096), 256, 0, s>>>(m->d_pc, total);
+    const int64_t total = (int64_t)g.nparts * g.Nz * 5 * g.bs;
+    DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_zero<<<std::min<int64_t>((total + 255) / 256, 4096), 256, 0, s>>>(m->d_pc, total));
     dim3 grid((unsigned)((m->nc + 127) / 128), DV_NSLOT);
-    k_pc_scatter<<<grid, 128, 0, s>>>(g, J, dh, m->d_pc);
-    const size_t static_smem = (2 * 1024 + 256) * sizeof(double) + 256 * sizeof(int);
-    size_t need = (size_t)2 * n2 * sizeof(double);
-    int use_smem = (need + static_smem) <= (size_t)smem_optin() ? 1 : 0;
-    size_t dyn = use_smem ? need : 0;
-    if (use_smem) DV_CUDA(cudaFuncSetAttribute(k_pc_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    k_pc_factor<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_work, m->d_pc_info, use_smem);
+    DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_scatter<<<grid, 128, 0, s>>>(g, J, dh, m->d_pc));
+    const int optin = smem_optin();
+    const size_t n2b = (size_t)g.nb * g.ld * sizeof(double);
+    if (g.nb <= PC_SMEM_NB && 9 * n2b + 2048 <= (size_t)optin) {
+        size_t dyn = 9 * n2b;
+        if (dyn > 48 * 1024) DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_smem<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_info));
+    } else {
+        const size_t static_smem = (2 * 1024 + 256) * sizeof(double) + 256 * sizeof(int);
+        size_t need = (size_t)2 * g.nb * g.nb * sizeof(double);
+        int use_smem = (need + static_smem) <= (size_t)optin ? 1 : 0;
+        size_t dyn = use_smem ? need : 0;
+        if (use_smem && dyn > 48 * 1024)
+            DV_CUDA(cudaFuncSetAttribute(k_pc_factor_glob, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_glob<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_work, m->d_pc_info, use_smem));
+    }
     DV_CUDA(cudaGetLastError());
     m->pc_mode = g.mode;
     m->pc_nb = g.nb;
     m->pc_nparts = g.nparts;
     m->pc_ready = 1;
+    return DV_OK;
+}
+
+template <int NJ>
+static int launch_apply(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
+                        size_t dyn) {
+    if (dyn > 48 * 1024)
+        DV_CUDA(cudaFuncSetAttribute(k_pc_apply<NJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err));
     return DV_OK;
 }
 
@@ -401,13 +797,20 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
         return DV_ERR_ARG;
     }
     PcGeom g = geom_of(m, m->pc_mode == 0 ? 0 : 1);
-    size_t dyn = (size_t)g.Nz * g.nb * sizeof(double);
-    if (dyn > 48 * 1024) DV_CUDA(cudaFuncSetAttribute(k_pc_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    if (dyn > (size_t)smem_optin()) {
-        set_error("preconditioner sweep vector exceeds shared memory");
-        return DV_ERR_UNSUPPORTED;
+    const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
+    const int nj = g.ld / PA_LANES;
+    if (g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7)) {
+        int rc = DV_OK;
+        switch (nj) {
+            case 1: rc = launch_apply<1>(g, m, b, sc, x, s, dyn); break;
+            case 3: rc = launch_apply<3>(g, m, b, sc, x, s, dyn); break;
+            case 5: rc = launch_apply<5>(g, m, b, sc, x, s, dyn); break;
+            default: rc = launch_apply<7>(g, m, b, sc, x, s, dyn); break;
+        }
+        if (rc != DV_OK) return rc;
+    } else {
+        DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply_glob<<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work));
     }
-    k_pc_apply<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, b, sc, x);
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }

@@ -16,6 +16,72 @@ namespace dv {
 
 static thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
+
+// ---------------------------------------------------------------- launch accounting / profiler
+struct ProfSlot {
+    int64_t launches = 0, timed = 0;
+    double ms = 0.0;
+};
+static ProfSlot g_prof[K_NKIND];
+static int64_t g_launches = 0;
+static bool g_prof_on = false;
+struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+};
+static std::vector<Pending> g_pending;
+static std::vector<cudaEvent_t> g_free_ev;
+static cudaEvent_t g_open_ev = nullptr;
+
+static cudaEvent_t ev_get() {
+    if (!g_free_ev.empty()) {
+        cudaEvent_t e = g_free_ev.back();
+        g_free_ev.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_begin(int kind, cudaStream_t s) {
+    ++g_launches;
+    ++g_prof[kind].launches;
+    if (!g_prof_on) return;
+    g_open_ev = ev_get();
+    cudaEventRecord(g_open_ev, s);
+}
+
+void prof_end(int kind, cudaStream_t s) {
+    if (!g_prof_on || !g_open_ev) return;
+    cudaEvent_t b = ev_get();
+    cudaEventRecord(b, s);
+    g_pending.push_back({kind, g_open_ev, b});
+    g_open_ev = nullptr;
+    if (g_pending.size() > 8192) {      // bound the pool: wait for the oldest and fold them in
+        cudaEventSynchronize(g_pending.back().b);
+        prof_flush();
+    }
+}
+
+void prof_flush() {
+    size_t keep = 0;
+    for (size_t q = 0; q < g_pending.size(); ++q) {
+        Pending& p = g_pending[q];
+        if (cudaEventQuery(p.b) == cudaSuccess) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            g_prof[p.kind].ms += ms;
+            g_prof[p.kind].timed += 1;
+            g_free_ev.push_back(p.a);
+            g_free_ev.push_back(p.b);
+        } else {
+            g_pending[keep++] = p;
+        }
+    }
+    g_pending.resize(keep);
+    cudaGetLastError();
+}
 int cuda_fail(cudaError_t e, const char* what) {
     g_err = std::string("CUDA error ") + cudaGetErrorString(e) + " in " + what;
     return DV_ERR_CUDA;
@@ -255,8 +321,8 @@ void work_free(Work& W) {
 // reductions returning host values (synchronise)
 static int rms_ratio_dev(Work& W, int64_t n, const double* a, const double* b, int mode, double* dst, cudaStream_t s) {
     unsigned g = vgrid(n);
-    k_sumsq<<<g, VB, 0, s>>>(n, a, b, W.part);
-    k_finish<<<1, VB, 0, s>>>((int)g, W.part, (double)n, mode, dst);
+    DV_LAUNCH(dv::K_VECTOR, s, k_sumsq<<<g, VB, 0, s>>>(n, a, b, W.part));
+    DV_LAUNCH(dv::K_VECTOR, s, k_finish<<<1, VB, 0, s>>>((int)g, W.part, (double)n, mode, dst));
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }
@@ -265,6 +331,7 @@ static int fetch(Work& W, const double* dev, int cnt, double* host, cudaStream_t
     DV_CUDA(cudaMemcpyAsync(W.hpin, dev, sizeof(double) * cnt, cudaMemcpyDeviceToHost, s));
     DV_CUDA(cudaStreamSynchronize(s));
     memcpy(host, W.hpin, sizeof(double) * cnt);
+    if (g_prof_on && !g_pending.empty()) prof_flush();
     return DV_OK;
 }
 
@@ -347,7 +414,7 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
         return DV_OK;
     }
     const int64_t ldv = n;
-    k_axpby<<<vgrid(n), VB, 0, st>>>(n, 1.0 / bn2, b, 0.0, nullptr, W.V);      // v0 = r / ||r||
+    DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<vgrid(n), VB, 0, st>>>(n, 1.0 / bn2, b, 0.0, nullptr, W.V));      // v0 = r / ||r||
     std::vector<double> H((size_t)kdim * (kdim + 1), 0.0), S(kdim + 1, 0.0), gc(kdim), gs(kdim);
     auto h = [&](int col, int k) -> double& { return H[(size_t)col * (kdim + 1) + k]; };
     S[0] = bn2;
@@ -360,12 +427,12 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
         DV_TRY(apply_AP(W, op, W.V + col * ldv, w, st));
         // classical Gram-Schmidt, twice (orthogonality equivalent to scipy's modified GS)
         const int m = col + 1;
-        k_dots<<<g, VB, 0, st>>>(n, m, W.V, ldv, w, W.part);
-        k_dots_finish<<<m + 1, VB, 0, st>>>((int)g, m + 1, W.part, W.hbuf);
-        k_orth_update<<<g, VB, 0, st>>>(n, m, W.V, ldv, W.hbuf, w);
-        k_dots<<<g, VB, 0, st>>>(n, m, W.V, ldv, w, W.part);
-        k_dots_finish<<<m + 1, VB, 0, st>>>((int)g, m + 1, W.part, W.hbuf + (kdim + 2));
-        k_orth_update<<<g, VB, 0, st>>>(n, m, W.V, ldv, W.hbuf + (kdim + 2), w);
+        DV_LAUNCH(dv::K_VECTOR, st, k_dots<<<g, VB, 0, st>>>(n, m, W.V, ldv, w, W.part));
+        DV_LAUNCH(dv::K_VECTOR, st, k_dots_finish<<<m + 1, VB, 0, st>>>((int)g, m + 1, W.part, W.hbuf));
+        DV_LAUNCH(dv::K_VECTOR, st, k_orth_update<<<g, VB, 0, st>>>(n, m, W.V, ldv, W.hbuf, w));
+        DV_LAUNCH(dv::K_VECTOR, st, k_dots<<<g, VB, 0, st>>>(n, m, W.V, ldv, w, W.part));
+        DV_LAUNCH(dv::K_VECTOR, st, k_dots_finish<<<m + 1, VB, 0, st>>>((int)g, m + 1, W.part, W.hbuf + (kdim + 2)));
+        DV_LAUNCH(dv::K_VECTOR, st, k_orth_update<<<g, VB, 0, st>>>(n, m, W.V, ldv, W.hbuf + (kdim + 2), w));
         DV_TRY(rms_ratio_dev(W, n, w, nullptr, 2, W.hbuf + 2 * (kdim + 2), st));
         DV_CUDA(cudaGetLastError());
         std::vector<double> hh(2 * (kdim + 2) + 1);
@@ -380,7 +447,7 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
             h(col, col + 1) = 0.0;
             breakdown = true;
         } else {
-            k_axpby<<<g, VB, 0, st>>>(n, 1.0 / h1, w, 0.0, nullptr, w);
+            DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0 / h1, w, 0.0, nullptr, w));
         }
         for (int k = 0; k < col; ++k) {
             double c = gc[k], s = gs[k];
@@ -416,10 +483,10 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
     if (y[0] != 0.0) y[0] /= h(0, 0);
     memcpy(W.hpin, y.data(), sizeof(double) * (col + 1));
     DV_CUDA(cudaMemcpyAsync(W.ybuf, W.hpin, sizeof(double) * (col + 1), cudaMemcpyHostToDevice, st));
-    k_combine<<<g, VB, 0, st>>>(n, col + 1, W.V, ldv, W.ybuf, W.x);
+    DV_LAUNCH(dv::K_VECTOR, st, k_combine<<<g, VB, 0, st>>>(n, col + 1, W.V, ldv, W.ybuf, W.x));
     // true residual r = b - AP x
     DV_TRY(apply_AP(W, op, W.x, W.r, st));
-    k_axpby<<<g, VB, 0, st>>>(n, 1.0, b, -1.0, W.r, W.r);
+    DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, b, -1.0, W.r, W.r));
     double rnorm;
     DV_TRY(rms_ratio_dev(W, n, W.r, nullptr, 2, W.scal + 10, st));
     DV_TRY(fetch(W, W.scal + 10, 1, &rnorm, st));
@@ -466,12 +533,12 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
     r.rate = 0.0;
     r.refreshed = 0;
     const double kappa = C.o.kappa, rtol = C.o.rtol;
-    auto scale = [&](const double* z, double* s) { k_scale<<<g, VB, 0, st>>>(m->nc, n, z, C.atol7, rtol, s); };
+    auto scale = [&](const double* z, double* s) { DV_LAUNCH(dv::K_VECTOR, st, k_scale<<<g, VB, 0, st>>>(m->nc, n, z, C.atol7, rtol, s)); };
     auto stage = [&](const double* z, double* f, double* R) -> int {
         // f = rhs(z); R = z - dh f - rhs_known
         DV_TRY(launch_rhs(m, t, z, f, nullptr, st));
-        k_axpby<<<g, VB, 0, st>>>(n, 1.0, z, -dh, f, R);
-        k_axpby<<<g, VB, 0, st>>>(n, 1.0, R, -1.0, rhs_known, R);
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, z, -dh, f, R));
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, R, -1.0, rhs_known, R));
         return DV_OK;
     };
     auto pnorm = [&](const double* RR, const double* ss, double* out) -> int {
@@ -482,7 +549,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
     auto cons_ok = [&](const double* R, const double* z, bool* ok) -> int {
         if (C.o.cons_tol <= 0.0) { *ok = true; return DV_OK; }
         scale(z, W.tmp);
-        k_cons<<<1, VB, 0, st>>>(m->p, R, W.tmp, W.scal);
+        DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<1, VB, 0, st>>>(m->p, R, W.tmp, W.scal));
         DV_CUDA(cudaGetLastError());
         double v[8];
         DV_TRY(fetch(W, W.scal, 8, v, st));
@@ -514,7 +581,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
     while (it + 1 < C.o.max_iter + polish) {
         ++it;
         scale(W.z, W.s);
-        k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.b);                    // b = -R/s
+        DV_LAUNCH(dv::K_VECTOR, st, k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.b));                    // b = -R/s
         DV_TRY(rms_ratio_dev(W, n, W.z, W.s, 1, W.scal + 1, st));           // zs = max(1, rms(z/s))
         Op op{m, t, dh, W.z, W.f, W.s, n};
         const double floor_ = (polish ? 1e-4 : 0.1 * kappa) * sqrt_n;
@@ -536,7 +603,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         }
         // dz = prec(w) * s
         DV_TRY(precond_apply(m, W.x, W.s, W.u, st));
-        k_mul<<<g, VB, 0, st>>>(n, W.u, W.s, W.dz);
+        DV_LAUNCH(dv::K_VECTOR, st, k_mul<<<g, VB, 0, st>>>(n, W.u, W.s, W.dz));
         double dzn;
         DV_TRY(rms_ratio(W, n, W.dz, nullptr, &dzn, st));
         if (!std::isfinite(dzn)) {
@@ -547,7 +614,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         }
         double lam = 1.0, rn_try = 0.0, pn_try = INFINITY;
         for (int ls = 0; ls < 4; ++ls) {
-            k_truncate<<<g, VB, 0, st>>>(n, C.npos, W.z, lam, W.dz, W.zt);
+            DV_LAUNCH(dv::K_VECTOR, st, k_truncate<<<g, VB, 0, st>>>(n, C.npos, W.z, lam, W.dz, W.zt));
             DV_TRY(stage(W.zt, W.ft, W.Rt));
             DV_TRY(rms_ratio(W, n, W.Rt, W.s, &rn_try, st));
             if (std::isfinite(rn_try)) DV_TRY(pnorm(W.Rt, W.s, &pn_try));
@@ -562,7 +629,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             return DV_OK;
         }
         // step = rms((z_try - z)/s)
-        k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.tmp);
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.tmp));
         double step;
         DV_TRY(rms_ratio(W, n, W.tmp, W.s, &step, st));
         std::swap(W.z, W.zt);
@@ -676,11 +743,43 @@ struct dv_integrator {
     dv_step_report rep;
 };
 
+namespace dv {
+// A bounded device wait that gave up leaves a flag in the model; surface it as an error.
+static int check_device_error(dv_model* m) {
+    int e = 0;
+    DV_CUDA(cudaMemcpy(&e, m->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+        set_error("a bounded device wait (preconditioner TMA copy) timed out");
+        return DV_ERR_CUDA;
+    }
+    return DV_OK;
+}
+}  // namespace dv
 using namespace dv;
 
 extern "C" {
 
 int dv_abi_version(void) { return DV_ABI_VERSION; }
+
+int dv_profile_enable(int32_t on) {
+    cudaDeviceSynchronize();
+    prof_flush();
+    for (auto& q : g_prof) q = ProfSlot();
+    g_prof_on = on != 0;
+    return DV_OK;
+}
+
+int dv_profile_read(int32_t kind, int64_t* launches, int64_t* timed, double* total_ms) {
+    if (kind < 0 || kind >= K_NKIND) { set_error("dv_profile_read: bad kernel kind"); return DV_ERR_ARG; }
+    DV_CUDA(cudaDeviceSynchronize());
+    prof_flush();
+    if (launches) *launches = g_prof[kind].launches;
+    if (timed) *timed = g_prof[kind].timed;
+    if (total_ms) *total_ms = g_prof[kind].ms;
+    return DV_OK;
+}
+
+int64_t dv_launch_count(void) { return g_launches; }
 size_t dv_step_params_size(void) { return sizeof(dv_step_params); }
 const char* dv_last_error(void) { return g_err.c_str(); }
 
@@ -696,7 +795,8 @@ int dv_device_count(int* n) {
 
 int dv_model_destroy(dv_model* m) {
     if (!m) return DV_OK;
-    void* ptrs[] = {m->d_aux, m->d_rec, m->d_acc, m->d_pc, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7};
+    void* ptrs[] = {m->d_aux, m->d_rec, m->d_acc, m->d_pc, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
+                    m->d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
     if (m->W) {
@@ -728,9 +828,9 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     bool full_ok = nb_full <= 512;
     m->pc_cap_nb = full_ok ? std::max(nb_full, nb_sector) : nb_sector;
     m->pc_cap_parts = p->Nth;
-    int64_t pc_need = std::max((int64_t)p->Nth * p->Nz * 5 * (int64_t)nb_sector * nb_sector,
-                               full_ok ? (int64_t)p->Nz * 5 * (int64_t)nb_full * nb_full : (int64_t)0);
-    int64_t work_need = (int64_t)m->pc_cap_parts * 4 * (int64_t)m->pc_cap_nb * m->pc_cap_nb;
+    int64_t pc_need = std::max(precond_doubles(nb_sector, p->Nth, p->Nz),
+                               full_ok ? precond_doubles(nb_full, 1, p->Nz) : (int64_t)0);
+    int64_t work_need = precond_work_doubles(m->pc_cap_nb, m->pc_cap_parts, p->Nz);
     const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
     bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
@@ -739,7 +839,8 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
                 cudaMalloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_atol7, sizeof(double) * DV_NB) != cudaSuccess;
+                cudaMalloc((void**)&m->d_atol7, sizeof(double) * DV_NB) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_err, sizeof(int)) != cudaSuccess;
     if (fail) {
         int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(model workspace)");
         dv_model_destroy(m);
@@ -759,6 +860,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     m->aux.n_nom = m->d_aux + nf;
     m->aux.cov = m->d_aux + 2 * nf;
     cudaMemset(m->d_rec, 0, sizeof(double) * rec_n);
+    cudaMemset(m->d_err, 0, sizeof(int));
     int32_t ncol = 0;
     std::vector<int64_t> colour((size_t)m->n);
     rc = dv_colour_columns(p->Nr, p->Nth, p->Nz, p->wall_on, colour.data(), &ncol);
@@ -831,6 +933,7 @@ int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_k
     NewtonCtx C{m, m->W, m->d_atol7, m->n, DV_NG * m->nc + DV_NA * m->nc, *o, r, nullptr};
     int rc = newton_krylov(C, t, z0, rhs_known, dh, z_out, st);
     cudaStreamSynchronize(st);
+    if (rc == DV_OK) rc = check_device_error(m);
     return rc;
 }
 
@@ -966,11 +1069,14 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         }
         const double dh = D_ * h;
         // ---- stage 1
-        if (sd) DV_CUDA(cudaMemcpyAsync(g->rhs1, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-        else k_xpay<<<gr, VB, 0, st>>>(n, g->y, dh, g->fn, g->rhs1);
+        if (sd) {
+            DV_CUDA(cudaMemcpyAsync(g->rhs1, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        } else {
+            DV_LAUNCH(dv::K_VECTOR, st, k_xpay<<<gr, VB, 0, st>>>(n, g->y, dh, g->fn, g->rhs1));
+        }
         if (g->have_slope) {
-            k_xpay<<<gr, VB, 0, st>>>(n, g->y, c_mid * h, g->slope, g->pred);
-            k_truncate_to<<<gr, VB, 0, st>>>(n, npos, g->pred, g->y, g->pred);
+            DV_LAUNCH(dv::K_VECTOR, st, k_xpay<<<gr, VB, 0, st>>>(n, g->y, c_mid * h, g->slope, g->pred));
+            DV_LAUNCH(dv::K_VECTOR, st, k_truncate_to<<<gr, VB, 0, st>>>(n, npos, g->pred, g->y, g->pred));
         } else {
             DV_CUDA(cudaMemcpyAsync(g->pred, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         }
@@ -994,9 +1100,12 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         }
         bool ok = r1.ok != 0;
         if (ok) {
-            if (sd) k_sd_rhs2<<<gr, VB, 0, st>>>(n, g->y, g->z1, dh, (1.0 - G_SD_) * h, g->rhs2);
-            else k_axpby<<<gr, VB, 0, st>>>(n, C1_, g->z1, -C2_, g->y, g->rhs2);
-            k_pred2<<<gr, VB, 0, st>>>(n, npos, g->y, g->z1, c_mid, g->pred);
+            if (sd) {
+                DV_LAUNCH(dv::K_VECTOR, st, k_sd_rhs2<<<gr, VB, 0, st>>>(n, g->y, g->z1, dh, (1.0 - G_SD_) * h, g->rhs2));
+            } else {
+                DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<gr, VB, 0, st>>>(n, C1_, g->z1, -C2_, g->y, g->rhs2));
+            }
+            DV_LAUNCH(dv::K_VECTOR, st, k_pred2<<<gr, VB, 0, st>>>(n, npos, g->y, g->z1, c_mid, g->pred));
             dv_newton_result r2;
             memset(&r2, 0, sizeof r2);
             NewtonCtx C2{m, &W, m->d_atol7, n, npos, no, &r2, &g->gm};
@@ -1030,10 +1139,13 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         // ---- error estimate filtered by M^-1 (core/solver.py:454-469)
         DV_TRY(launch_rhs(m, g->t + c_mid * h, g->z1, g->f1, g->d_g + DV_NACC, st));
         DV_TRY(launch_rhs(m, g->t + h, g->z2, g->f2, g->d_g + 2 * DV_NACC, st));
-        if (sd) k_err_vec<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, SW1_, g->fn, SW2_, g->f1, SW3_, g->f2, g->ev);
-        else k_err_vec<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, W1_, g->fn, W2_, g->f1, W3_, g->f2, g->ev);
+        if (sd) {
+            DV_LAUNCH(dv::K_VECTOR, st, k_err_vec<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, SW1_, g->fn, SW2_, g->f1, SW3_, g->f2, g->ev));
+        } else {
+            DV_LAUNCH(dv::K_VECTOR, st, k_err_vec<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, W1_, g->fn, W2_, g->f1, W3_, g->f2, g->ev));
+        }
         DV_TRY(precond_apply(m, g->ev, nullptr, g->ev, st));
-        k_err_scale<<<gr, VB, 0, st>>>(m->nc, n, g->y, g->z2, m->d_atol7, g->o.rtol, g->es);
+        DV_LAUNCH(dv::K_VECTOR, st, k_err_scale<<<gr, VB, 0, st>>>(m->nc, n, g->y, g->z2, m->d_atol7, g->o.rtol, g->es));
         double en;
         DV_TRY(rms_ratio(W, n, g->ev, g->es, &en, st));
         if (!std::isfinite(en)) en = 1e6;
@@ -1057,7 +1169,7 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
                 g->acc[q] = C1_ * acc_g - C2_ * g->acc[q] + D_ * h * g2[q];
             }
         }
-        k_slope<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, g->slope);
+        DV_LAUNCH(dv::K_VECTOR, st, k_slope<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, g->slope));
         g->have_slope = true;
         std::swap(g->y, g->z2);
         std::swap(g->fn, g->f2);
@@ -1078,7 +1190,7 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         sync_nfev();
         DV_CUDA(cudaStreamSynchronize(st));
         *rep = R;
-        return DV_OK;
+        return check_device_error(m);
     }
     R.t = g->t;
     sync_nfev();

@@ -17,7 +17,7 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
-from . import host
+from . import counters, host
 from ._lib import DV_NACC, DvNewtonOpts, DvNewtonResult, DvStepParams, check, load
 from .params import build_params
 
@@ -213,6 +213,7 @@ class TVSAModel:
         if a.shape != (self.n_core,):
             raise ValueError(f"state vector must have shape ({self.n_core},), got {a.shape}")
         buf.copy_(torch.from_numpy(a), non_blocking=False)
+        counters.h2d(a.nbytes)
         return buf, False
 
     # ------------------------------------------------------------------ RHS
@@ -229,6 +230,7 @@ class TVSAModel:
             if on_dev:
                 return f, (acc.clone() if acc is not None else None)
             fh = f.cpu().numpy()
+            counters.d2h(fh.nbytes + (8 * DV_NACC if acc is not None else 0))
             return fh, (acc.cpu().numpy() if acc is not None else None)
 
     def stage_residual(self, t, y, gamma_h, rhs_known):
@@ -239,7 +241,10 @@ class TVSAModel:
             R = torch.empty_like(yd) if on_dev else self._f
             check(self.lib.dv_stage_residual(self.handle, float(t), _ptr(yd), float(gamma_h), _ptr(kd), _ptr(R),
                                              _stream()), "dv_stage_residual")
-            return R if on_dev else R.cpu().numpy()
+            if on_dev:
+                return R
+            counters.d2h(8 * self.n_core)
+            return R.cpu().numpy()
 
     def _diag_dict(self, t, yd):
         g = self.grid
@@ -247,6 +252,7 @@ class TVSAModel:
             self._diag = torch.empty(self.diag_doubles, dtype=torch.float64, device=self.device)
         check(self.lib.dv_rhs_diag(self.handle, float(t), _ptr(yd), _ptr(self._diag), _stream()), "dv_rhs_diag")
         d = self._diag.cpu().numpy()
+        counters.d2h(d.nbytes)
         Nr, Nth, Nz = g.shape
         nc, nf, nw = g.ncell, Nr * Nth, Nth * Nz
         o = 0

@@ -1,0 +1,224 @@
+"""Step runner and cycle driver on the GPU classes.
+
+``run_step`` has the signature and result of the reference's steps/_runner.py:87-188 (build the
+model and integrator of one cycle step, record the outlet at every accepted step through
+``model.rhs(diag=True)``, return the end state and a ``StepResult``); ``run_cycle`` chains the
+steps of ``cfg.cycle`` like vtsa_cycle.py:72-90 without the CSV hand-off (states stay in memory).
+
+``run_cycle_device`` is the device-resident variant used for throughput measurements: the state
+stays on the GPU between steps, no outlet recording, only the per-step constants (end pressures
+at step start) are read back.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+import torch
+
+from . import host
+from .model import TVSAModel
+from .solver import TRBDF2
+
+R_GAS = host.R_GAS
+
+
+@dataclass
+class StepResult:
+    name: str
+    type: str
+    cycle: int
+    t_start_cycle: float
+    duration_planned: float
+    duration: float
+    stopped_early: bool
+    acc: Dict[str, float]
+    inv_start: Dict[str, float]
+    inv_end: Dict[str, float]
+    outlet: List[Dict] = field(default_factory=list)
+    snapshots: List[Dict] = field(default_factory=list)
+    solver: Dict = field(default_factory=dict)
+    wall_time: float = 0.0
+    T_jacket: float = 298.15
+    jacket_on: bool = True
+    product_port: str = "V3"
+    valves: Dict = field(default_factory=dict)
+    ads_start: Dict[str, float] = field(default_factory=dict)
+    ads_end: Dict[str, float] = field(default_factory=dict)
+
+
+def _end_summary(model, d, end, c_feed_co2):
+    """Outlet composition / flow of one end (steps/_runner.py:50-84)."""
+    b = d["bnd"][end]
+    Fout = -b["F_in"]
+    tot = Fout.sum(axis=0)
+    Ftot = float(tot.sum())
+    k_lay = 0 if end == "top" else -1
+    T_lay = d["T"][..., k_lay]
+    A = model.grid.Az * np.ones_like(T_lay)
+    P_face = float(np.sum(b["P_face"] * A) / np.sum(A))
+    out_faces = tot > 0.0
+    if "F_outpart" in b:
+        Fout = b["F_outpart"]
+        tot = Fout.sum(axis=0)
+        out_faces = tot > 0.0
+    F_leaving = float(tot[out_faces].sum()) if np.any(out_faces) else 0.0
+    if F_leaving > 1e-14:
+        ys = [float(Fout[k][out_faces].sum()) / F_leaving for k in range(model.ng)]
+        T_g = float(np.sum(T_lay[out_faces] * tot[out_faces]) / F_leaving)
+    else:
+        yl = d["y"][..., k_lay]
+        ys = [float(np.sum(yl[k] * A) / np.sum(A)) for k in range(model.ng)]
+        T_g = float(np.sum(T_lay * A) / np.sum(A))
+    out = {f"{end}_valve": model.conds[end].valve or "closed", f"{end}_valve_state": model.conds[end].state.value,
+           f"{end}_flow_out_mol_s": Ftot, f"{end}_P_Pa": P_face, f"{end}_T_K": T_g}
+    for k, s in enumerate(model.species):
+        out[f"{end}_y_{s}"] = ys[k]
+    c_co2 = ys[model.i_co2] * P_face / (R_GAS * T_g)
+    out[f"{end}_c_CO2_mol_m3"] = c_co2
+    out[f"{end}_C_over_Cfeed"] = c_co2 / c_feed_co2 if c_feed_co2 > 0 else np.nan
+    return out
+
+
+def run_step(state_in, cfg, grid, props, step: Dict, cycle_idx: int = 1, t_cycle0: float = 0.0,
+             T_jacket_prev: Optional[float] = None, logger=None, snapshots: Optional[int] = None,
+             record_outlet: bool = True):
+    """One cycle step on the GPU (steps/_runner.py:87-188)."""
+    log = logger or (lambda *a, **k: None)
+    model = TVSAModel(cfg, grid, props, step, state_in, T_jacket_prev)
+    y0 = model.pack(state_in)
+    dur = float(step["duration"])
+    n_snap = snapshots if snapshots is not None else cfg.run.snapshots_per_step
+    t_out = np.linspace(0.0, dur, max(2, n_snap))
+    yf = host.humid_air_composition(model.species, cfg.feed.P, cfg.feed.T, cfg.feed.RH if model.water else 0.0,
+                                    cfg.feed.y_co2_dry, float(host.arden_buck(cfg.feed.T)))
+    c_feed_co2 = yf[model.i_co2] * cfg.feed.P / (R_GAS * cfg.feed.T)
+    outlet: List[Dict] = []
+    every = cfg.solver.outlet_record_every
+    counter = [0]
+    V = grid.volume_full()
+    Vt = float(V.sum())
+
+    def record(t, y, acc):
+        d = model.rhs(t, y, diag=True)
+        row = {"cycle": cycle_idx, "step": step["name"], "t_step_s": t, "t_cycle_s": t_cycle0 + t,
+               "t_total_s": state_in.t + t}
+        for end in ("top", "bottom"):
+            row.update(_end_summary(model, d, end, c_feed_co2))
+        row["bed_T_mean_K"] = float(np.sum(d["T"] * V) / Vt)
+        row["bed_P_mean_Pa"] = float(np.sum(d["P"] * V) / Vt)
+        c, q, e, Tw = model.unpack(y)
+        for n, s in enumerate(model.adsorbed):
+            row[f"bed_q_{s}_mean"] = float(np.sum(q[n] * V) / Vt)
+        ai = model.acc_index
+        for v in ("V1", "V2", "V3"):
+            row[f"cum_CO2_out_{v}_mol"] = acc[ai[f"n_out_{v}_CO2"]]
+        row["cum_Q_jacket_J"] = acc[ai["Q_jac_pos"]] + acc[ai["Q_jac_neg"]]
+        outlet.append(row)
+
+    def on_step(t, y, acc):
+        counter[0] += 1
+        if record_outlet and counter[0] % every == 0:
+            record(t, y, acc)
+
+    if record_outlet:
+        record(0.0, y0, np.zeros(model.n_acc))
+    stop = step.get("stop_on")
+    stop_fn = stop_val = None
+    direction = 1
+    if stop:
+        stop_fn = model.stop_metric
+        stop_val = stop["value"]
+        direction = -1 if stop["criterion"] == "min_temperature" else 1
+    wall0 = time.time()
+    integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * dur)
+    res = integ.integrate(y0, dur, t_out, on_step=on_step if record_outlet else None, stop_fn=stop_fn,
+                          stop_value=stop_val, stop_direction=direction)
+    solver_stats = {"method": "trbdf2", "steps": res.n_steps, "rejected": res.n_reject,
+                    "newton_fail": res.n_newton_fail, "krylov": res.n_krylov, "jacobians": res.n_jac,
+                    "lu": res.n_lu, "nfev": res.nfev, "groups": integ.jac.ngroups, **integ.stats}
+    if record_outlet and outlet[-1]["t_step_s"] < res.t:
+        record(res.t, res.y, res.acc)
+    wall = time.time() - wall0
+    state_out = model.to_state(res.y, state_in, state_in.t + res.t, step["name"])
+    state_out.cycle = cycle_idx
+    snaps = []
+    for (ts, ys, _a) in res.snapshots:
+        st = model.to_state(ys, state_in, state_in.t + ts, step["name"])
+        st.cycle = cycle_idx
+        snaps.append({"cycle": cycle_idx, "step": step["name"], "t_step": ts, "t_cycle": t_cycle0 + ts,
+                      "t_total": state_in.t + ts, "state": st})
+    inv0, inv1 = model.inventories(y0), model.inventories(res.y)
+    acc_d = {nm: float(res.acc[i]) for i, nm in enumerate(model.acc_names)}
+    T_jac = model.T_jacket(res.t) if model.jacket_on else cfg.ambient.T
+    sr = StepResult(name=step["name"], type=step["type"], cycle=cycle_idx, t_start_cycle=t_cycle0,
+                    duration_planned=dur, duration=res.t, stopped_early=res.stopped_early, acc=acc_d,
+                    inv_start=inv0, inv_end=inv1, outlet=outlet, snapshots=snaps, solver=solver_stats,
+                    wall_time=wall, T_jacket=float(T_jac), jacket_on=model.jacket_on,
+                    product_port=step.get("product_port", "V3"), valves=dict(step["valves"]),
+                    ads_start={s: inv0[f"ads_{s}"] for s in model.adsorbed},
+                    ads_end={s: inv1[f"ads_{s}"] for s in model.adsorbed})
+    log(f"    {step['name']:<14s} {res.t:9.1f} s  steps={res.n_steps:>5}  wall={wall:6.2f}s")
+    return state_out, sr
+
+
+def run_cycle(state, cfg, grid, props, cycle_idx: int = 1, T_jac_prev=None, logger=None, record_outlet=True):
+    """All steps of cfg.cycle in order (vtsa_cycle.py:72-90, states handed over in memory)."""
+    steps_out = []
+    t_cycle = 0.0
+    for step in cfg.cycle:
+        state, sr = run_step(state, cfg, grid, props, step, cycle_idx=cycle_idx, t_cycle0=t_cycle,
+                             T_jacket_prev=T_jac_prev, logger=logger, record_outlet=record_outlet)
+        t_cycle += sr.duration
+        T_jac_prev = sr.T_jacket if sr.jacket_on else T_jac_prev
+        steps_out.append(sr)
+    return state, steps_out, T_jac_prev
+
+
+class _PState:
+    """State stand-in carrying only the start pressures a model reads."""
+
+    def __init__(self, P):
+        self.P = P
+
+
+def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None):
+    """Device-resident cycle: y stays on the GPU from step to step; returns (y_end, per-step stats).
+
+    Per step only the start pressure field (for the valve ramps) is evaluated, through the model's
+    diagnostics kernel on the device state; the hand-off keeps e (internal energy) as the unknown,
+    which is what the reference's T round trip (pack(to_state(y))) reproduces to round-off."""
+    y = y0
+    stats = []
+    last_model = None
+    for step in cfg.cycle:
+        P = last_model.rhs(0.0, y, diag=True)["P"] if last_model is not None else _pressure_host(cfg, grid, props, y)
+        model = TVSAModel(cfg, grid, props, step, _PState(P), T_jac_prev)
+        dur = float(step["duration"])
+        integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * dur)
+        res = integ.integrate(y, dur, np.array([dur]), keep_on_device=True)
+        y = res.y
+        stats.append({"step": step["name"], "steps": res.n_steps, "rejected": res.n_reject, "nfev": res.nfev,
+                      "jac": res.n_jac, "lu": res.n_lu, **integ.stats})
+        T_jac_prev = model.T_jacket(res.t) if model.jacket_on else T_jac_prev
+        last_model = model
+    return y, stats, T_jac_prev
+
+
+def _pressure_host(cfg, grid, props, y):
+    yh = y.detach().cpu().numpy() if isinstance(y, torch.Tensor) else y
+    n = grid.ncell
+    c = yh[:3 * n].reshape((3,) + grid.shape)
+    q = yh[3 * n:5 * n].reshape((2,) + grid.shape)
+    e = yh[5 * n:6 * n].reshape(grid.shape)
+    so, th = cfg.sorbent, cfg.thermo
+    eps_t, rho_b = so.total_voidage, cfg.derived.bulk_density
+    cpg = np.asarray(props.cp)
+    A = eps_t * (cpg[0] * c[0] + cpg[1] * c[1] + cpg[2] * c[2]) + rho_b * (so.cp_solid + th.cp_ads_co2 * q[0]
+                                                                           + th.cp_ads_h2o * q[1])
+    B = eps_t * R_GAS * (c[0] + c[1] + c[2])
+    Hq = rho_b * (th.dH_ads_co2 * q[0] + th.dH_ads_h2o * q[1])
+    T = (e - Hq + A * th.T_ref) / (A - B)
+    return (c[0] + c[1] + c[2]) * R_GAS * T

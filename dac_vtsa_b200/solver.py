@@ -20,6 +20,7 @@ from typing import Callable, List, Optional
 import numpy as np
 import torch
 
+from . import counters
 from ._lib import DvSolverOpts, DvStepReport, check, load
 from .config import gpu_option
 from .jacobian import FDJacobian
@@ -120,6 +121,7 @@ class TRBDF2:
             self._y_host = torch.empty(self.m.n_core, dtype=torch.float64).pin_memory()
         check(self.lib.dv_integrator_copy_y(self.handle, C.c_void_p(self._y_host.data_ptr()), self._stream()),
               "dv_integrator_copy_y")
+        counters.d2h(8 * self.m.n_core)
         return self._y_host.numpy().copy()
 
     def integrate(self, y0, t_end: float, t_out, on_step: Optional[Callable] = None,
@@ -138,6 +140,7 @@ class TRBDF2:
             else:
                 y0h = np.ascontiguousarray(y0, dtype=np.float64)
                 y0d = torch.from_numpy(y0h).to(m.device)
+                counters.h2d(y0h.nbytes)
             check(self.lib.dv_integrator_start(self.handle, C.c_void_p(y0d.data_ptr()), float(t_end),
                                                self._stream()), "dv_integrator_start")
             acc = np.zeros(m.n_acc)

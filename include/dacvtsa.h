@@ -126,6 +126,16 @@ size_t dv_step_params_size(void);
 const char* dv_last_error(void);
 int dv_device_count(int* n);
 
+/* Launch accounting (no reference counterpart; instrumentation of this library).  Every kernel launch
+ * is counted per kind: 0 residual (rhs / stage residual / diagnostics / accumulators), 1 finite-
+ * difference matvec residual, 2 FD Jacobian, 3 preconditioner assembly + factorisation,
+ * 4 preconditioner sweep, 5 vector / reduction kernels.  With profiling enabled each launch is also
+ * bracketed by CUDA events on its own stream; dv_profile_read synchronises the device and returns the
+ * launches, the timed launches and their summed device time [ms].  dv_profile_enable resets. */
+int dv_profile_enable(int32_t on);
+int dv_profile_read(int32_t kind, int64_t* launches, int64_t* timed, double* total_ms);
+int64_t dv_launch_count(void);
+
 /* ------------------------------------------------------------------ model
  * Replaces TVSAModel.__init__ (core/residual.py:41-123).  Host inputs: feed_flux and n_nom over
  * (Nr, Ntheta) [mol/s per inlet face; mol/m2/s nominal column flux, zeros without feed],

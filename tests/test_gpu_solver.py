@@ -40,7 +40,13 @@ def test_preconditioner_solves_partition_system(mode):
     b = np.random.default_rng(7).standard_normal(m.n_core) * m.atol
     x_ref = spla.spsolve(M, b)
     x = m.precond_solve(b)
-    assert np.abs(x - x_ref).max() <= 1e-9 * np.abs(x_ref).max()
+    # componentwise backward error |M x - b| / (|M| |x| + |b|): block LU with partial pivoting is
+    # backward stable; the forward error may grow with cond(M) (stiff pressure couplings)
+    Ma = abs(M)
+    berr = np.abs(M @ x - b) / (Ma @ np.abs(x) + np.abs(b))
+    berr_ref = np.abs(M @ x_ref - b) / (Ma @ np.abs(x_ref) + np.abs(b))
+    assert berr.max() <= max(1e-12, 10 * berr_ref.max()), (berr.max(), berr_ref.max())
+    assert np.abs(x - x_ref).max() <= 1e-6 * np.abs(x_ref).max()
 
 
 def test_implicit_solver_matches_rk4_on_short_transient():
