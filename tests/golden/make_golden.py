@@ -205,7 +205,8 @@ def make_bench_state(ref_root, t_mid=4000.0):
 
 def make_bench_state_heating(ref_root, t_heat=4000.0):
     """Reference state of the 8x8x32 benchmark bed after the full adsorption (8000 s) and blowdown
-    (60 s) steps and t_heat seconds of heating, from the seeded constant-pressure initial state."""
+    (60 s) steps of the cycle and t_heat seconds of heating, from the seeded constant-pressure initial
+    state (input of the heating half of the CPU throughput sample in bench.py)."""
     sys.path.insert(0, ref_root)
     import config.parameters as rp
     from core.grid import Grid
@@ -213,6 +214,7 @@ def make_bench_state_heating(ref_root, t_heat=4000.0):
     from core.solver import TRBDF2
     from core.state import initial_state
     from properties import R_GAS, get_backend
+    from steps._runner import run_step
     over = {"grid.Nr": 8, "grid.Ntheta": 8, "grid.Nz": 32, "solver.scheme": "trbdf2",
             "operation.T_adsorption_jacket": 288.0, "operation.T_cool": 288.0, "operation.T_heat": 373.0,
             "operation.P_vacuum": 1e4, "feed.T": 288.0, "feed.RH": 0.5, "ambient.T": 288.0}
@@ -226,7 +228,6 @@ def make_bench_state_heating(ref_root, t_heat=4000.0):
     st.c = y * (101325.0 / (R_GAS * T))[None]
     st.T = T
     st.Tw = np.full(g.wall_shape, 288.0)
-    from steps._runner import run_step
     T_prev = None
     for si in (0, 1):
         st, sr = run_step(st, cfg, g, props, cfg.cycle[si], T_jacket_prev=T_prev, snapshots=2)
@@ -237,12 +238,10 @@ def make_bench_state_heating(ref_root, t_heat=4000.0):
     res = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * float(step["duration"])).integrate(
         m.pack(st), t_heat, [t_heat])
     print(step["name"], res.n_steps, "steps", res.wall_time, "s", flush=True)
-    T_prev = m.T_jacket(t_heat)
-    st = m.to_state(res.y, st, st.t + res.t, step["name"])
-    P0 = st.P
-    np.savez_compressed(os.path.join(HERE, "bench_state_8x8x32_heat4000.npz"), y=m.pack(st), t=t_heat,
-                        P_start_top=float(np.mean(P0[:, :, 0])), P_start_bottom=float(np.mean(P0[:, :, -1])),
-                        T_jacket_prev=float(T_prev), over=np.array(json.dumps(over)))
+    np.savez_compressed(os.path.join(HERE, "bench_state_8x8x32_heat4000.npz"), y=res.y, t=res.t,
+                        T_jacket=float(m.T_jacket(t_heat)), over=np.array(json.dumps(over)),
+                        n_steps=res.n_steps, wall=res.wall_time)
+    print("heating bench state written")
 
 
 if __name__ == "__main__":
