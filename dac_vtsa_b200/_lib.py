@@ -129,6 +129,7 @@ SIGNATURES = [
     ("dv_integrator_advance", C.c_int, [P, D, C.POINTER(DvStepReport), P]),
     ("dv_integrator_y", P, [P]),
     ("dv_integrator_copy_y", C.c_int, [P, P, P]),
+    ("dv_rhs_acc_noalloc", C.c_int, [C.POINTER(DvStepParams), P, P, P, D, P, P, P, P]),
 ]
 
 _lib = None

@@ -17,6 +17,8 @@ enum KernelKind { K_RESIDUAL = 0, K_MATVEC = 1, K_FDJAC = 2, K_PC_FACTOR = 3, K_
 void prof_begin(int kind, cudaStream_t s);
 void prof_end(int kind, cudaStream_t s);
 void prof_flush();
+// Count one launch of `kind` without the profiler's events (for code that must not create any).
+void count_launch(int kind);
 #define DV_LAUNCH(kind, stream, ...)      \
     do {                                  \
         dv::prof_begin(kind, stream);     \

@@ -3,6 +3,8 @@
 #include "dv_internal.h"
 #include "dv_residual.cuh"
 
+#include <mutex>
+
 namespace dv {
 
 RecLayout rec_layout(const dv_step_params& p) {
@@ -311,3 +313,76 @@ int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0,
 }
 
 }  // namespace dv
+
+// ---------------------------------------------------------------- allocation-free residual + accumulators
+// dv_rhs_acc_noalloc evaluates f = dy/dt and the accumulator rates without a dv_model, so without
+// any device allocation.  It exists for callers that may not allocate device memory once they are
+// running: a plant controller or state estimator that reserves its device memory at start-up and
+// forbids allocation inside its loop, or a host framework whose allocator owns the device and
+// does not let plugins call cudaMalloc.  dv_model_create allocates the model's workspaces, so
+// those callers cannot use dv_rhs.  The face and wall records that dv_rhs keeps in the model live
+// here in one file-scope device array instead, shared by every call on the device.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 2u << 20;    // 2 MiB per device, held until process exit
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+// Device address of g_noalloc_scratch per device, looked up once with that device current (in
+// host code the symbol names a host-side shadow, never a device address).
+static double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+static std::mutex g_noalloc_mu;
+
+}  // namespace
+
+extern "C" int dv_rhs_acc_noalloc(const dv_step_params* p, const double* feed_flux, const double* n_nom,
+                                  const double* coverage, double t, const double* y, double* f, double* acc,
+                                  void* stream) {
+    using namespace dv;
+    if (!p || !feed_flux || !n_nom || !coverage || !y || !f || !acc) {
+        set_error("dv_rhs_acc_noalloc: null argument");
+        return DV_ERR_ARG;
+    }
+    if (p->Nr < 1 || p->Nth < 1 || p->Nz < 1 || p->Nr > DV_MAX_NR) {
+        set_error("dv_rhs_acc_noalloc: bad grid size");
+        return DV_ERR_ARG;
+    }
+    const RecLayout rl = rec_layout(*p);
+    const size_t need = sizeof(double) * (size_t)rl.total;
+    if (need > kNoAllocScratchBytes) {
+        set_error("dv_rhs_acc_noalloc: the grid needs " + std::to_string(need) + " bytes of record scratch; the "
+                  "static scratch holds " + std::to_string(kNoAllocScratchBytes) + " (use dv_model_create + dv_rhs)");
+        return DV_ERR_ARG;
+    }
+    int dev = 0;
+    DV_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("dv_rhs_acc_noalloc: device index out of range");
+        return DV_ERR_ARG;
+    }
+    double* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {                   // first call on this device: look up the address
+            void* ptr = nullptr;
+            DV_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+            g_noalloc_ptr[dev] = (double*)ptr;
+        }
+        base = g_noalloc_ptr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    // The array keeps the previous call's records; records that this grid and step never write
+    // (ends without a valve, the wall of a wall-less column) must read as zero.
+    DV_CUDA(cudaMemsetAsync(base, 0, need, s));
+    Rec rec = make_rec(rl, base);
+    const int64_t nc = (int64_t)p->Nr * p->Nth * p->Nz;
+    count_launch(K_RESIDUAL);
+    k_cells<M_RHS, true><<<nblk(nc, 128), 128, 0, s>>>(*p, Aux{feed_flux, n_nom, coverage}, rec, t, y, nullptr,
+                                                      nullptr, nullptr, nullptr, 0.0, f);
+    count_launch(K_RESIDUAL);
+    k_accumulators<<<1, 256, 0, s>>>(*p, rec.bnd, rec.Qj, rec.Qa, rec.Qw, rec.Qhx, acc);
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}

@@ -52,6 +52,11 @@ void prof_begin(int kind, cudaStream_t s) {
     cudaEventRecord(g_open_ev, s);
 }
 
+void count_launch(int kind) {
+    ++g_launches;
+    ++g_prof[kind].launches;
+}
+
 void prof_end(int kind, cudaStream_t s) {
     if (!g_prof_on || !g_open_ev) return;
     cudaEvent_t b = ev_get();

@@ -231,6 +231,22 @@ const double* dv_integrator_y(const dv_integrator* g);
 /* Copy the current state into dst (device or host memory); synchronises `stream`. */
 int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream);
 
+/* ------------------------------------------------------------------ allocation-free residual
+ * No counterpart in the reference: an addition of this library.  Same results as dv_rhs with
+ * accumulators (f = dy/dt and the DV_NACC rates) for callers that must not allocate device
+ * memory while they run -- a controller or estimator that reserves its memory at start-up, or a
+ * host framework whose allocator owns the device -- and therefore cannot call dv_model_create.
+ * The caller passes the step constants (p, host) and DEVICE arrays: feed_flux and n_nom over
+ * (Nr, Ntheta), coverage over (Ntheta, Nz) (the arrays dv_model_create takes on the host), y and
+ * f (n_core), acc (DV_NACC).  The face and wall records live in a static 2 MiB device array per
+ * device (enough for 16x16x64); larger grids are rejected with DV_ERR_ARG.  The first call on a
+ * device looks up that array's address with the device current; make that first call before any
+ * stream capture.  Each call clears the part it uses on `stream` before its kernels run.  Every
+ * call on a device shares the array: calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller.  Asynchronous on `stream`. */
+int dv_rhs_acc_noalloc(const dv_step_params* p, const double* feed_flux, const double* n_nom,
+                       const double* coverage, double t, const double* y, double* f, double* acc, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
