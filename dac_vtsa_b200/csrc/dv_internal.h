@@ -57,6 +57,8 @@ struct RecLayout {
     int64_t T, P, y, qstar, uz, ur, uth, bnd, Qj, Qa, Qw, Rb, Qhx, total;
 };
 RecLayout rec_layout(const dv_step_params& p);
+// Doubles of the split residual's scratch (per-cell properties + per-face fluxes).
+int64_t split_doubles(const dv_step_params& p);
 
 }  // namespace dv
 
@@ -67,6 +69,7 @@ struct dv_model {
     dv::DevAux aux;
     dv::RecLayout rl;
     double* d_rec;                  // internal record scratch (accumulators)
+    double* d_split;                // per-cell properties and per-face fluxes of the split residual
     double* d_acc;                  // DV_NACC
     int64_t nfev;
     int64_t jac_doubles;

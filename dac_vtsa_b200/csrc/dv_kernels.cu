@@ -258,51 +258,350 @@ __global__ void __launch_bounds__(128) k_fd_jacobian(dv_step_params p, Aux aux, 
         outer_wall ? (fw - f0[(int64_t)DV_NV * nc + (int64_t)j * p.Nz + k]) / h : 0.0;
 }
 
+// ---------------------------------------------------------------- split residual
+// The residual as three launches with short per-thread chains: per-cell properties and uptake
+// (k_cprops), the flux through every face once (k_faces), per-cell divergence and sources
+// (k_assemble, through cell_tail).  Each step evaluates the same expressions on the same inputs
+// as cell_eval, so the results are the same bits; the thread-per-cell kernel computes the
+// properties of every cell seven times and every face twice.
+enum { SP_C0 = 0, SP_T = 3, SP_P, SP_CPOS, SP_Y0, SP_MU = SP_Y0 + 3, SP_KG, SP_RHO, SP_CPM, SP_DM, SP_LAM0,
+       SP_RATE0, SP_QS0 = SP_RATE0 + 2, SP_NCELL = SP_QS0 + 2 };
+
+struct Split {
+    double* cell;          // [SP_NCELL][nc]
+    double* zf;            // [4][ncol (Nz+1)]: +z flux through face kf of a column (kf 0 = top end, Nz = bottom end)
+    double* rf;            // [4][(Nr-1) Nth Nz]: +r flux between rings i and i+1 at (j, k)
+    double* tf;            // [4][Nr Nth Nz]: +theta flux between sectors j and j+1 (periodic) at (i, k)
+    int64_t nc, nzf, nrf, ntf;
+};
+
+int64_t split_doubles(const dv_step_params& p) {
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz, ncol = (int64_t)p.Nr * p.Nth;
+    return SP_NCELL * nc + 4 * (ncol * (p.Nz + 1) + (int64_t)(p.Nr - 1) * p.Nth * p.Nz + nc);
+}
+
+static Split split_of(const dv_step_params& p, double* base) {
+    Split S;
+    S.nc = (int64_t)p.Nr * p.Nth * p.Nz;
+    S.nzf = (int64_t)p.Nr * p.Nth * (p.Nz + 1);
+    S.nrf = (int64_t)(p.Nr - 1) * p.Nth * p.Nz;
+    S.ntf = S.nc;
+    S.cell = base;
+    S.zf = S.cell + SP_NCELL * S.nc;
+    S.rf = S.zf + 4 * S.nzf;
+    S.tf = S.rf + 4 * S.nrf;
+    return S;
+}
+
+static __device__ __forceinline__ void sp_get(const Split& S, int64_t c, Cell& s, Props& o) {
+    const double* a = S.cell;
+    const int64_t nc = S.nc;
+#pragma unroll
+    for (int q = 0; q < DV_NG; ++q) {
+        s.c[q] = a[(SP_C0 + q) * nc + c];
+        o.y[q] = a[(SP_Y0 + q) * nc + c];
+    }
+    s.q[0] = s.q[1] = s.e = 0.0;            // not read by the face and wall terms
+    o.T = a[SP_T * nc + c];
+    o.P = a[SP_P * nc + c];
+    o.Tp = 0.0;                             // only the uptake reads it (done in k_cprops)
+    o.Cpos = a[SP_CPOS * nc + c];
+    o.mu = a[SP_MU * nc + c];
+    o.kg = a[SP_KG * nc + c];
+    o.rho = a[SP_RHO * nc + c];
+    o.cpm = a[SP_CPM * nc + c];
+    o.Dm = a[SP_DM * nc + c];
+    o.lam0 = a[SP_LAM0 * nc + c];
+}
+
+static __device__ __forceinline__ void flux_put(double* base, int64_t stride, int64_t ix, const Flux& F) {
+#pragma unroll
+    for (int q = 0; q < DV_NG; ++q) base[q * stride + ix] = F.F[q];
+    base[DV_NG * stride + ix] = F.H;
+}
+
+static __device__ __forceinline__ void flux_get(const double* base, int64_t stride, int64_t ix, Flux& F) {
+#pragma unroll
+    for (int q = 0; q < DV_NG; ++q) F.F[q] = base[q * stride + ix];
+    F.H = base[DV_NG * stride + ix];
+}
+
+// Direction scale of the finite-difference matvec: sig = sqrt(eps) ||z|| / ||v|| (core/solver.py:196-203).
+static __device__ __forceinline__ double matvec_sig(const double* scal) {
+    return 1.4901161193847656e-08 * scal[1] / scal[0];
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
+                                               const double* __restrict__ u, const double* __restrict__ sc,
+                                               const double* __restrict__ scal) {
+    const int64_t nc = S.nc;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    Cell s;
+    if (MODE == M_MATVEC) {
+        if (scal[0] == 0.0) return;         // zero direction: k_assemble writes zeros
+        LoadDir ld{y, u, sc, matvec_sig(scal)};
+        load_cell(ld, nc, c, s);
+    } else {
+        LoadPlain ld{y};
+        load_cell(ld, nc, c, s);
+    }
+    Props o;
+    cell_props(p, s, o);
+    double rate[DV_NA], qstar[DV_NA];
+    uptake(p, s, o, rate, qstar);
+    double* a = S.cell;
+#pragma unroll
+    for (int q = 0; q < DV_NG; ++q) {
+        a[(SP_C0 + q) * nc + c] = s.c[q];
+        a[(SP_Y0 + q) * nc + c] = o.y[q];
+    }
+    a[SP_T * nc + c] = o.T;
+    a[SP_P * nc + c] = o.P;
+    a[SP_CPOS * nc + c] = o.Cpos;
+    a[SP_MU * nc + c] = o.mu;
+    a[SP_KG * nc + c] = o.kg;
+    a[SP_RHO * nc + c] = o.rho;
+    a[SP_CPM * nc + c] = o.cpm;
+    a[SP_DM * nc + c] = o.Dm;
+    a[SP_LAM0 * nc + c] = o.lam0;
+#pragma unroll
+    for (int q = 0; q < DV_NA; ++q) {
+        a[(SP_RATE0 + q) * nc + c] = rate[q];
+        a[(SP_QS0 + q) * nc + c] = qstar[q];
+    }
+}
+
+// MUSCL slope of cell kk of a column starting at cell index base (zero next to the ends).
+static __device__ __forceinline__ void sp_slope(const dv_step_params& p, const Split& S, int64_t base, int kk,
+                                                bool muscl, double s[4]) {
+    s[0] = s[1] = s[2] = s[3] = 0.0;
+    if (!muscl || kk < 1 || kk > p.Nz - 2) return;
+    const double* a = S.cell;
+    const int64_t nc = S.nc, c = base + kk;
+#pragma unroll
+    for (int q = 0; q < DV_NG; ++q) {
+        const double* cq = a + (SP_C0 + q) * nc;
+        s[q] = limited_slope(p.limiter, cq[c] - cq[c - 1], cq[c + 1] - cq[c]);
+    }
+    const double* T = a + SP_T * nc;
+    s[3] = limited_slope(p.limiter, T[c] - T[c - 1], T[c + 1] - T[c]);
+}
+
+// One thread per face: interior z faces, r faces, theta faces, then the two end faces of every
+// column (kept last so the warps of each range run one kind of face).
+template <bool REC>
+__global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S, Rec rec, double t,
+                                              const double* __restrict__ scal) {
+    if (scal && scal[0] == 0.0) return;
+    const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
+    const int64_t ncol = (int64_t)Nr * Nth;
+    const int64_t nzi = ncol * (Nz - 1);
+    const int64_t nr = (Nr > 1) ? S.nrf : 0;
+    const int64_t nt = (Nth > 1) ? S.ntf : 0;
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < nzi) {
+        const int64_t col = g / (Nz - 1);
+        const int k = (int)(g % (Nz - 1));
+        const int i = (int)(col / Nth);
+        const int64_t base = col * Nz;
+        const bool muscl = (Nz >= 3 && p.limiter != DV_LIM_UPWIND);
+        double sL[4], sR[4];
+        sp_slope(p, S, base, k, muscl, sL);
+        sp_slope(p, S, base, k + 1, muscl, sR);
+        Cell a, b;
+        Props L, R;
+        sp_get(S, base + k, a, L);
+        sp_get(S, base + k + 1, b, R);
+        Flux F;
+        double uz;
+        zface(p, i, L, R, a, b, sL, sR, muscl, aux.n_nom[col], F, &uz);
+        flux_put(S.zf, S.nzf, col * (Nz + 1) + k + 1, F);
+        if (REC) rec.uz[col * (Nz - 1) + k] = uz;
+        return;
+    }
+    g -= nzi;
+    if (g < nr) {                       // between (i, j, k) and (i+1, j, k); g = that first cell's index
+        const int i = (int)(g / ((int64_t)Nth * Nz));
+        Cell a, b;
+        Props A, B;
+        sp_get(S, g, a, A);
+        sp_get(S, g + (int64_t)Nth * Nz, b, B);
+        Flux F;
+        double ur;
+        tface(p, A, B, a, b, p.drc[i], p.Ar[i], F, &ur);
+        flux_put(S.rf, S.nrf, g, F);
+        if (REC) rec.ur[g] = ur;
+        return;
+    }
+    g -= nr;
+    if (g < nt) {                       // between (i, j, k) and (i, j+1 mod Nth, k); g = the first cell
+        const int k = (int)(g % Nz);
+        const int64_t r = g / Nz;
+        const int j = (int)(r % Nth);
+        const int i = (int)(r / Nth);
+        const int jp = (j == Nth - 1) ? 0 : j + 1;
+        Cell a, b;
+        Props A, B;
+        sp_get(S, g, a, A);
+        sp_get(S, ((int64_t)i * Nth + jp) * Nz + k, b, B);
+        Flux F;
+        double ut;
+        tface(p, A, B, a, b, p.arc[i], p.Ath[i], F, &ut);
+        flux_put(S.tf, S.ntf, g, F);
+        if (REC) rec.uth[g] = ut;
+        return;
+    }
+    g -= nt;
+    if (g < 2 * ncol) {
+        const int e = (int)(g / ncol);
+        const int64_t col = g % ncol;
+        const int i = (int)(col / Nth);
+        const int64_t c = col * Nz + (e == 0 ? 0 : Nz - 1);
+        Cell s;
+        Props o;
+        sp_get(S, c, s, o);
+        double F_in[DV_NG], H_in;
+        end_face(p, p.ends[e], t, i, s, o, aux.feed_flux[col], F_in, H_in,
+                 REC ? rec.bnd + (int64_t)e * BR_N * ncol + col : nullptr, ncol);
+        Flux F;                           // stored as the +z flux through the face
+#pragma unroll
+        for (int q = 0; q < DV_NG; ++q) F.F[q] = (e == 0) ? F_in[q] : -F_in[q];
+        F.H = (e == 0) ? H_in : -H_in;
+        flux_put(S.zf, S.nzf, col * (Nz + 1) + (e == 0 ? 0 : Nz), F);
+    }
+}
+
+template <int MODE, bool REC>
+__global__ void __launch_bounds__(64) k_assemble(dv_step_params p, Aux aux, Split S, Rec rec, double t,
+                                                 const double* __restrict__ y, const double* __restrict__ u,
+                                                 const double* __restrict__ sc, const double* __restrict__ f0,
+                                                 const double* __restrict__ scal, double gh,
+                                                 double* __restrict__ out) {
+    const int64_t nc = S.nc;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    int i, j, k;
+    cell_ijk(p, c, i, j, k);
+    const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
+    const bool outer_wall = (i == Nr - 1) && p.wall_on;
+    const int64_t iw = (int64_t)DV_NV * nc + (int64_t)j * Nz + k;
+    if (MODE == M_MATVEC && scal[0] == 0.0) {      // matvec of a zero direction is zero
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) out[v * nc + c] = 0.0;
+        if (outer_wall) out[iw] = 0.0;
+        return;
+    }
+    Cell s0;
+    Props P0;
+    sp_get(S, c, s0, P0);
+    double rate[DV_NA], qstar[DV_NA];
+#pragma unroll
+    for (int q = 0; q < DV_NA; ++q) {
+        rate[q] = S.cell[(SP_RATE0 + q) * nc + c];
+        qstar[q] = S.cell[(SP_QS0 + q) * nc + c];
+    }
+    const int64_t col = (int64_t)i * Nth + j;
+    Flux Fzm, Fzp, Frm, Frp, Ftm, Ftp;
+    flux_get(S.zf, S.nzf, col * (Nz + 1) + k, Fzm);
+    flux_get(S.zf, S.nzf, col * (Nz + 1) + k + 1, Fzp);
+    if (Nr > 1) {
+        if (i > 0) flux_get(S.rf, S.nrf, c - (int64_t)Nth * Nz, Frm);
+        if (i < Nr - 1) flux_get(S.rf, S.nrf, c, Frp);
+    }
+    if (Nth > 1) {
+        const int jm = (j == 0) ? Nth - 1 : j - 1;
+        flux_get(S.tf, S.ntf, ((int64_t)i * Nth + jm) * Nz + k, Ftm);
+        flux_get(S.tf, S.ntf, c, Ftp);
+    }
+    double f[DV_NV], fw = 0.0;
+    if (MODE == M_MATVEC) {
+        const double sig = matvec_sig(scal);
+        LoadDir ld{y, u, sc, sig};
+        cell_tail(p, aux, ld, t, i, j, k, P0, rate, qstar, Fzm, Fzp, Frm, Frp, Ftm, Ftp, f,
+                  outer_wall ? &fw : nullptr, REC ? &rec : nullptr);
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) {
+            const int64_t ix = v * nc + c;
+            const double vv = u[ix] * sc[ix];
+            out[ix] = (vv - gh * (f[v] - f0[ix]) / sig) / sc[ix];
+        }
+        if (outer_wall) {
+            const double vv = u[iw] * sc[iw];
+            out[iw] = (vv - gh * (fw - f0[iw]) / sig) / sc[iw];
+        }
+        return;
+    }
+    LoadPlain ld{y};
+    cell_tail(p, aux, ld, t, i, j, k, P0, rate, qstar, Fzm, Fzp, Frm, Frp, Ftm, Ftp, f,
+              outer_wall ? &fw : nullptr, REC ? &rec : nullptr);
+    if (MODE == M_RHS) {
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) out[v * nc + c] = f[v];
+        if (outer_wall) out[iw] = fw;
+    } else {
+#pragma unroll
+        for (int v = 0; v < DV_NV; ++v) {
+            const int64_t ix = v * nc + c;
+            out[ix] = y[ix] - gh * f[v] - u[ix];
+        }
+        if (outer_wall) out[iw] = y[iw] - gh * fw - u[iw];
+    }
+}
+
 static Aux aux_of(const dv_model* m) { return Aux{m->aux.feed_flux, m->aux.n_nom, m->aux.cov}; }
 
 static unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
 
-int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, cudaStream_t s) {
-    Rec rec = make_rec(m->rl, m->d_rec);
-    if (acc) {
-        DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
-                                                              nullptr, 0.0, f));
-        DV_LAUNCH(dv::K_RESIDUAL, s, k_accumulators<<<1, 256, 0, s>>>(m->p, rec.bnd, rec.Qj, rec.Qa, rec.Qw, rec.Qhx, acc));
-    } else {
-        DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_RHS, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
-                                                               nullptr, 0.0, f));
-    }
+// The split residual: properties, faces, assembly (three launches counted under `kind`).
+template <int MODE, bool REC>
+static int split_residual(dv_model* m, const Rec& rec, double t, const double* y, const double* u, const double* sc,
+                          const double* f0, const double* scal, double gh, double* out, cudaStream_t s, int kind) {
+    const dv_step_params& p = m->p;
+    const Split S = split_of(p, m->d_split);
+    const int64_t ncol = (int64_t)p.Nr * p.Nth;
+    const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
+    DV_LAUNCH(kind, s, k_cprops<MODE><<<nblk(m->nc, 64), 64, 0, s>>>(p, S, y, u, sc, scal));
+    DV_LAUNCH(kind, s, k_faces<REC><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t,
+                                                                  MODE == M_MATVEC ? scal : nullptr));
+    DV_LAUNCH(kind, s, k_assemble<MODE, REC><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t, y, u, sc, f0,
+                                                                           scal, gh, out));
     m->nfev += 1;
     DV_CUDA(cudaGetLastError());
     return DV_OK;
+}
+
+int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, cudaStream_t s) {
+    Rec rec = make_rec(m->rl, m->d_rec);
+    if (acc) {
+        int rc = split_residual<M_RHS, true>(m, rec, t, y, nullptr, nullptr, nullptr, nullptr, 0.0, f, s,
+                                             dv::K_RESIDUAL);
+        if (rc != DV_OK) return rc;
+        DV_LAUNCH(dv::K_RESIDUAL, s, k_accumulators<<<1, 256, 0, s>>>(m->p, rec.bnd, rec.Qj, rec.Qa, rec.Qw, rec.Qhx, acc));
+        DV_CUDA(cudaGetLastError());
+        return DV_OK;
+    }
+    return split_residual<M_RHS, false>(m, rec, t, y, nullptr, nullptr, nullptr, nullptr, 0.0, f, s, dv::K_RESIDUAL);
 }
 
 int launch_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known,
                           double* R, cudaStream_t s) {
     Rec rec = make_rec(m->rl, m->d_rec);
-    DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_STAGE, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, rhs_known, nullptr, nullptr,
-                                                             nullptr, gamma_h, R));
-    m->nfev += 1;
-    DV_CUDA(cudaGetLastError());
-    return DV_OK;
+    return split_residual<M_STAGE, false>(m, rec, t, y, rhs_known, nullptr, nullptr, nullptr, gamma_h, R, s,
+                                          dv::K_RESIDUAL);
 }
 
 int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream_t s) {
-    Rec rec = make_rec(m->rl, diag);
-    DV_LAUNCH(dv::K_RESIDUAL, s, k_cells<M_RHS, true><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, y, nullptr, nullptr, nullptr,
-                                                          nullptr, 0.0, m->d_rec));   // f discarded into scratch
-    m->nfev += 1;
-    DV_CUDA(cudaGetLastError());
-    return DV_OK;
+    Rec rec = make_rec(m->rl, diag);      // f is discarded into the model's record scratch
+    return split_residual<M_RHS, true>(m, rec, t, y, nullptr, nullptr, nullptr, nullptr, 0.0, m->d_rec, s,
+                                       dv::K_RESIDUAL);
 }
 
 int launch_matvec(dv_model* m, double t, const double* z, const double* u, const double* sc, const double* f0,
                   double dh, const double* scal, double* out, cudaStream_t s) {
     Rec rec = make_rec(m->rl, m->d_rec);
-    DV_LAUNCH(dv::K_MATVEC, s, k_cells<M_MATVEC, false><<<nblk(m->nc, 128), 128, 0, s>>>(m->p, aux_of(m), rec, t, z, u, sc, f0, scal, dh, out));
-    m->nfev += 1;
-    DV_CUDA(cudaGetLastError());
-    return DV_OK;
+    return split_residual<M_MATVEC, false>(m, rec, t, z, u, sc, f0, scal, dh, out, s, dv::K_MATVEC);
 }
 
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s) {

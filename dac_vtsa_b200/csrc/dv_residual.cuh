@@ -65,6 +65,103 @@ static __device__ __forceinline__ void slope4(int lim, const Cell& m, const doub
     s[3] = limited_slope(lim, To - Tm, Tp - To);
 }
 
+// Divergence of the face fluxes, sorption sinks, wall / jacket / exchanger terms and records of
+// cell (i,j,k) (core/residual.py:298-365): f[0..5]; *fw = dTw/dt of its wall node.  Shared by the
+// thread-per-cell residual and the split residual's assembly, so both add in the same order.
+template <class L>
+static __device__ __forceinline__ void cell_tail(const dv_step_params& p, const Aux& aux, const L& ld, double t, int i,
+                                                 int j, int k, const Props& P0, const double rate[DV_NA],
+                                                 const double qstar[DV_NA], const Flux& Fzm, const Flux& Fzp,
+                                                 const Flux& Frm, const Flux& Frp, const Flux& Ftm, const Flux& Ftp,
+                                                 double f[DV_NV], double* fw, const Rec* rec) {
+    const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
+    const int64_t nc = (int64_t)Nr * Nth * Nz;
+    const int64_t c0 = ((int64_t)i * Nth + j) * Nz + k;
+    const int64_t off_w = (int64_t)DV_NV * nc;
+    // ---------------- divergence (physics/mass.py:61-74) and species balance
+    const double V = p.V[i];
+#pragma unroll
+    for (int q = 0; q < DV_NG; ++q) {
+        double d = Fzp.F[q] - Fzm.F[q];
+        if (Nr > 1) {
+            if (i < Nr - 1) d = d + Frp.F[q];
+            if (i > 0) d = d - Frm.F[q];
+        }
+        if (Nth > 1) d = d + (Ftp.F[q] - Ftm.F[q]);
+        double sink = (q < DV_NA) ? rate[q] : 0.0;
+        f[q] = -d / (p.eps_t * V) - (p.rho_b / p.eps_t) * sink;
+    }
+    f[3] = rate[0];
+    f[4] = rate[1];
+    double de = Fzp.H - Fzm.H;
+    if (Nr > 1) {
+        if (i < Nr - 1) de = de + Frp.H;
+        if (i > 0) de = de - Frm.H;
+    }
+    if (Nth > 1) de = de + (Ftp.H - Ftm.H);
+    // ---------------- wall / jacket / exchanger (core/residual.py:328-359)
+    double src = 0.0;
+    const double Tj = jacket_T(p, t);
+    if (i == Nr - 1) {
+        const int64_t wn = (int64_t)j * Nz + k;
+        const double cov = aux.cov[wn];
+        const double To = P0.T;
+        const double R_bed = wall_R_bed(p, P0);
+        double Q_jac, Q_amb, Q_wb;
+        if (p.wall_on) {
+            const double Tw = ld(off_w + wn);
+            Q_jac = p.jacket_on ? cov * p.h_jac * p.A_wall_out * (Tj - Tw) : 0.0;
+            Q_amb = (1.0 - cov) * p.h_amb * p.A_wall_out * (p.T_amb - Tw);
+            Q_wb = p.A_wall_in * (Tw - To) / R_bed;
+            double cond = 0.0;
+            if (Nz > 1) {
+                if (k < Nz - 1) cond = cond + p.wall_kz * (ld(off_w + wn + 1) - Tw);
+                if (k > 0) cond = cond - p.wall_kz * (Tw - ld(off_w + wn - 1));
+            }
+            if (Nth > 1) {
+                const int jm = (j == 0) ? Nth - 1 : j - 1;
+                const int jp = (j == Nth - 1) ? 0 : j + 1;
+                const double Twp = ld(off_w + (int64_t)jp * Nz + k);
+                const double Twm = ld(off_w + (int64_t)jm * Nz + k);
+                cond = cond + p.wall_kt * (Twp - Tw);
+                cond = cond - p.wall_kt * (Tw - Twm);
+            }
+            if (fw) *fw = (Q_jac + Q_amb - Q_wb + cond) / p.wall_C;
+        } else {
+            if (p.jacket_on && p.h_jac > 0.0) {
+                double R_j = p.lumped ? R_bed : R_bed + 1.0 / p.h_jac;
+                Q_jac = cov * p.A_wall_in * (Tj - To) / R_j;
+            } else {
+                Q_jac = 0.0;
+            }
+            Q_amb = (p.h_amb > 0.0) ? (1.0 - cov) * p.A_wall_in * (p.T_amb - To) / (R_bed + 1.0 / p.h_amb) : 0.0;
+            Q_wb = Q_jac + Q_amb;
+        }
+        src = src + Q_wb;
+        if (rec) {
+            rec->Qj[wn] = Q_jac;
+            rec->Qa[wn] = Q_amb;
+            rec->Qw[wn] = Q_wb;
+            rec->Rb[wn] = R_bed;
+        }
+    }
+    double Q_hx = 0.0;
+    if (p.hx_on) {
+        Q_hx = p.hA_v * V * (Tj - P0.T);
+        src = src + Q_hx;
+    }
+    f[5] = (-de + src) / V;
+    if (rec) {
+        rec->Qhx[c0] = Q_hx;
+        rec->T[c0] = P0.T;
+        rec->P[c0] = P0.P;
+#pragma unroll
+        for (int q = 0; q < DV_NG; ++q) rec->y[q * nc + c0] = P0.y[q];
+        rec->qstar[c0] = qstar[0];
+        rec->qstar[nc + c0] = qstar[1];
+    }
+}
+
 // f[0..5] = d(c, q, e)/dt of cell (i,j,k); *fw = dTw/dt of its wall node (outer ring, wall on).
 template <class L>
 static __device__ void cell_eval(const dv_step_params& p, const Aux& aux, const L& ld, double t, int i, int j, int k,
@@ -72,7 +169,6 @@ static __device__ void cell_eval(const dv_step_params& p, const Aux& aux, const 
     const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
     const int64_t nc = (int64_t)Nr * Nth * Nz;
     const int64_t c0 = ((int64_t)i * Nth + j) * Nz + k;
-    const int64_t off_w = (int64_t)DV_NV * nc;
     Cell s0;
     load_cell(ld, nc, c0, s0);
     Props P0;
@@ -166,88 +262,7 @@ static __device__ void cell_eval(const dv_step_params& p, const Aux& aux, const 
         tface(p, P0, Pb, s0, sb, p.arc[i], p.Ath[i], Ftp, &ut);
         if (rec) rec->uth[c0] = ut;
     }
-    // ---------------- divergence (physics/mass.py:61-74) and species balance
-    const double V = p.V[i];
-#pragma unroll
-    for (int q = 0; q < DV_NG; ++q) {
-        double d = Fzp.F[q] - Fzm.F[q];
-        if (Nr > 1) {
-            if (i < Nr - 1) d = d + Frp.F[q];
-            if (i > 0) d = d - Frm.F[q];
-        }
-        if (Nth > 1) d = d + (Ftp.F[q] - Ftm.F[q]);
-        double sink = (q < DV_NA) ? rate[q] : 0.0;
-        f[q] = -d / (p.eps_t * V) - (p.rho_b / p.eps_t) * sink;
-    }
-    f[3] = rate[0];
-    f[4] = rate[1];
-    double de = Fzp.H - Fzm.H;
-    if (Nr > 1) {
-        if (i < Nr - 1) de = de + Frp.H;
-        if (i > 0) de = de - Frm.H;
-    }
-    if (Nth > 1) de = de + (Ftp.H - Ftm.H);
-    // ---------------- wall / jacket / exchanger (core/residual.py:328-359)
-    double src = 0.0;
-    const double Tj = jacket_T(p, t);
-    if (i == Nr - 1) {
-        const int64_t wn = (int64_t)j * Nz + k;
-        const double cov = aux.cov[wn];
-        const double To = P0.T;
-        const double R_bed = wall_R_bed(p, P0);
-        double Q_jac, Q_amb, Q_wb;
-        if (p.wall_on) {
-            const double Tw = ld(off_w + wn);
-            Q_jac = p.jacket_on ? cov * p.h_jac * p.A_wall_out * (Tj - Tw) : 0.0;
-            Q_amb = (1.0 - cov) * p.h_amb * p.A_wall_out * (p.T_amb - Tw);
-            Q_wb = p.A_wall_in * (Tw - To) / R_bed;
-            double cond = 0.0;
-            if (Nz > 1) {
-                if (k < Nz - 1) cond = cond + p.wall_kz * (ld(off_w + wn + 1) - Tw);
-                if (k > 0) cond = cond - p.wall_kz * (Tw - ld(off_w + wn - 1));
-            }
-            if (Nth > 1) {
-                const int jm = (j == 0) ? Nth - 1 : j - 1;
-                const int jp = (j == Nth - 1) ? 0 : j + 1;
-                const double Twp = ld(off_w + (int64_t)jp * Nz + k);
-                const double Twm = ld(off_w + (int64_t)jm * Nz + k);
-                cond = cond + p.wall_kt * (Twp - Tw);
-                cond = cond - p.wall_kt * (Tw - Twm);
-            }
-            if (fw) *fw = (Q_jac + Q_amb - Q_wb + cond) / p.wall_C;
-        } else {
-            if (p.jacket_on && p.h_jac > 0.0) {
-                double R_j = p.lumped ? R_bed : R_bed + 1.0 / p.h_jac;
-                Q_jac = cov * p.A_wall_in * (Tj - To) / R_j;
-            } else {
-                Q_jac = 0.0;
-            }
-            Q_amb = (p.h_amb > 0.0) ? (1.0 - cov) * p.A_wall_in * (p.T_amb - To) / (R_bed + 1.0 / p.h_amb) : 0.0;
-            Q_wb = Q_jac + Q_amb;
-        }
-        src = src + Q_wb;
-        if (rec) {
-            rec->Qj[wn] = Q_jac;
-            rec->Qa[wn] = Q_amb;
-            rec->Qw[wn] = Q_wb;
-            rec->Rb[wn] = R_bed;
-        }
-    }
-    double Q_hx = 0.0;
-    if (p.hx_on) {
-        Q_hx = p.hA_v * V * (Tj - P0.T);
-        src = src + Q_hx;
-    }
-    f[5] = (-de + src) / V;
-    if (rec) {
-        rec->Qhx[c0] = Q_hx;
-        rec->T[c0] = P0.T;
-        rec->P[c0] = P0.P;
-#pragma unroll
-        for (int q = 0; q < DV_NG; ++q) rec->y[q * nc + c0] = P0.y[q];
-        rec->qstar[c0] = qstar[0];
-        rec->qstar[nc + c0] = qstar[1];
-    }
+    cell_tail(p, aux, ld, t, i, j, k, P0, rate, qstar, Fzm, Fzp, Frm, Frp, Ftm, Ftp, f, fw, rec);
 }
 
 }  // namespace dv

@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 #include "dv_internal.h"
+
+#include <utility>
 #include "dv_physics.cuh"
 
 namespace dv {
@@ -261,7 +263,7 @@ __global__ void k_cons(dv_step_params p, const double* __restrict__ R, const dou
                     acc += p.eps_t * V * x[m * nc + c];
                     if (m < DV_NA) acc += p.rho_b * V * x[(DV_NG + m) * nc + c];
                 } else {
-                    acc += V * x[(int64_t)DV_NV * nc + c];
+                    acc += V * x[(int64_t)(DV_NG + DV_NA) * nc + c];      // e block
                 }
             }
             if (m == DV_NG)
@@ -299,6 +301,19 @@ __global__ void k_err_vec(int64_t n, const double* __restrict__ y, const double*
 }
 
 // ---------------------------------------------------------------- workspace
+// Test aid: with DVTSA_FILL=<byte>[,<mask>] in the environment, newly allocated workspaces are
+// filled with that byte (mask bits: 1 model, 2 Krylov workspace, 4 integrator, 8 pinned host
+// buffers; default all).  A result that changes with the byte reads memory nothing wrote.
+static void debug_fill(void* p, size_t bytes, int group, bool host = false) {
+    const char* e = getenv("DVTSA_FILL");
+    if (!e || !p) return;
+    int byte = 0, mask = 15;
+    if (sscanf(e, "%i,%i", &byte, &mask) < 1) return;
+    if (!(mask & group)) return;
+    if (host) memset(p, byte & 0xff, bytes);
+    else cudaMemset(p, byte & 0xff, bytes);
+}
+
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
     W.n = n;
     W.kdim = kdim;
@@ -311,6 +326,16 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
         return cuda_fail(cudaGetLastError(), "cudaMalloc(Krylov workspace)");
     if (cudaMallocHost((void**)&W.hpin, sizeof(double) * 4 * (kdim + 8)) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMallocHost");
+    {
+        const size_t d = sizeof(double);
+        std::pair<double*, int64_t> bufs[] = {{W.V, (kdim + 1) * n}, {W.w, n}, {W.u, n}, {W.x, n}, {W.r, n}, {W.b, n},
+                                              {W.s, n}, {W.z, n}, {W.f, n}, {W.R, n}, {W.dz, n}, {W.zt, n}, {W.ft, n},
+                                              {W.Rt, n}, {W.tmp, n}, {W.best, n},
+                                              {W.part, (int64_t)W.nparts * (kdim + 2)}, {W.scal, 16},
+                                              {W.hbuf, 4 * (kdim + 2)}, {W.ybuf, kdim + 2}, {W.J, jac_doubles}};
+        for (auto& b : bufs) debug_fill(b.first, d * (size_t)b.second, 2);
+        debug_fill(W.hpin, d * 4 * (kdim + 8), 8, true);
+    }
     return DV_OK;
 }
 
@@ -800,7 +825,7 @@ int dv_device_count(int* n) {
 
 int dv_model_destroy(dv_model* m) {
     if (!m) return DV_OK;
-    void* ptrs[] = {m->d_aux, m->d_rec, m->d_acc, m->d_pc, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
+    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_acc, m->d_pc, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
                     m->d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -839,6 +864,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
     bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_split, sizeof(double) * split_doubles(*p)) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
@@ -851,6 +877,13 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
         dv_model_destroy(m);
         return rc;
     }
+    debug_fill(m->d_rec, sizeof(double) * rec_n, 1);
+    debug_fill(m->d_split, sizeof(double) * split_doubles(*p), 1);
+    debug_fill(m->d_acc, sizeof(double) * DV_NACC, 1);
+    debug_fill(m->d_pc, sizeof(double) * pc_need, 1);
+    debug_fill(m->d_pc_work, sizeof(double) * work_need, 1);
+    debug_fill(m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb, 1);
+    debug_fill(m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts, 1);
     m->W = new Work();
     int rc = work_alloc(*m->W, m->n, 30, m->jac_doubles);
     if (rc != DV_OK) {
@@ -976,6 +1009,9 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
         dv_integrator_destroy(g);
         return rc;
     }
+    for (double** v : vecs) debug_fill(*v, sizeof(double) * g->n, 4);
+    debug_fill(g->d_g, sizeof(double) * 3 * DV_NACC, 4);
+    debug_fill(g->h_g, sizeof(double) * 3 * DV_NACC, 8, true);
     *out = g;
     return DV_OK;
 }

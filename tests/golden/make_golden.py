@@ -197,9 +197,12 @@ def make_bench_state(ref_root, t_mid=4000.0):
     st.T = T
     st.Tw = np.full(g.wall_shape, 288.0)
     m = TVSAModel(cfg, g, props, cfg.cycle[0], st)
-    res = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * 8000.0).integrate(m.pack(st), t_mid, [t_mid])
+    ts = [0.0]
+    res = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * 8000.0).integrate(
+        m.pack(st), t_mid, [t_mid], on_step=lambda t, y, a: ts.append(t))
     np.savez_compressed(os.path.join(HERE, "bench_state_8x8x32_ads4000.npz"), y=res.y, t=res.t,
-                        over=np.array(json.dumps(over)), n_steps=res.n_steps, wall=res.wall_time)
+                        over=np.array(json.dumps(over)), n_steps=res.n_steps, wall=res.wall_time,
+                        h_last=np.diff(ts)[-3:])
     print("bench state written:", res.n_steps, "steps,", res.wall_time, "s")
 
 
@@ -235,12 +238,13 @@ def make_bench_state_heating(ref_root, t_heat=4000.0):
         print(sr.name, sr.duration, "s", sr.solver, sr.wall_time, "s", flush=True)
     step = cfg.cycle[2]
     m = TVSAModel(cfg, g, props, step, st, T_prev)
+    ts = [0.0]
     res = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * float(step["duration"])).integrate(
-        m.pack(st), t_heat, [t_heat])
+        m.pack(st), t_heat, [t_heat], on_step=lambda t, y, a: ts.append(t))
     print(step["name"], res.n_steps, "steps", res.wall_time, "s", flush=True)
     np.savez_compressed(os.path.join(HERE, "bench_state_8x8x32_heat4000.npz"), y=res.y, t=res.t,
                         T_jacket=float(m.T_jacket(t_heat)), over=np.array(json.dumps(over)),
-                        n_steps=res.n_steps, wall=res.wall_time)
+                        n_steps=res.n_steps, wall=res.wall_time, h_last=np.diff(ts)[-3:])
     print("heating bench state written")
 
 

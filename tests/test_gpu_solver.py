@@ -126,3 +126,23 @@ def test_free_running_adsorption_matches_reference_to_tolerance():
         resid = (inv1[f"tot_{s}"] - inv0[f"tot_{s}"]) - (fin - fout)
         scale = max(abs(fin), abs(fout), abs(inv0[f"tot_{s}"]), abs(inv1[f"tot_{s}"]))
         assert abs(resid) / scale < 1e-4
+
+
+def test_results_do_not_depend_on_unwritten_memory(monkeypatch):
+    """The same 200 s adsorption with every new workspace pre-filled by different bytes (zeros, a
+    huge finite value, NaN) gives bit-identical states and solver statistics: no kernel or host step
+    reads memory that nothing wrote (such a read once let the energy balance test pick up bytes past
+    the end of the residual vector)."""
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.solver import TRBDF2
+    runs = []
+    for fill in ("0x00", "0x7f", "0xff"):
+        monkeypatch.setenv("DVTSA_FILL", fill)
+        d, m, cfg, meta = _c0_model(TVSAModel)
+        dur = meta["duration"]
+        integ = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur)
+        res = integ.integrate(d["s0_y0"], dur, [dur])
+        runs.append((res.y, res.n_steps, res.n_krylov, dict(integ.stats)))
+    for y, n_steps, n_krylov, stats in runs[1:]:
+        assert np.array_equal(y, runs[0][0])
+        assert (n_steps, n_krylov, stats) == runs[0][1:]
