@@ -19,6 +19,7 @@ void prof_end(int kind, cudaStream_t s);
 void prof_flush();
 // Count one launch of `kind` without the profiler's events (for code that must not create any).
 void count_launch(int kind);
+void count_launches(int kind, int64_t n);
 #define DV_LAUNCH(kind, stream, ...)      \
     do {                                  \
         dv::prof_begin(kind, stream);     \
@@ -42,6 +43,15 @@ struct Work {
     double* hpin = nullptr;       // pinned host mirror of small results
     double* J = nullptr;          // Jacobian storage used by in-stage refreshes
     int nparts = 0;
+    // device-driven GMRES: one CUDA graph per workspace (built at first use), its device state
+    double *vin = nullptr, *wout = nullptr;   // normalised basis vector in / operator output
+    void* gm = nullptr;                       // device GMRES state
+    void* gm_host = nullptr;                  // pinned host mirror of it
+    cudaGraph_t gm_graph = nullptr;
+    cudaGraphExec_t gm_exec = nullptr;
+    cudaStream_t gm_cs = nullptr;             // capture stream
+    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0;
+    int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
 void work_free(Work& W);
@@ -102,4 +112,10 @@ int64_t precond_doubles(int nb, int nparts, int Nz);
 int64_t precond_work_doubles(int nb, int nparts, int Nz);
 // x = diag(1/sc) M^-1 diag(sc) b  (sc may be NULL: plain solve)
 int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);
+// The same launches without launch accounting or attribute changes, for stream capture (the
+// attributes are set by an earlier precond_apply).  Returns the number of kernels launched.
+int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);
+// FD matvec of the split residual for stream capture: t and gh are read from dargs[0..1] (device).
+int matvec_capture(dv_model* m, const double* dargs, const double* z, const double* u, const double* sc,
+                   const double* f0, const double* scal, double* out, cudaStream_t s);
 }  // namespace dv

@@ -393,8 +393,9 @@ static __device__ __forceinline__ void sp_slope(const dv_step_params& p, const S
 // column (kept last so the warps of each range run one kind of face).
 template <bool REC>
 __global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S, Rec rec, double t,
-                                              const double* __restrict__ scal) {
+                                              const double* __restrict__ scal, const double* __restrict__ dargs) {
     if (scal && scal[0] == 0.0) return;
+    if (dargs) t = dargs[0];
     const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
     const int64_t ncol = (int64_t)Nr * Nth;
     const int64_t nzi = ncol * (Nz - 1);
@@ -478,10 +479,14 @@ __global__ void __launch_bounds__(64) k_assemble(dv_step_params p, Aux aux, Spli
                                                  const double* __restrict__ y, const double* __restrict__ u,
                                                  const double* __restrict__ sc, const double* __restrict__ f0,
                                                  const double* __restrict__ scal, double gh,
-                                                 double* __restrict__ out) {
+                                                 double* __restrict__ out, const double* __restrict__ dargs) {
     const int64_t nc = S.nc;
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
+    if (dargs) {                  // launched from a CUDA graph: time and step factor live on the device
+        t = dargs[0];
+        gh = dargs[1];
+    }
     int i, j, k;
     cell_ijk(p, c, i, j, k);
     const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
@@ -564,9 +569,9 @@ static int split_residual(dv_model* m, const Rec& rec, double t, const double* y
     const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
     DV_LAUNCH(kind, s, k_cprops<MODE><<<nblk(m->nc, 64), 64, 0, s>>>(p, S, y, u, sc, scal));
     DV_LAUNCH(kind, s, k_faces<REC><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t,
-                                                                  MODE == M_MATVEC ? scal : nullptr));
+                                                                  MODE == M_MATVEC ? scal : nullptr, nullptr));
     DV_LAUNCH(kind, s, k_assemble<MODE, REC><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t, y, u, sc, f0,
-                                                                           scal, gh, out));
+                                                                           scal, gh, out, nullptr));
     m->nfev += 1;
     DV_CUDA(cudaGetLastError());
     return DV_OK;
@@ -602,6 +607,21 @@ int launch_matvec(dv_model* m, double t, const double* z, const double* u, const
                   double dh, const double* scal, double* out, cudaStream_t s) {
     Rec rec = make_rec(m->rl, m->d_rec);
     return split_residual<M_MATVEC, false>(m, rec, t, z, u, sc, f0, scal, dh, out, s, dv::K_MATVEC);
+}
+
+int matvec_capture(dv_model* m, const double* dargs, const double* z, const double* u, const double* sc,
+                   const double* f0, const double* scal, double* out, cudaStream_t s) {
+    const dv_step_params& p = m->p;
+    const Split S = split_of(p, m->d_split);
+    const Rec rec = make_rec(m->rl, m->d_rec);
+    const int64_t ncol = (int64_t)p.Nr * p.Nth;
+    const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
+    k_cprops<M_MATVEC><<<nblk(m->nc, 64), 64, 0, s>>>(p, S, z, u, sc, scal);
+    k_faces<false><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, scal, dargs);
+    k_assemble<M_MATVEC, false><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, z, u, sc, f0, scal, 0.0,
+                                                             out, dargs);
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
 }
 
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s) {

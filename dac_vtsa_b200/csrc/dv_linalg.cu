@@ -815,4 +815,22 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
     return DV_OK;
 }
 
+int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s) {
+    PcGeom g = geom_of(m, m->pc_mode == 0 ? 0 : 1);
+    const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
+    const int nj = g.ld / PA_LANES;
+    if (g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7)) {
+        switch (nj) {
+            case 1: k_pc_apply<1><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
+            case 3: k_pc_apply<3><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
+            case 5: k_pc_apply<5><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
+            default: k_pc_apply<7><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
+        }
+    } else {
+        k_pc_apply_glob<<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work);
+    }
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
 }  // namespace dv

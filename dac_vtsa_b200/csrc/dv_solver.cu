@@ -59,6 +59,11 @@ void count_launch(int kind) {
     ++g_prof[kind].launches;
 }
 
+void count_launches(int kind, int64_t n) {
+    g_launches += n;
+    g_prof[kind].launches += n;
+}
+
 void prof_end(int kind, cudaStream_t s) {
     if (!g_prof_on || !g_open_ev) return;
     cudaEvent_t b = ev_get();
@@ -300,6 +305,19 @@ __global__ void k_err_vec(int64_t n, const double* __restrict__ y, const double*
     }
 }
 
+// ---------------------------------------------------------------- device GMRES state
+// Everything scipy's gmres loop keeps between Arnoldi steps, on the device, so a CUDA graph can run
+// the loop without the host (see gmres_graph).  The first four doubles are written by the host
+// before each launch; the matvec kernels read t and dh from them.
+constexpr int GM_KMAX = 30;
+struct GmDev {
+    double t, dh, rtol, atol;
+    double bn2, atol_eff, ptol, presid, scale, rnorm;
+    int col, done, skip, iters, info, ncomb, pad0, pad1;
+    double H[GM_KMAX * (GM_KMAX + 1)], S[GM_KMAX + 1], gc[GM_KMAX], gs[GM_KMAX], y[GM_KMAX + 1];
+};
+static size_t gm_state_bytes() { return sizeof(GmDev); }
+
 // ---------------------------------------------------------------- workspace
 // Test aid: with DVTSA_FILL=<byte>[,<mask>] in the environment, newly allocated workspaces are
 // filled with that byte (mask bits: 1 model, 2 Krylov workspace, 4 integrator, 8 pinned host
@@ -322,8 +340,10 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
     if (A(&W.V, (kdim + 1) * n) || A(&W.w, n) || A(&W.u, n) || A(&W.x, n) || A(&W.r, n) || A(&W.b, n) ||
         A(&W.s, n) || A(&W.z, n) || A(&W.f, n) || A(&W.R, n) || A(&W.dz, n) || A(&W.zt, n) || A(&W.ft, n) ||
         A(&W.Rt, n) || A(&W.tmp, n) || A(&W.best, n) || A(&W.part, (int64_t)W.nparts * (kdim + 2)) ||
-        A(&W.scal, 16) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles))
+        A(&W.scal, 16) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles) ||
+        A(&W.vin, n) || A(&W.wout, n) || cudaMalloc(&W.gm, gm_state_bytes()) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMalloc(Krylov workspace)");
+    if (cudaMallocHost(&W.gm_host, 256) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaMallocHost");
     if (cudaMallocHost((void**)&W.hpin, sizeof(double) * 4 * (kdim + 8)) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMallocHost");
     {
@@ -332,19 +352,27 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
                                               {W.s, n}, {W.z, n}, {W.f, n}, {W.R, n}, {W.dz, n}, {W.zt, n}, {W.ft, n},
                                               {W.Rt, n}, {W.tmp, n}, {W.best, n},
                                               {W.part, (int64_t)W.nparts * (kdim + 2)}, {W.scal, 16},
-                                              {W.hbuf, 4 * (kdim + 2)}, {W.ybuf, kdim + 2}, {W.J, jac_doubles}};
+                                              {W.hbuf, 4 * (kdim + 2)}, {W.ybuf, kdim + 2}, {W.J, jac_doubles},
+                                              {W.vin, n}, {W.wout, n}};
         for (auto& b : bufs) debug_fill(b.first, d * (size_t)b.second, 2);
+        debug_fill(W.gm, gm_state_bytes(), 2);
+        debug_fill(W.gm_host, 256, 8, true);
         debug_fill(W.hpin, d * 4 * (kdim + 8), 8, true);
     }
     return DV_OK;
 }
 
 void work_free(Work& W) {
+    if (W.gm_exec) cudaGraphExecDestroy(W.gm_exec);
+    if (W.gm_graph) cudaGraphDestroy(W.gm_graph);
+    if (W.gm_cs) cudaStreamDestroy(W.gm_cs);
     double* ptrs[] = {W.V, W.w, W.u, W.x, W.r, W.b, W.s, W.z, W.f, W.R, W.dz, W.zt, W.ft, W.Rt, W.tmp, W.best,
-                      W.part, W.scal, W.hbuf, W.ybuf, W.J};
+                      W.part, W.scal, W.hbuf, W.ybuf, W.J, W.vin, W.wout};
     for (double* p : ptrs)
         if (p) cudaFree(p);
+    if (W.gm) cudaFree(W.gm);
     if (W.hpin) cudaFreeHost(W.hpin);
+    if (W.gm_host) cudaFreeHost(W.gm_host);
     W = Work();
 }
 
@@ -524,6 +552,369 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
     return DV_OK;
 }
 
+
+static int check_device_error(dv_model* m);
+
+// ---------------------------------------------------------------- device-driven GMRES
+// The loop of gmres() above as a CUDA graph: the pre-loop kernels, a conditional WHILE node whose
+// body is one Arnoldi step (normalise the previous basis vector, precondition, FD matvec, two
+// classical Gram-Schmidt passes, Givens update and the stopping test on the device), and the
+// post-loop least-squares solve, combination and true-residual check.  Same kernels and the same
+// arithmetic in the same order as gmres(), so the same bits, without a host round trip per step.
+
+__device__ __forceinline__ double std_max_d(double a, double b) { return (a < b) ? b : a; }   // std::max
+__device__ __forceinline__ double std_min_d(double a, double b) { return (b < a) ? b : a; }   // std::min
+
+// LAPACK dlartg (3.10+), as lartg() above
+__device__ void lartg_d(double f, double g, double& c, double& s, double& r) {
+    const double safmin = 2.2250738585072014e-308;          // smallest normal double
+    const double safmax = 1.0 / safmin;
+    const double rtmin = sqrt(safmin), rtmax = sqrt(safmax / 2);
+    double f1 = fabs(f), g1 = fabs(g);
+    if (g == 0.0) {
+        c = 1.0; s = 0.0; r = f;
+    } else if (f == 0.0) {
+        c = 0.0; s = copysign(1.0, g); r = g1;
+    } else if (f1 > rtmin && f1 < rtmax && g1 > rtmin && g1 < rtmax) {
+        double d = sqrt(f * f + g * g);
+        c = f1 / d;
+        r = copysign(d, f);
+        s = g / r;
+    } else {
+        double u = std_min_d(safmax, std_max_d(safmin, std_max_d(f1, g1)));
+        double fs = f / u, gs = g / u;
+        double d = sqrt(fs * fs + gs * gs);
+        c = fabs(fs) / d;
+        r = copysign(d, f);
+        s = gs / r;
+        r *= u;
+    }
+}
+
+__global__ void k_gm_init(GmDev* st, const double* __restrict__ scal, int kdim, cudaGraphConditionalHandle hnd) {
+    for (int q = threadIdx.x; q < kdim * (kdim + 1); q += blockDim.x) st->H[q] = 0.0;
+    for (int q = threadIdx.x; q <= kdim; q += blockDim.x) st->S[q] = 0.0;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double bn2 = scal[9];
+    const double atol_eff = std_max_d(st->atol, st->rtol * bn2);
+    bool skip = (bn2 == 0.0);
+    double ptol = 0.0;
+    if (!skip) {
+        ptol = bn2 * std_min_d(1.0, atol_eff / bn2);
+        if (bn2 < atol_eff) skip = true;
+    }
+    st->bn2 = bn2;
+    st->atol_eff = atol_eff;
+    st->ptol = ptol;
+    st->info = 0;
+    st->skip = skip;
+    st->done = skip;
+    st->col = 0;
+    st->iters = 0;
+    st->ncomb = 0;
+    st->presid = 0.0;
+    st->scale = skip ? 0.0 : 1.0 / bn2;      // v0 = r / ||r||
+    st->S[0] = bn2;
+    cudaGraphSetConditional(hnd, skip ? 0u : 1u);
+}
+
+// V[col] = src * scale (src = b for the first vector, else the orthogonalised operator output) and
+// its copy vin, the preconditioner's input
+__global__ void k_gm_norm(int64_t n, const GmDev* __restrict__ st, const double* __restrict__ b,
+                          const double* __restrict__ wout, double* __restrict__ V, int64_t ldv,
+                          double* __restrict__ vin) {
+    const int col = st->col;
+    const double sc = st->scale;
+    const double* src = (col == 0) ? b : wout;
+    double* v = V + (int64_t)col * ldv;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double x = sc * src[i];
+        v[i] = x;
+        vin[i] = x;
+    }
+}
+
+__global__ void k_dots_gm(int64_t n, const GmDev* __restrict__ st, const double* __restrict__ V, int64_t ldv,
+                          const double* __restrict__ w, double* __restrict__ part) {
+    __shared__ double sh[VB];
+    const int m = st->col + 1;
+    for (int q = 0; q <= m; ++q) {
+        const double* a = (q < m) ? V + q * ldv : w;
+        double acc = 0.0;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            acc += a[i] * w[i];
+        sh[threadIdx.x] = acc;
+        __syncthreads();
+        for (int s2 = VB / 2; s2 > 0; s2 >>= 1) {
+            if (threadIdx.x < s2) sh[threadIdx.x] += sh[threadIdx.x + s2];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[(int64_t)blockIdx.x * (m + 1) + q] = sh[0];
+        __syncthreads();
+    }
+}
+
+__global__ void k_dots_finish_gm(int nblk, const GmDev* __restrict__ st, const double* __restrict__ part,
+                                 double* __restrict__ out) {
+    const int m1 = st->col + 2;
+    const int q = blockIdx.x;
+    if (q >= m1) return;
+    __shared__ double sh[VB];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[(int64_t)b * m1 + q];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s2 = VB / 2; s2 > 0; s2 >>= 1) {
+        if (threadIdx.x < s2) sh[threadIdx.x] += sh[threadIdx.x + s2];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[q] = sh[0];
+}
+
+__global__ void k_orth_update_gm(int64_t n, const GmDev* __restrict__ st, const double* __restrict__ V, int64_t ldv,
+                                 const double* __restrict__ h, double* __restrict__ w) {
+    const int m = st->col + 1;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int q = 0; q < m; ++q) acc += h[q] * V[q * ldv + i];
+        w[i] -= acc;
+    }
+}
+
+// Hessenberg column, Givens rotations, residual estimate and the stopping test of gmres()
+__global__ void k_gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, cudaGraphConditionalHandle hnd) {
+    if (threadIdx.x != 0) return;
+    const double eps = 2.220446049250313e-16;                 // double epsilon
+    const int col = st->col;
+    const int m = col + 1;
+    double* H = st->H;
+    auto h = [&](int c, int k) -> double& { return H[c * (kdim + 1) + k]; };
+    const double h0 = sqrt(hh[m]);
+    for (int k = 0; k <= col; ++k) h(col, k) = hh[k] + hh[(kdim + 2) + k];
+    const double h1 = hh[2 * (kdim + 2)];
+    h(col, col + 1) = h1;
+    bool breakdown = false;
+    if (h1 <= eps * h0 || !(h1 == h1)) {
+        h(col, col + 1) = 0.0;
+        breakdown = true;
+    } else {
+        st->scale = 1.0 / h1;
+    }
+    for (int k = 0; k < col; ++k) {
+        double c = st->gc[k], s2 = st->gs[k];
+        double n0 = h(col, k), n1 = h(col, k + 1);
+        h(col, k) = c * n0 + s2 * n1;
+        h(col, k + 1) = -s2 * n0 + c * n1;
+    }
+    double c, s2, mag;
+    lartg_d(h(col, col), h(col, col + 1), c, s2, mag);
+    st->gc[col] = c;
+    st->gs[col] = s2;
+    h(col, col) = mag;
+    h(col, col + 1) = 0.0;
+    double tmp = -s2 * st->S[col];
+    st->S[col] = c * st->S[col];
+    st->S[col + 1] = tmp;
+    const double presid = fabs(tmp);
+    st->presid = presid;
+    st->iters += 1;
+    const bool stop = !(presid == presid) || presid <= st->ptol || breakdown || col + 1 == kdim;
+    if (!stop) st->col = col + 1;
+    st->done = stop;
+    cudaGraphSetConditional(hnd, stop ? 0u : 1u);
+}
+
+// least squares by back substitution (as in gmres()); ybuf = y, ncomb = its length
+__global__ void k_gm_solve(GmDev* st, double* __restrict__ ybuf, int kdim) {
+    if (threadIdx.x != 0) return;
+    if (st->skip) {
+        st->ncomb = 0;
+        return;
+    }
+    const int col = st->col;
+    double* H = st->H;
+    auto h = [&](int c, int k) -> double& { return H[c * (kdim + 1) + k]; };
+    double* S = st->S;
+    if (h(col, col) == 0.0) S[col] = 0.0;
+    double* y = st->y;
+    for (int k = 0; k <= col; ++k) y[k] = S[k];
+    for (int k = col; k > 0; --k) {
+        if (y[k] != 0.0) {
+            y[k] /= h(k, k);
+            double tmp = y[k];
+            for (int q = 0; q < k; ++q) y[q] -= tmp * h(k, q);
+        }
+    }
+    if (y[0] != 0.0) y[0] /= h(0, 0);
+    for (int k = 0; k <= col; ++k) ybuf[k] = y[k];
+    st->ncomb = col + 1;
+}
+
+__global__ void k_combine_gm(int64_t n, const GmDev* __restrict__ st, const double* __restrict__ V, int64_t ldv,
+                             const double* __restrict__ y, double* __restrict__ x) {
+    const int m = st->ncomb;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int q = 0; q < m; ++q) acc += y[q] * V[q * ldv + i];
+        x[i] = acc;
+    }
+}
+
+__global__ void k_gm_info(GmDev* st, const double* __restrict__ scal) {
+    if (threadIdx.x != 0) return;
+    const double rnorm = scal[10];
+    st->rnorm = rnorm;
+    st->info = st->skip ? 0 : ((rnorm <= st->atol_eff) ? 0 : 1);
+}
+
+// Host view of the results read back after a graph run.
+struct GmHost {
+    double args[4];               // t, dh, rtol, atol
+    int res[6];                   // col, done, skip, iters, info, ncomb
+};
+
+static int gm_build(dv_model* m, Work& W, int kdim) {
+    if (W.gm_exec) { cudaGraphExecDestroy(W.gm_exec); W.gm_exec = nullptr; }
+    if (W.gm_graph) { cudaGraphDestroy(W.gm_graph); W.gm_graph = nullptr; }
+    if (!W.gm_cs) DV_CUDA(cudaStreamCreateWithFlags(&W.gm_cs, cudaStreamNonBlocking));
+    cudaStream_t body_cs = nullptr;
+    DV_CUDA(cudaStreamCreateWithFlags(&body_cs, cudaStreamNonBlocking));
+    GmDev* st = (GmDev*)W.gm;
+    const double* dargs = (const double*)st;              // t, dh
+    const int64_t n = W.n, ldv = n;
+    const unsigned g = vgrid(n);
+    cudaStream_t cs = W.gm_cs;
+    int64_t fixed[K_NKIND] = {0}, iter[K_NKIND] = {0};
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+    cudaGraph_t cg = nullptr;
+    cudaGraphConditionalHandle hnd = 0;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaStreamCaptureStatus cst;
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hnd, cg, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        // pre: ||b||, loop state
+        k_sumsq<<<g, VB, 0, cs>>>(n, W.b, nullptr, W.part);
+        k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 9);
+        k_gm_init<<<1, VB, 0, cs>>>(st, W.scal, kdim, hnd);
+        fixed[K_VECTOR] += 3;
+        e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &ndeps);
+    }
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraph_t body = nullptr;
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = hnd;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&cnode, cg, deps, ndeps, &cp);
+        if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+    }
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(body_cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+        // body: one Arnoldi step
+        k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
+        iter[K_VECTOR] += 1;
+        int rc = precond_apply_capture(m, W.vin, W.s, W.u, body_cs);
+        iter[K_PC_APPLY] += 1;
+        k_sumsq<<<g, VB, 0, body_cs>>>(n, W.u, nullptr, W.part);
+        k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
+        iter[K_VECTOR] += 2;
+        if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, body_cs);
+        iter[K_MATVEC] += 3;
+        for (int pass = 0; pass < 2; ++pass) {
+            double* hb = W.hbuf + pass * (kdim + 2);
+            k_dots_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.wout, W.part);
+            k_dots_finish_gm<<<kdim + 2, VB, 0, body_cs>>>((int)g, st, W.part, hb);
+            k_orth_update_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, hb, W.wout);
+        }
+        k_sumsq<<<g, VB, 0, body_cs>>>(n, W.wout, nullptr, W.part);
+        k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 2, W.hbuf + 2 * (kdim + 2));
+        k_gm_givens<<<1, 32, 0, body_cs>>>(st, W.hbuf, kdim, hnd);
+        iter[K_VECTOR] += 9;
+        cudaGraph_t tmp = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(body_cs, &tmp);
+        e = (rc != DV_OK) ? cudaErrorUnknown : e2;
+    }
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &cnode, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+        // post: y, x = V y, true residual r = b - AP x
+        k_gm_solve<<<1, 32, 0, cs>>>(st, W.ybuf, kdim);
+        k_combine_gm<<<g, VB, 0, cs>>>(n, st, W.V, ldv, W.ybuf, W.x);
+        fixed[K_VECTOR] += 2;
+        int rc = precond_apply_capture(m, W.x, W.s, W.u, cs);
+        fixed[K_PC_APPLY] += 1;
+        k_sumsq<<<g, VB, 0, cs>>>(n, W.u, nullptr, W.part);
+        k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
+        if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.r, cs);
+        fixed[K_MATVEC] += 3;
+        k_axpby<<<g, VB, 0, cs>>>(n, 1.0, W.b, -1.0, W.r, W.r);
+        k_sumsq<<<g, VB, 0, cs>>>(n, W.r, nullptr, W.part);
+        k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 10);
+        k_gm_info<<<1, 32, 0, cs>>>(st, W.scal);
+        fixed[K_VECTOR] += 6;
+        if (rc != DV_OK) e = cudaErrorUnknown;
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e3 = cudaStreamEndCapture(cs, &graph);     // always end the capture
+    if (e == cudaSuccess) e = e3;
+    cudaStreamDestroy(body_cs);
+    if (e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return cuda_fail(e, "building the GMRES graph");
+    }
+    W.gm_graph = graph;
+    DV_CUDA(cudaGraphInstantiate(&W.gm_exec, graph, 0));
+    W.gm_kdim = kdim;
+    W.gm_mode = m->pc_mode;
+    W.gm_nb = m->pc_nb;
+    W.gm_nparts = m->pc_nparts;
+    for (int k = 0; k < K_NKIND; ++k) {
+        W.gm_fixed[k] = fixed[k];
+        W.gm_iter[k] = iter[k];
+    }
+    return DV_OK;
+}
+
+// gmres() run by the graph; same contract.  b, op.z, op.f, op.s must be the workspace's own
+// vectors (the graph is built on their addresses).
+static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
+                       int64_t* inner, cudaStream_t st) {
+    dv_model* m = op.m;
+    if (!W.gm_exec || W.gm_kdim != kdim || W.gm_mode != m->pc_mode || W.gm_nb != m->pc_nb ||
+        W.gm_nparts != m->pc_nparts)
+        DV_TRY(gm_build(m, W, kdim));
+    GmHost* hst = (GmHost*)W.gm_host;
+    hst->args[0] = op.t;
+    hst->args[1] = op.dh;
+    hst->args[2] = rtol;
+    hst->args[3] = atol;
+    GmDev* dev = (GmDev*)W.gm;
+    DV_CUDA(cudaMemcpyAsync(dev, hst->args, sizeof(hst->args), cudaMemcpyHostToDevice, st));
+    DV_CUDA(cudaGraphLaunch(W.gm_exec, st));
+    DV_CUDA(cudaMemcpyAsync(hst->res, &dev->col, sizeof(hst->res), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaStreamSynchronize(st));
+    const int iters = hst->res[3], skip = hst->res[2];
+    *info = hst->res[4];
+    *inner += iters;
+    m->nfev += iters + (skip ? 0 : 1);
+    for (int k = 0; k < K_NKIND; ++k) count_launches(k, W.gm_fixed[k] + W.gm_iter[k] * iters);
+    if (g_prof_on && !g_pending.empty()) prof_flush();
+    return check_device_error(m);
+}
+
+// The graph when it applies; the host-driven loop while launches are being profiled one by one.
+static int gmres_any(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
+                     int64_t* inner, cudaStream_t st) {
+    if (g_prof_on || b != W.b || op.z != W.z || op.f != W.f || op.s != W.s || kdim > GM_KMAX)
+        return gmres(W, op, b, rtol, atol, kdim, info, inner, st);
+    return gmres_graph(W, op, b, rtol, atol, kdim, info, inner, st);
+}
+
 }  // namespace dv
 // ================================================================== Newton-Krylov stage solve
 namespace dv {
@@ -617,7 +1008,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         const double floor_ = (polish ? 1e-4 : 0.1 * kappa) * sqrt_n;
         int info = 0;
         int64_t inner = 0;
-        DV_TRY(gmres(W, op, W.b, polish ? 1e-3 : C.o.eta, floor_, C.o.krylov_dim, &info, &inner, st));
+        DV_TRY(gmres_any(W, op, W.b, polish ? 1e-3 : C.o.eta, floor_, C.o.krylov_dim, &info, &inner, st));
         if (polish) r.gmres_polish += inner;
         else { r.gmres_iters += inner; if (C.gm_counter) *C.gm_counter += inner; }
         if (info != 0 && C.o.allow_refresh && !new_lu && !polish) {
@@ -627,7 +1018,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             r.jac_refresh_in_newton += 1;
             DV_TRY(pnorm(W.R, W.s, &pn));
             int64_t inner2 = 0;
-            DV_TRY(gmres(W, op, W.b, C.o.eta, floor_, C.o.krylov_dim, &info, &inner2, st));
+            DV_TRY(gmres_any(W, op, W.b, C.o.eta, floor_, C.o.krylov_dim, &info, &inner2, st));
             r.gmres_iters += inner2;
             if (C.gm_counter) *C.gm_counter += inner2;
         }
@@ -662,9 +1053,10 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.tmp));
         double step;
         DV_TRY(rms_ratio(W, n, W.tmp, W.s, &step, st));
-        std::swap(W.z, W.zt);
-        std::swap(W.f, W.ft);
-        std::swap(W.R, W.Rt);
+        // accept the trial point (copies, not pointer swaps: the GMRES graph is built on these addresses)
+        DV_TRY(copy(W.zt, W.z));
+        DV_TRY(copy(W.ft, W.f));
+        DV_TRY(copy(W.Rt, W.R));
         rn = rn_try;
         pn = pn_try;
         const double rate = (step_prev < 0.0) ? 0.0 : step / std::max(step_prev, 1e-300);
