@@ -3,8 +3,11 @@
 // The reference preconditions GMRES with a SuperLU factorisation of M = I - d h J restricted to
 // theta sectors (+ the innermost rings fully coupled), core/solver.py:334-337 and
 // core/jacobian.py:50-69,88-91.  Here M is partitioned into z-planes: a partition is either one
-// theta sector (mode theta_block: cells (i, j, k) for all rings i of sector j, plus the wall
-// node (j, k)) or a whole cross-section (mode full).  Inside a partition every coupling of the
+// theta sector (mode 0: cells (i, j, k) for all rings i of sector j, plus the wall node (j, k)),
+// a whole cross-section (mode 1), or, in mode 2, the innermost ring of every sector as one
+// partition plus rings 1.. of each sector (with its wall node) as the others: the inner ring's
+// theta couplings stay in the preconditioner, which the reference keeps for its innermost rings.
+// Inside a partition every coupling of the
 // stencil is kept: within a plane (r, and theta in full mode) and between planes k-2..k+2 (the
 // MUSCL z+-2 reach).  The partition matrix is block-pentadiagonal in z with dense nb x nb blocks
 // (row-major, leading dimension ld >= nb, zero padded), factorised by block Gaussian elimination:
@@ -24,8 +27,27 @@ namespace dv {
 
 struct PcGeom {
     int Nr, Nth, Nz, wall, mode, nb, nparts, ld;
+    int ncv;               // cell unknowns (6 per cell) of the partition; nb - ncv wall nodes follow
     int64_t nc, bs;        // bs: block stride in doubles (nb*ld rounded up to even: 16-byte multiple)
 };
+
+// Geometry as seen by one partition: nb and ncv of that partition (ld, bs and strides stay the
+// largest partition's).  Mode 2: parts 0..Nth-1 are sectors (rings 1..Nr-1 + wall), part Nth the core.
+static __host__ __device__ __forceinline__ PcGeom pc_part(const PcGeom& g, int part) {
+    PcGeom q = g;
+    if (g.mode == 2) {
+        if (part == g.Nth) { q.ncv = DV_NV * g.Nth; q.nb = q.ncv; }
+        else { q.ncv = DV_NV * (g.Nr - 1); q.nb = q.ncv + (g.wall ? 1 : 0); }
+    }
+    return q;
+}
+
+// partition of the cell unknowns of cell (i, j)
+static __device__ __forceinline__ int pc_part_of(const PcGeom& g, int i, int j) {
+    if (g.mode == 0) return j;
+    if (g.mode == 2) return (i == 0) ? g.Nth : j;
+    return 0;
+}
 
 #define PC_SMEM_NB 56      // largest block the shared-memory factorisation keeps resident (9 blocks)
 
@@ -39,6 +61,17 @@ static inline int pc_ld(int nb) {
 
 static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int k, int l) {
     const int64_t offw = (int64_t)DV_NV * g.nc;
+    if (g.mode == 2) {
+        if (part == g.Nth) {                    // core: (sector j, var v) of ring 0
+            const int j = l / DV_NV, v = l % DV_NV;
+            return (int64_t)v * g.nc + (int64_t)j * g.Nz + k;
+        }
+        if (l < DV_NV * (g.Nr - 1)) {           // sector `part`, rings 1..Nr-1
+            const int i = 1 + l / DV_NV, v = l % DV_NV;
+            return (int64_t)v * g.nc + ((int64_t)i * g.Nth + part) * g.Nz + k;
+        }
+        return offw + (int64_t)part * g.Nz + k;
+    }
     if (g.mode == 0) {   // theta sector `part`
         if (l < DV_NV * g.Nr) {
             int i = l / DV_NV, v = l % DV_NV;
@@ -55,6 +88,10 @@ static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int
 
 // local index of (cell (i, j), var v) / wall (j) inside its partition
 static __device__ __forceinline__ int pc_local(const PcGeom& g, int i, int j, int v) {
+    if (g.mode == 2) {
+        if (v == DV_NV) return DV_NV * (g.Nr - 1);
+        return (i == 0) ? j * DV_NV + v : (i - 1) * DV_NV + v;
+    }
     if (g.mode == 0) return (v < DV_NV) ? i * DV_NV + v : DV_NV * g.Nr;
     return (v < DV_NV) ? (i * g.Nth + j) * DV_NV + v : DV_NV * g.Nr * g.Nth + j;
 }
@@ -62,8 +99,7 @@ static __device__ __forceinline__ int pc_local(const PcGeom& g, int i, int j, in
 // The z-couplings A(k, k+-1), A(k, k+-2) only connect a cell to itself in another plane: they are
 // block diagonal with 6x6 cell blocks (and 1x1 wall entries).  First index / size of the block of l:
 static __device__ __forceinline__ void pc_cellblock(const PcGeom& g, int l, int& b0, int& bsz) {
-    const int ncv = (g.mode == 0) ? DV_NV * g.Nr : DV_NV * g.Nr * g.Nth;
-    if (l < ncv) { b0 = (l / DV_NV) * DV_NV; bsz = DV_NV; }
+    if (l < g.ncv) { b0 = (l / DV_NV) * DV_NV; bsz = DV_NV; }
     else { b0 = l; bsz = 1; }
 }
 
@@ -91,11 +127,11 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
         case 4: nk = k + 2; ok = nk < g.Nz; break;
         case 5: ni = i - 1; ok = ni >= 0; break;
         case 6: ni = i + 1; ok = ni < g.Nr; break;
-        case 7: ok = g.Nth > 1 && g.mode == 1; nj = (j == 0) ? g.Nth - 1 : j - 1; break;
-        default: ok = g.Nth > 1 && g.mode == 1; nj = (j == g.Nth - 1) ? 0 : j + 1; break;
+        case 7: ok = g.Nth > 1 && g.mode != 0; nj = (j == 0) ? g.Nth - 1 : j - 1; break;
+        default: ok = g.Nth > 1 && g.mode != 0; nj = (j == g.Nth - 1) ? 0 : j + 1; break;
     }
-    if (!ok) return;
-    const int part = (g.mode == 0) ? j : 0;
+    const int part = pc_part_of(g, i, j);
+    if (!ok || pc_part_of(g, ni, nj) != part) return;      // coupling across partitions: dropped
     const int d = nk - k;
     double* B = A + (((int64_t)part * g.Nz + k) * 5 + (d + 2)) * g.bs;
     const bool row_wall_ok = g.wall && i == g.Nr - 1;
@@ -288,7 +324,8 @@ static __device__ void cp_block(int64_t n, const double* src, double* dst) {
 }
 
 // One CTA per partition, every working block resident in shared memory (nb <= PC_SMEM_NB).
-__global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom g, double* __restrict__ A, int* __restrict__ info) {
+__global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __restrict__ A, int* __restrict__ info) {
+    const PcGeom g = pc_part(gin, (int)blockIdx.x);
     extern __shared__ __align__(16) double dsm[];
     __shared__ int perm[64];
     __shared__ double fcol[64], prow[64];
@@ -459,8 +496,9 @@ static __device__ int cta_inverse(int nb, int ld, double* D, double* W, double* 
     return bad;
 }
 
-__global__ void __launch_bounds__(256) k_pc_factor_glob(PcGeom g, double* __restrict__ A, double* __restrict__ work,
+__global__ void __launch_bounds__(256) k_pc_factor_glob(PcGeom gin, double* __restrict__ A, double* __restrict__ work,
                                                         int* __restrict__ info, int use_smem) {
+    const PcGeom g = pc_part(gin, (int)blockIdx.x);
     extern __shared__ double dsm[];
     __shared__ double shA[1024], shB[1024];
     __shared__ double red_v[256];
@@ -470,8 +508,9 @@ __global__ void __launch_bounds__(256) k_pc_factor_glob(PcGeom g, double* __rest
     const int64_t n2 = (int64_t)nb * ld;
     const int64_t bs = g.bs;
     double* base = A + (int64_t)part * g.Nz * 5 * bs;
-    double* T = work + (int64_t)part * 4 * n2;
-    double* W = use_smem ? dsm : (T + n2);
+    const int64_t n2w = (int64_t)gin.nb * ld;          // workspace stride: the largest partition's block
+    double* T = work + (int64_t)part * 4 * n2w;
+    double* W = use_smem ? dsm : (T + n2w);
     int bad = 0;
     for (int k = 0; k < g.Nz; ++k) {
         double* Ak = base + (int64_t)k * 5 * bs;
@@ -542,13 +581,14 @@ static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) 
 #define PA_THREADS 512
 #define PA_LANES 8
 template <int NJ>
-__global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom g, const double* __restrict__ A,
+__global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const double* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
                                                          double* __restrict__ x, int* __restrict__ err) {
     extern __shared__ __align__(128) double dsm[];
     __shared__ __align__(8) uint64_t bars[2];
     constexpr int LD = NJ * PA_LANES;
     const int part = blockIdx.x;
+    const PcGeom g = pc_part(gin, part);
     const int nb = g.nb;
     const int tid = threadIdx.x;
     const int64_t bs = g.bs;
@@ -662,11 +702,12 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom g, const double*
 
 // Sweep for partitions too large for the shared-memory pipeline: same fused stages, operands read
 // from global memory (L2).
-__global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom g, const double* __restrict__ A,
+__global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const double* __restrict__ A,
                                                        const double* __restrict__ b, const double* __restrict__ sc,
                                                        double* __restrict__ x, double* __restrict__ xs_all) {
     __shared__ double tv[512];
     const int part = blockIdx.x;
+    const PcGeom g = pc_part(gin, part);
     const int nb = g.nb, ld = g.ld;
     const int tid = threadIdx.x;
     const int64_t bs = g.bs;
@@ -714,13 +755,22 @@ static PcGeom geom_of(const dv_model* m, int mode) {
     g.Nth = m->p.Nth;
     g.Nz = m->p.Nz;
     g.wall = m->p.wall_on;
-    g.mode = (m->p.Nth > 1 && mode == 0) ? 0 : 1;
+    // mode 2 needs a second ring and a second sector; below that it is mode 0 (or 1 for one sector)
+    if (mode == 2 && (m->p.Nr < 2 || m->p.Nth < 2)) mode = 0;
+    g.mode = (m->p.Nth > 1 && (mode == 0 || mode == 2)) ? mode : 1;
     g.nc = m->nc;
     if (g.mode == 0) {
         g.nb = DV_NV * g.Nr + (g.wall ? 1 : 0);
+        g.ncv = DV_NV * g.Nr;
         g.nparts = g.Nth;
+    } else if (g.mode == 2) {
+        const int nb_sector = DV_NV * (g.Nr - 1) + (g.wall ? 1 : 0), nb_core = DV_NV * g.Nth;
+        g.nb = std::max(nb_sector, nb_core);
+        g.ncv = g.nb;                       // per-partition values come from pc_part
+        g.nparts = g.Nth + 1;
     } else {
         g.nb = DV_NV * g.Nr * g.Nth + (g.wall ? g.Nth : 0);
+        g.ncv = DV_NV * g.Nr * g.Nth;
         g.nparts = 1;
     }
     g.ld = pc_ld(g.nb);
@@ -796,7 +846,7 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
         set_error("preconditioner applied before it was factorised");
         return DV_ERR_ARG;
     }
-    PcGeom g = geom_of(m, m->pc_mode == 0 ? 0 : 1);
+    PcGeom g = geom_of(m, m->pc_mode);
     const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
     const int nj = g.ld / PA_LANES;
     if (g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7)) {
@@ -816,7 +866,7 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
 }
 
 int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s) {
-    PcGeom g = geom_of(m, m->pc_mode == 0 ? 0 : 1);
+    PcGeom g = geom_of(m, m->pc_mode);
     const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
     const int nj = g.ld / PA_LANES;
     if (g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7)) {

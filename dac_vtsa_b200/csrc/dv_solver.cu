@@ -1248,10 +1248,14 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     int nb_sector = DV_NV * p->Nr + (p->wall_on ? 1 : 0);
     int nb_full = DV_NV * p->Nr * p->Nth + (p->wall_on ? p->Nth : 0);
     bool full_ok = nb_full <= 512;
-    m->pc_cap_nb = full_ok ? std::max(nb_full, nb_sector) : nb_sector;
-    m->pc_cap_parts = p->Nth;
+    // mode 2 (innermost ring of all sectors as one partition + rings 1.. per sector): Nth + 1 parts
+    const int nb_ring = (p->Nr >= 2 && p->Nth >= 2)
+                            ? std::max(DV_NV * (p->Nr - 1) + (p->wall_on ? 1 : 0), DV_NV * p->Nth) : 0;
+    m->pc_cap_nb = std::max(full_ok ? std::max(nb_full, nb_sector) : nb_sector, nb_ring);
+    m->pc_cap_parts = p->Nth + 1;
     int64_t pc_need = std::max(precond_doubles(nb_sector, p->Nth, p->Nz),
                                full_ok ? precond_doubles(nb_full, 1, p->Nz) : (int64_t)0);
+    if (nb_ring) pc_need = std::max(pc_need, precond_doubles(nb_ring, p->Nth + 1, p->Nz));
     int64_t work_need = precond_work_doubles(m->pc_cap_nb, m->pc_cap_parts, p->Nz);
     const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
     bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||

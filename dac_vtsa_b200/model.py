@@ -24,6 +24,10 @@ from .params import build_params
 R_GAS = host.R_GAS
 
 
+# preconditioner partitions (dv_precond_factor modes)
+PRECOND_MODES = {"sector": 0, "full": 1, "theta_block": 2}
+
+
 def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -292,10 +296,12 @@ class TVSAModel:
 
     # ------------------------------------------------------------------ linear algebra entry points
     def precond_factor(self, J_block: torch.Tensor, dh: float, mode: str = "theta_block"):
-        """Factorise I - dh J (block layout J) along z per theta sector or cross-section."""
+        """Factorise I - dh J (block layout J) along z per partition: "theta_block" (the innermost ring
+        of all sectors as one partition, rings 1.. of each sector as the others), "sector" (whole
+        sectors) or "full" (whole cross-sections)."""
         with torch.cuda.device(self.device):
-            check(self.lib.dv_precond_factor(self.handle, _ptr(J_block), float(dh),
-                                             0 if mode == "theta_block" else 1, _stream()), "dv_precond_factor")
+            check(self.lib.dv_precond_factor(self.handle, _ptr(J_block), float(dh), PRECOND_MODES[mode],
+                                             _stream()), "dv_precond_factor")
 
     def precond_solve(self, b):
         """x = M^-1 b with the stored factors (the reference's lu.solve)."""
@@ -312,7 +318,7 @@ class TVSAModel:
         s = self.cfg.solver
         o = DvNewtonOpts()
         o.max_iter, o.krylov_dim, o.allow_refresh = int(max_iter), int(krylov_dim), int(bool(allow_refresh))
-        o.precond_mode = 0 if precond_mode == "theta_block" else 1
+        o.precond_mode = PRECOND_MODES[precond_mode]
         o.kappa, o.eta = float(kappa), float(eta)
         o.rtol = float(s.rtol if rtol is None else rtol)
         o.cons_tol = float((s.conservation_tol or 0.0) if cons_tol is None else cons_tol)

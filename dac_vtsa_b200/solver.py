@@ -24,6 +24,7 @@ from . import counters
 from ._lib import DvSolverOpts, DvStepReport, check, load
 from .config import gpu_option
 from .jacobian import FDJacobian
+from .model import PRECOND_MODES
 
 GAMMA = 2.0 - np.sqrt(2.0)
 D = GAMMA / 2.0
@@ -77,7 +78,12 @@ class TRBDF2:
         o.max_newton_iter = s.max_newton_iter
         o.jacobian_max_age = s.jacobian_max_age
         o.gmres_refresh = s.gmres_refresh
-        o.precond_mode = 0 if self.precond == "theta_block" else 1
+        # theta_block: the reference keeps the theta couplings of its innermost precond_theta_rings
+        # rings; the GPU partitions keep those of the innermost ring (mode 2), or none when 0 rings
+        if self.precond == "theta_block":
+            o.precond_mode = PRECOND_MODES["theta_block" if s.precond_theta_rings >= 1 else "sector"]
+        else:
+            o.precond_mode = PRECOND_MODES["full"]
         o.max_steps = s.max_steps_per_step
         o.rtol = s.rtol
         o.newton_kappa = s.newton_kappa

@@ -173,9 +173,12 @@ int dv_colour_columns(int32_t Nr, int32_t Nth, int32_t Nz, int32_t wall, int64_t
 int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, void* stream);
 
 /* ------------------------------------------------------------------ preconditioner
- * Factorise M = I - dh J restricted to theta sectors (theta_block) or whole cross-sections
- * (full) as a block-pentadiagonal LU along z (replaces splu of TRBDF2._factor,
- * core/solver.py:334-337); mode 0 = theta_block, 1 = full.  Stored in the model. */
+ * Factorise M = I - dh J restricted to partitions of the cross-section as a block-pentadiagonal
+ * LU along z (replaces splu of TRBDF2._factor, core/solver.py:334-337).  mode 0 = theta sectors
+ * (all rings of a sector + its wall), 1 = whole cross-sections, 2 = the innermost ring of all
+ * sectors as one partition and rings 1.. of each sector (+ wall) as the others (keeps the inner
+ * ring's theta coupling, as the reference's theta_block keeps its innermost rings'; falls back to
+ * mode 0 below 2 rings or 2 sectors).  Stored in the model. */
 int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, void* stream);
 /* x = M^-1 b with the stored factors (lu.solve). b and x may alias. */
 int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream);

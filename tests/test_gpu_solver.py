@@ -11,15 +11,23 @@ from cases import build, config0_overrides, golden
 pytestmark = pytest.mark.gpu
 
 
-def _sector_of(m):
+def _partition_of(m, mode):
+    """Partition id of every unknown: theta sector ("sector"), sector with the innermost ring of all
+    sectors split off as one more partition ("theta_block"), or one partition ("full")."""
     g = m.grid
     n = g.ncell
     idx = np.arange(m.n_core)
     cellpart = idx < 6 * n
-    return np.where(cellpart, ((idx % n) // g.Nz) % g.Nth, (idx - 6 * n) // g.Nz)
+    sector = np.where(cellpart, ((idx % n) // g.Nz) % g.Nth, (idx - 6 * n) // g.Nz)
+    ring = np.where(cellpart, (idx % n) // (g.Nth * g.Nz), g.Nr - 1)
+    if mode == "sector":
+        return sector
+    if mode == "theta_block":
+        return np.where(ring == 0, g.Nth, sector)
+    return np.zeros_like(idx)
 
 
-@pytest.mark.parametrize("mode", ["theta_block", "full"])
+@pytest.mark.parametrize("mode", ["theta_block", "sector", "full"])
 def test_preconditioner_solves_partition_system(mode):
     """dv_precond_solve == exact sparse solve of I - dh J restricted to the partition couplings."""
     from dac_vtsa_b200.jacobian import FDJacobian
@@ -31,10 +39,8 @@ def test_preconditioner_solves_partition_system(mode):
     dh = 0.3 * 7.0
     m.precond_factor(jac.block(5.0, d["y"]), dh, mode)
     Jc = Jc.tocoo()
-    keep = np.ones(Jc.nnz, dtype=bool)
-    if mode == "theta_block":
-        sec = _sector_of(m)
-        keep = sec[Jc.row] == sec[Jc.col]
+    part = _partition_of(m, mode)
+    keep = part[Jc.row] == part[Jc.col]
     Jk = sp.csc_matrix((Jc.data[keep], (Jc.row[keep], Jc.col[keep])), shape=Jc.shape)
     M = (sp.identity(m.n_core, format="csc") - dh * Jk).tocsc()
     b = np.random.default_rng(7).standard_normal(m.n_core) * m.atol
