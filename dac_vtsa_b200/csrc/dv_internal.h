@@ -45,6 +45,8 @@ struct Work {
     int nparts = 0;
     // device-driven GMRES: one CUDA graph per workspace (built at first use), its device state
     double *vin = nullptr, *wout = nullptr;   // normalised basis vector in / operator output
+    unsigned* tickets = nullptr;              // ticket counters of the fused reductions (zeroed)
+    double* apart = nullptr;                  // per-CTA partials of the fused sweep's reduction
     void* gm = nullptr;                       // device GMRES state
     void* gm_host = nullptr;                  // pinned host mirror of it
     cudaGraph_t gm_graph = nullptr;
@@ -112,9 +114,27 @@ int64_t precond_doubles(int nb, int nparts, int Nz);
 int64_t precond_work_doubles(int nb, int nparts, int Nz);
 // x = diag(1/sc) M^-1 diag(sc) b  (sc may be NULL: plain solve)
 int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);
+// Work the shared-memory sweep can do on the side when it runs in the GMRES graph.  Prologue (V
+// non-null): the input is src = (*col == 0 ? src0 : src1) scaled by *scale, and is also stored to
+// V[*col].  Epilogue (out non-null): *out = sqrt(sum x^2 / n) over the result, reduced through
+// per-CTA partials `part` and a ticket counter (the last CTA sums them in CTA order).
+struct PaFuse {
+    const int* col = nullptr;
+    const double* scale = nullptr;
+    const double* src0 = nullptr;
+    const double* src1 = nullptr;
+    double* V = nullptr;
+    int64_t ldv = 0;
+    double* part = nullptr;
+    unsigned* ticket = nullptr;
+    double* out = nullptr;
+    int64_t n = 0;
+};
+bool precond_apply_fusable(dv_model* m);
 // The same launches without launch accounting or attribute changes, for stream capture (the
 // attributes are set by an earlier precond_apply).  Returns the number of kernels launched.
-int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);
+int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
+                          const PaFuse& F = PaFuse());
 // FD matvec of the split residual for stream capture: t and gh are read from dargs[0..1] (device).
 int matvec_capture(dv_model* m, const double* dargs, const double* z, const double* u, const double* sc,
                    const double* f0, const double* scal, double* out, cudaStream_t s);

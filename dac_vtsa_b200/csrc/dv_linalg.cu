@@ -583,7 +583,7 @@ static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) 
 template <int NJ>
 __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const double* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
-                                                         double* __restrict__ x, int* __restrict__ err) {
+                                                         double* __restrict__ x, int* __restrict__ err, PaFuse F) {
     extern __shared__ __align__(128) double dsm[];
     __shared__ __align__(8) uint64_t bars[2];
     constexpr int LD = NJ * PA_LANES;
@@ -616,12 +616,22 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
         bulk_load(smem_u32(buf0), stage_src(0), stage_bytes(0), smem_u32(&bars[0]));
         if (S > 1) bulk_load(smem_u32(buf1), stage_src(1), stage_bytes(1), smem_u32(&bars[1]));
     }
+    const int fcol = F.V ? *F.col : 0;
+    const double fscale = F.V ? *F.scale : 0.0;
+    const double* fsrc = (fcol == 0) ? F.src0 : F.src1;
     for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
         const int k = q / LD, l = q - k * LD;
         double v = 0.0;
         if (l < nb) {
             const int64_t gi = pc_glob(g, part, k, l);
-            v = sc ? b[gi] * sc[gi] : b[gi];
+            double bv;
+            if (F.V) {                           // normalise the basis vector on the way in
+                bv = fscale * fsrc[gi];
+                F.V[(int64_t)fcol * F.ldv + gi] = bv;
+            } else {
+                bv = b[gi];
+            }
+            v = sc ? bv * sc[gi] : bv;
         }
         xs[q] = v;
     }
@@ -684,18 +694,44 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
         }
         __syncthreads();
     }
+    double ss = 0.0;
     if (!ok) {                                   // drain copies still in flight (bounded) and leave x untouched
         if (tid == 0) {
             mbar_wait(smem_u32(&bars[0]), 0);
             mbar_wait(smem_u32(&bars[1]), 0);
         }
-        return;
+    } else {
+        for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
+            const int k = q / LD, l = q - k * LD;
+            if (l < nb) {
+                const int64_t gi = pc_glob(g, part, k, l);
+                const double xv = sc ? xs[q] / sc[gi] : xs[q];
+                x[gi] = xv;
+                ss += xv * xv;
+            }
+        }
     }
-    for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
-        const int k = q / LD, l = q - k * LD;
-        if (l < nb) {
-            const int64_t gi = pc_glob(g, part, k, l);
-            x[gi] = sc ? xs[q] / sc[gi] : xs[q];
+    if (F.out) {                                 // rms of the result: per-CTA partial, last CTA finishes
+        __shared__ double wsum[PA_THREADS / 32];
+        __shared__ bool last;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, off);
+        if ((tid & 31) == 0) wsum[tid >> 5] = ss;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < PA_THREADS / 32; ++w) t += wsum[w];
+            F.part[part] = t;
+            __threadfence();
+            last = (atomicAdd(F.ticket, 1u) == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (last && tid == 0) {
+            __threadfence();
+            double t = 0.0;
+            for (int c = 0; c < (int)gridDim.x; ++c) t += ((volatile double*)F.part)[c];
+            *F.out = sqrt(t / (double)F.n);
+            *F.ticket = 0u;
         }
     }
 }
@@ -837,7 +873,7 @@ static int launch_apply(const PcGeom& g, dv_model* m, const double* b, const dou
                         size_t dyn) {
     if (dyn > 48 * 1024)
         DV_CUDA(cudaFuncSetAttribute(k_pc_apply<NJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err));
+    DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, PaFuse()));
     return DV_OK;
 }
 
@@ -865,18 +901,30 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
     return DV_OK;
 }
 
-int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s) {
+bool precond_apply_fusable(dv_model* m) {
     PcGeom g = geom_of(m, m->pc_mode);
     const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
     const int nj = g.ld / PA_LANES;
-    if (g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7)) {
+    return g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7);
+}
+
+int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
+                          const PaFuse& F) {
+    PcGeom g = geom_of(m, m->pc_mode);
+    const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
+    const int nj = g.ld / PA_LANES;
+    if (precond_apply_fusable(m)) {
         switch (nj) {
-            case 1: k_pc_apply<1><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
-            case 3: k_pc_apply<3><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
-            case 5: k_pc_apply<5><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
-            default: k_pc_apply<7><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err); break;
+            case 1: k_pc_apply<1><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
+            case 3: k_pc_apply<3><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
+            case 5: k_pc_apply<5><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
+            default: k_pc_apply<7><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
         }
     } else {
+        if (F.V || F.out) {
+            set_error("fused sweep requested for a partition the shared-memory sweep does not take");
+            return DV_ERR_ARG;
+        }
         k_pc_apply_glob<<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work);
     }
     DV_CUDA(cudaGetLastError());

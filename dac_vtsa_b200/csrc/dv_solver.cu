@@ -341,7 +341,8 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
         A(&W.s, n) || A(&W.z, n) || A(&W.f, n) || A(&W.R, n) || A(&W.dz, n) || A(&W.zt, n) || A(&W.ft, n) ||
         A(&W.Rt, n) || A(&W.tmp, n) || A(&W.best, n) || A(&W.part, (int64_t)W.nparts * (kdim + 2)) ||
         A(&W.scal, 16) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles) ||
-        A(&W.vin, n) || A(&W.wout, n) || cudaMalloc(&W.gm, gm_state_bytes()) != cudaSuccess)
+        A(&W.vin, n) || A(&W.wout, n) || A(&W.apart, 4096) || cudaMalloc(&W.gm, gm_state_bytes()) != cudaSuccess ||
+        cudaMalloc((void**)&W.tickets, 16 * sizeof(unsigned)) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMalloc(Krylov workspace)");
     if (cudaMallocHost(&W.gm_host, 256) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaMallocHost");
     if (cudaMallocHost((void**)&W.hpin, sizeof(double) * 4 * (kdim + 8)) != cudaSuccess)
@@ -358,7 +359,10 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
         debug_fill(W.gm, gm_state_bytes(), 2);
         debug_fill(W.gm_host, 256, 8, true);
         debug_fill(W.hpin, d * 4 * (kdim + 8), 8, true);
+        debug_fill(W.apart, d * 4096, 2);
     }
+    if (cudaMemset(W.tickets, 0, 16 * sizeof(unsigned)) != cudaSuccess)   // ticket counters start at zero
+        return cuda_fail(cudaGetLastError(), "cudaMemset(tickets)");
     return DV_OK;
 }
 
@@ -367,10 +371,11 @@ void work_free(Work& W) {
     if (W.gm_graph) cudaGraphDestroy(W.gm_graph);
     if (W.gm_cs) cudaStreamDestroy(W.gm_cs);
     double* ptrs[] = {W.V, W.w, W.u, W.x, W.r, W.b, W.s, W.z, W.f, W.R, W.dz, W.zt, W.ft, W.Rt, W.tmp, W.best,
-                      W.part, W.scal, W.hbuf, W.ybuf, W.J, W.vin, W.wout};
+                      W.part, W.scal, W.hbuf, W.ybuf, W.J, W.vin, W.wout, W.apart};
     for (double* p : ptrs)
         if (p) cudaFree(p);
     if (W.gm) cudaFree(W.gm);
+    if (W.tickets) cudaFree(W.tickets);
     if (W.hpin) cudaFreeHost(W.hpin);
     if (W.gm_host) cudaFreeHost(W.gm_host);
     W = Work();
@@ -683,8 +688,7 @@ __global__ void k_orth_update_gm(int64_t n, const GmDev* __restrict__ st, const 
 }
 
 // Hessenberg column, Givens rotations, residual estimate and the stopping test of gmres()
-__global__ void k_gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, cudaGraphConditionalHandle hnd) {
-    if (threadIdx.x != 0) return;
+__device__ void gm_givens(GmDev* st, const double* hh, int kdim, cudaGraphConditionalHandle hnd) {
     const double eps = 2.220446049250313e-16;                 // double epsilon
     const int col = st->col;
     const int m = col + 1;
@@ -723,6 +727,121 @@ __global__ void k_gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, 
     if (!stop) st->col = col + 1;
     st->done = stop;
     cudaGraphSetConditional(hnd, stop ? 0u : 1u);
+}
+
+__global__ void k_gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, cudaGraphConditionalHandle hnd) {
+    if (threadIdx.x == 0) gm_givens(st, hh, kdim, hnd);
+}
+
+// ---- fused classical Gram-Schmidt of the graph body (three kernels per Arnoldi step)
+// Block sums of the first cnt entries of acc (VB threads) into part[blockIdx.x * GM_PS + q];
+// returns true in the block that finished last (after the other blocks' partials are visible).
+constexpr int GM_PS = GM_KMAX + 2;      // partial stride per block
+__device__ __forceinline__ bool gm_block_partials(const double (&acc)[GM_KMAX + 1], int cnt, double* part,
+                                                  unsigned* ticket) {
+    __shared__ double sm[VB / 32][GM_PS];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q <= GM_KMAX; ++q) {
+        if (q < cnt) {
+            double v = acc[q];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0) sm[wid][q] = v;
+        }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < cnt) {
+        double t = 0.0;
+        for (int w2 = 0; w2 < VB / 32; ++w2) t += sm[w2][threadIdx.x];
+        part[(int64_t)blockIdx.x * GM_PS + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// out[q] = sum over blocks of part[.. q], q < cnt, in block order (called by the last block)
+__device__ __forceinline__ void gm_finish_partials(const double* part, int cnt, double* out, unsigned* ticket) {
+    if ((int)threadIdx.x < cnt) {
+        double t = 0.0;
+        for (int b2 = 0; b2 < (int)gridDim.x; ++b2)
+            t += ((volatile const double*)part)[(int64_t)b2 * GM_PS + threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// pass 1: out[q] = V_q . w (q < m) and out[m] = w . w, m = col + 1
+__global__ void __launch_bounds__(VB) k_cgs_dots(int64_t n, const GmDev* __restrict__ st, const double* __restrict__ V,
+                                                 int64_t ldv, const double* __restrict__ w, double* __restrict__ part,
+                                                 unsigned* ticket, double* __restrict__ out) {
+    const int m = st->col + 1;
+    double acc[GM_KMAX + 1];
+#pragma unroll
+    for (int q = 0; q <= GM_KMAX; ++q) acc[q] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int q = 0; q <= GM_KMAX; ++q) {
+            if (q < m) acc[q] += V[q * ldv + i] * wi;
+            else if (q == m) acc[q] += wi * wi;
+        }
+    }
+    if (gm_block_partials(acc, m + 1, part, ticket)) gm_finish_partials(part, m + 1, out, ticket);
+}
+
+// w -= sum_q h[q] V_q, then pass 2: out[q] = V_q . w (q < m)
+__global__ void __launch_bounds__(VB) k_cgs_orth_dots(int64_t n, const GmDev* __restrict__ st,
+                                                      const double* __restrict__ V, int64_t ldv,
+                                                      const double* __restrict__ h, double* __restrict__ w,
+                                                      double* __restrict__ part, unsigned* ticket,
+                                                      double* __restrict__ out) {
+    const int m = st->col + 1;
+    double acc[GM_KMAX + 1];
+#pragma unroll
+    for (int q = 0; q <= GM_KMAX; ++q) acc[q] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double o = 0.0;
+        for (int q = 0; q < m; ++q) o += h[q] * V[q * ldv + i];
+        const double wi = w[i] - o;
+        w[i] = wi;
+#pragma unroll
+        for (int q = 0; q < GM_KMAX; ++q)
+            if (q < m) acc[q] += V[q * ldv + i] * wi;
+    }
+    if (gm_block_partials(acc, m, part, ticket)) gm_finish_partials(part, m, out, ticket);
+}
+
+// w -= sum_q h2[q] V_q, ||w|| into hh[2 (kdim+2)], then the Givens update and stopping test
+__global__ void __launch_bounds__(VB) k_cgs_orth_norm(int64_t n, GmDev* st, const double* __restrict__ V, int64_t ldv,
+                                                      double* __restrict__ hh, double* __restrict__ w,
+                                                      double* __restrict__ part, unsigned* ticket, int kdim,
+                                                      cudaGraphConditionalHandle hnd) {
+    const int m = st->col + 1;
+    const double* h2 = hh + (kdim + 2);
+    double acc[GM_KMAX + 1];
+    acc[0] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double o = 0.0;
+        for (int q = 0; q < m; ++q) o += h2[q] * V[q * ldv + i];
+        const double wi = w[i] - o;
+        w[i] = wi;
+        acc[0] += wi * wi;
+    }
+    if (gm_block_partials(acc, 1, part, ticket)) {
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int b2 = 0; b2 < (int)gridDim.x; ++b2) t += ((volatile const double*)part)[(int64_t)b2 * GM_PS];
+            hh[2 * (kdim + 2)] = sqrt(t);
+            *ticket = 0u;
+            gm_givens(st, hh, kdim, hnd);
+        }
+    }
 }
 
 // least squares by back substitution (as in gmres()); ybuf = y, ncomb = its length
@@ -814,27 +933,52 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
     }
     if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(body_cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    const bool fused = precond_apply_fusable(m);
     if (e == cudaSuccess) {
         // body: one Arnoldi step
-        k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
-        iter[K_VECTOR] += 1;
-        int rc = precond_apply_capture(m, W.vin, W.s, W.u, body_cs);
-        iter[K_PC_APPLY] += 1;
-        k_sumsq<<<g, VB, 0, body_cs>>>(n, W.u, nullptr, W.part);
-        k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
-        iter[K_VECTOR] += 2;
-        if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, body_cs);
-        iter[K_MATVEC] += 3;
-        for (int pass = 0; pass < 2; ++pass) {
-            double* hb = W.hbuf + pass * (kdim + 2);
-            k_dots_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.wout, W.part);
-            k_dots_finish_gm<<<kdim + 2, VB, 0, body_cs>>>((int)g, st, W.part, hb);
-            k_orth_update_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, hb, W.wout);
+        int rc = DV_OK;
+        if (fused) {        // sweep with normalisation prologue and rms epilogue; CGS2 in three kernels
+            PaFuse F;
+            F.col = &st->col;
+            F.scale = &st->scale;
+            F.src0 = W.b;
+            F.src1 = W.wout;
+            F.V = W.V;
+            F.ldv = ldv;
+            F.part = W.apart;
+            F.ticket = W.tickets + 0;
+            F.out = W.scal + 0;
+            F.n = n;
+            rc = precond_apply_capture(m, W.vin, W.s, W.u, body_cs, F);
+            iter[K_PC_APPLY] += 1;
+            if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, body_cs);
+            iter[K_MATVEC] += 3;
+            k_cgs_dots<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.wout, W.part, W.tickets + 1, W.hbuf);
+            k_cgs_orth_dots<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 2,
+                                                   W.hbuf + (kdim + 2));
+            k_cgs_orth_norm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 3, kdim, hnd);
+            iter[K_VECTOR] += 3;
+        } else {
+            k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
+            iter[K_VECTOR] += 1;
+            rc = precond_apply_capture(m, W.vin, W.s, W.u, body_cs);
+            iter[K_PC_APPLY] += 1;
+            k_sumsq<<<g, VB, 0, body_cs>>>(n, W.u, nullptr, W.part);
+            k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
+            iter[K_VECTOR] += 2;
+            if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, body_cs);
+            iter[K_MATVEC] += 3;
+            for (int pass = 0; pass < 2; ++pass) {
+                double* hb = W.hbuf + pass * (kdim + 2);
+                k_dots_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.wout, W.part);
+                k_dots_finish_gm<<<kdim + 2, VB, 0, body_cs>>>((int)g, st, W.part, hb);
+                k_orth_update_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, hb, W.wout);
+            }
+            k_sumsq<<<g, VB, 0, body_cs>>>(n, W.wout, nullptr, W.part);
+            k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 2, W.hbuf + 2 * (kdim + 2));
+            k_gm_givens<<<1, 32, 0, body_cs>>>(st, W.hbuf, kdim, hnd);
+            iter[K_VECTOR] += 9;
         }
-        k_sumsq<<<g, VB, 0, body_cs>>>(n, W.wout, nullptr, W.part);
-        k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 2, W.hbuf + 2 * (kdim + 2));
-        k_gm_givens<<<1, 32, 0, body_cs>>>(st, W.hbuf, kdim, hnd);
-        iter[K_VECTOR] += 9;
         cudaGraph_t tmp = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(body_cs, &tmp);
         e = (rc != DV_OK) ? cudaErrorUnknown : e2;
@@ -845,17 +989,28 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         k_gm_solve<<<1, 32, 0, cs>>>(st, W.ybuf, kdim);
         k_combine_gm<<<g, VB, 0, cs>>>(n, st, W.V, ldv, W.ybuf, W.x);
         fixed[K_VECTOR] += 2;
-        int rc = precond_apply_capture(m, W.x, W.s, W.u, cs);
+        int rc;
+        if (fused) {
+            PaFuse F;
+            F.part = W.apart;
+            F.ticket = W.tickets + 4;
+            F.out = W.scal + 0;
+            F.n = n;
+            rc = precond_apply_capture(m, W.x, W.s, W.u, cs, F);
+        } else {
+            rc = precond_apply_capture(m, W.x, W.s, W.u, cs);
+            k_sumsq<<<g, VB, 0, cs>>>(n, W.u, nullptr, W.part);
+            k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
+            fixed[K_VECTOR] += 2;
+        }
         fixed[K_PC_APPLY] += 1;
-        k_sumsq<<<g, VB, 0, cs>>>(n, W.u, nullptr, W.part);
-        k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
         if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.r, cs);
         fixed[K_MATVEC] += 3;
         k_axpby<<<g, VB, 0, cs>>>(n, 1.0, W.b, -1.0, W.r, W.r);
         k_sumsq<<<g, VB, 0, cs>>>(n, W.r, nullptr, W.part);
         k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 10);
         k_gm_info<<<1, 32, 0, cs>>>(st, W.scal);
-        fixed[K_VECTOR] += 6;
+        fixed[K_VECTOR] += 4;
         if (rc != DV_OK) e = cudaErrorUnknown;
     }
     cudaGraph_t graph = nullptr;
