@@ -340,7 +340,7 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
     if (A(&W.V, (kdim + 1) * n) || A(&W.w, n) || A(&W.u, n) || A(&W.x, n) || A(&W.r, n) || A(&W.b, n) ||
         A(&W.s, n) || A(&W.z, n) || A(&W.f, n) || A(&W.R, n) || A(&W.dz, n) || A(&W.zt, n) || A(&W.ft, n) ||
         A(&W.Rt, n) || A(&W.tmp, n) || A(&W.best, n) || A(&W.part, (int64_t)W.nparts * (kdim + 2)) ||
-        A(&W.scal, 16) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles) ||
+        A(&W.scal, 32) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles) ||
         A(&W.vin, n) || A(&W.wout, n) || A(&W.apart, 4096) || cudaMalloc(&W.gm, gm_state_bytes()) != cudaSuccess ||
         cudaMalloc((void**)&W.tickets, 16 * sizeof(unsigned)) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMalloc(Krylov workspace)");
@@ -352,7 +352,7 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
         std::pair<double*, int64_t> bufs[] = {{W.V, (kdim + 1) * n}, {W.w, n}, {W.u, n}, {W.x, n}, {W.r, n}, {W.b, n},
                                               {W.s, n}, {W.z, n}, {W.f, n}, {W.R, n}, {W.dz, n}, {W.zt, n}, {W.ft, n},
                                               {W.Rt, n}, {W.tmp, n}, {W.best, n},
-                                              {W.part, (int64_t)W.nparts * (kdim + 2)}, {W.scal, 16},
+                                              {W.part, (int64_t)W.nparts * (kdim + 2)}, {W.scal, 32},
                                               {W.hbuf, 4 * (kdim + 2)}, {W.ybuf, kdim + 2}, {W.J, jac_doubles},
                                               {W.vin, n}, {W.wout, n}};
         for (auto& b : bufs) debug_fill(b.first, d * (size_t)b.second, 2);
@@ -1052,7 +1052,12 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
     DV_CUDA(cudaMemcpyAsync(dev, hst->args, sizeof(hst->args), cudaMemcpyHostToDevice, st));
     DV_CUDA(cudaGraphLaunch(W.gm_exec, st));
     DV_CUDA(cudaMemcpyAsync(hst->res, &dev->col, sizeof(hst->res), cudaMemcpyDeviceToHost, st));
-    DV_CUDA(cudaStreamSynchronize(st));
+    return DV_OK;
+}
+
+// Results of the last gmres_graph launch, once the stream has been synchronised.
+static int gmres_graph_collect(Work& W, dv_model* m, int* info, int64_t* inner) {
+    GmHost* hst = (GmHost*)W.gm_host;
     const int iters = hst->res[3], skip = hst->res[2];
     *info = hst->res[4];
     *inner += iters;
@@ -1063,11 +1068,25 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
 }
 
 // The graph when it applies; the host-driven loop while launches are being profiled one by one.
-static int gmres_any(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
-                     int64_t* inner, cudaStream_t st) {
+// With *pending set on return the graph is still running: call gmres_graph_collect after the
+// next synchronisation of the stream.
+static int gmres_start(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
+                       int64_t* inner, bool* pending, cudaStream_t st) {
+    *pending = false;
     if (g_prof_on || b != W.b || op.z != W.z || op.f != W.f || op.s != W.s || kdim > GM_KMAX)
         return gmres(W, op, b, rtol, atol, kdim, info, inner, st);
-    return gmres_graph(W, op, b, rtol, atol, kdim, info, inner, st);
+    DV_TRY(gmres_graph(W, op, b, rtol, atol, kdim, info, inner, st));
+    *pending = true;
+    return DV_OK;
+}
+
+static int gmres_any(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
+                     int64_t* inner, cudaStream_t st) {
+    bool pending = false;
+    DV_TRY(gmres_start(W, op, b, rtol, atol, kdim, info, inner, &pending, st));
+    if (!pending) return DV_OK;
+    DV_CUDA(cudaStreamSynchronize(st));
+    return gmres_graph_collect(W, op.m, info, inner);
 }
 
 }  // namespace dv
@@ -1135,6 +1154,36 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         return DV_OK;
     };
 
+    auto cons_eval = [&](const double* v) -> bool {
+        if (C.o.cons_tol <= 0.0) return true;
+        bool ok = true;
+        for (int q = 0; q < 4; ++q)
+            if (!(std::fabs(v[q]) <= C.o.cons_tol * v[4 + q])) ok = false;
+        return ok;
+    };
+    // Queue the evaluation of the full Newton step from the GMRES solution W.x: dz, the trial point
+    // at lam = 1 with its stage residual, and the scalars the host tests (rms(dz), rms(R/s), the
+    // preconditioned norm, the step length, the balance sums); copy them into W.hpin[16..47].
+    auto speculate = [&]() -> int {
+        DV_TRY(precond_apply(m, W.x, W.s, W.u, st));
+        DV_LAUNCH(dv::K_VECTOR, st, k_mul<<<g, VB, 0, st>>>(n, W.u, W.s, W.dz));
+        DV_TRY(rms_ratio_dev(W, n, W.dz, nullptr, 0, W.scal + 11, st));
+        DV_LAUNCH(dv::K_VECTOR, st, k_truncate<<<g, VB, 0, st>>>(n, C.npos, W.z, 1.0, W.dz, W.zt));
+        DV_TRY(stage(W.zt, W.ft, W.Rt));
+        DV_TRY(rms_ratio_dev(W, n, W.Rt, W.s, 0, W.scal + 12, st));
+        DV_TRY(precond_apply(m, W.Rt, nullptr, W.tmp, st));
+        DV_TRY(rms_ratio_dev(W, n, W.tmp, W.s, 0, W.scal + 13, st));
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.r));
+        DV_TRY(rms_ratio_dev(W, n, W.r, W.s, 0, W.scal + 14, st));
+        if (C.o.cons_tol > 0.0) {
+            scale(W.zt, W.w);
+            // into scal[16..23]: scal[0..1] still feed the matvec of a GMRES rerun after a refresh
+            DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<1, VB, 0, st>>>(m->p, W.Rt, W.w, W.scal + 16));
+        }
+        DV_CUDA(cudaMemcpyAsync(W.hpin + 16, W.scal, sizeof(double) * 32, cudaMemcpyDeviceToHost, st));
+        return DV_OK;
+    };
+
     DV_TRY(copy(z0, W.z));
     DV_TRY(stage(W.z, W.f, W.R));
     scale(W.z, W.s);
@@ -1163,10 +1212,19 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         const double floor_ = (polish ? 1e-4 : 0.1 * kappa) * sqrt_n;
         int info = 0;
         int64_t inner = 0;
-        DV_TRY(gmres_any(W, op, W.b, polish ? 1e-3 : C.o.eta, floor_, C.o.krylov_dim, &info, &inner, st));
+        bool pending = false;
+        DV_TRY(gmres_start(W, op, W.b, polish ? 1e-3 : C.o.eta, floor_, C.o.krylov_dim, &info, &inner, &pending, st));
+        // the full step (lam = 1) and every norm the host tests next, queued behind GMRES, read
+        // back with one synchronisation (same kernels and inputs as evaluating them one by one)
+        DV_TRY(speculate());
+        DV_CUDA(cudaStreamSynchronize(st));
+        if (pending) DV_TRY(gmres_graph_collect(W, m, &info, &inner));
+        bool spec_ok = true;
         if (polish) r.gmres_polish += inner;
         else { r.gmres_iters += inner; if (C.gm_counter) *C.gm_counter += inner; }
         if (info != 0 && C.o.allow_refresh && !new_lu && !polish) {
+            spec_ok = false;                                 // factors change: the speculation is void
+            m->nfev -= 1;                                    // (its residual evaluation is not counted)
             DV_TRY(refresh_J(C, t, W.z, dh, st));
             new_lu = true;
             r.refreshed = 1;
@@ -1177,11 +1235,13 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             r.gmres_iters += inner2;
             if (C.gm_counter) *C.gm_counter += inner2;
         }
+        if (!spec_ok) {
+            DV_TRY(speculate());
+            DV_CUDA(cudaStreamSynchronize(st));
+        }
+        const double* sv = W.hpin + 16;                      // speculated scalars (see speculate)
         // dz = prec(w) * s
-        DV_TRY(precond_apply(m, W.x, W.s, W.u, st));
-        DV_LAUNCH(dv::K_VECTOR, st, k_mul<<<g, VB, 0, st>>>(n, W.u, W.s, W.dz));
-        double dzn;
-        DV_TRY(rms_ratio(W, n, W.dz, nullptr, &dzn, st));
+        const double dzn = sv[11];
         if (!std::isfinite(dzn)) {
             DV_TRY(copy(z0, zout));
             r.iters = it + 1;
@@ -1190,11 +1250,16 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         }
         double lam = 1.0, rn_try = 0.0, pn_try = INFINITY;
         for (int ls = 0; ls < 4; ++ls) {
-            DV_LAUNCH(dv::K_VECTOR, st, k_truncate<<<g, VB, 0, st>>>(n, C.npos, W.z, lam, W.dz, W.zt));
-            DV_TRY(stage(W.zt, W.ft, W.Rt));
-            DV_TRY(rms_ratio(W, n, W.Rt, W.s, &rn_try, st));
-            if (std::isfinite(rn_try)) DV_TRY(pnorm(W.Rt, W.s, &pn_try));
-            else pn_try = INFINITY;
+            if (ls == 0) {                                   // lam = 1: already evaluated
+                rn_try = sv[12];
+                pn_try = std::isfinite(rn_try) ? sv[13] : INFINITY;
+            } else {
+                DV_LAUNCH(dv::K_VECTOR, st, k_truncate<<<g, VB, 0, st>>>(n, C.npos, W.z, lam, W.dz, W.zt));
+                DV_TRY(stage(W.zt, W.ft, W.Rt));
+                DV_TRY(rms_ratio(W, n, W.Rt, W.s, &rn_try, st));
+                if (std::isfinite(rn_try)) DV_TRY(pnorm(W.Rt, W.s, &pn_try));
+                else pn_try = INFINITY;
+            }
             if (std::isfinite(pn_try) && (pn_try <= (1.0 - 1e-4 * lam) * pn || ls == 3)) break;
             lam *= 0.5;
         }
@@ -1205,9 +1270,14 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             return DV_OK;
         }
         // step = rms((z_try - z)/s)
-        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.tmp));
         double step;
-        DV_TRY(rms_ratio(W, n, W.tmp, W.s, &step, st));
+        if (lam == 1.0) {
+            step = sv[14];
+        } else {
+            DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.tmp));
+            DV_TRY(rms_ratio(W, n, W.tmp, W.s, &step, st));
+        }
+        const bool cons_spec = (lam == 1.0);
         // accept the trial point (copies, not pointer swaps: the GMRES graph is built on these addresses)
         DV_TRY(copy(W.zt, W.z));
         DV_TRY(copy(W.ft, W.f));
@@ -1226,7 +1296,8 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
                 DV_TRY(copy(W.z, W.best));
             }
             bool ok;
-            DV_TRY(cons_ok(W.R, W.z, &ok));
+            if (cons_spec) ok = cons_eval(sv + 16);
+            else DV_TRY(cons_ok(W.R, W.z, &ok));
             if (ok) {
                 DV_TRY(copy(W.z, zout));
                 r.ok = 1; r.iters = it + 1; r.rate = rate;
