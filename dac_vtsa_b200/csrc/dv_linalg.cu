@@ -580,22 +580,21 @@ static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) 
 // j < NJ, are a fixed, fully unrolled batch of loads (padding columns hold zeros).
 #define PA_THREADS 512
 #define PA_LANES 8
-template <int NJ>
+template <int NJ, int NBUF>
 __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const double* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
                                                          double* __restrict__ x, int* __restrict__ err, PaFuse F) {
     extern __shared__ __align__(128) double dsm[];
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t bars[NBUF];
     constexpr int LD = NJ * PA_LANES;
     const int part = blockIdx.x;
     const PcGeom g = pc_part(gin, part);
     const int nb = g.nb;
     const int tid = threadIdx.x;
     const int64_t bs = g.bs;
-    double* xs = dsm;                          // [Nz][LD]: b, then z, then x (padding zero)
-    double* tv = xs + (int64_t)g.Nz * LD;      // [LD]
-    double* buf0 = tv + LD;                    // [3 bs]
-    double* buf1 = buf0 + 3 * bs;
+    double* xs = dsm;                          // [Nz][LD]: b, then z (forward sweep, in place)
+    double* xb = xs + (int64_t)g.Nz * LD;      // [Nz][LD]: x (backward sweep); padding columns zero
+    double* buf0 = xb + (int64_t)g.Nz * LD;    // NBUF ring buffers of [3 bs]: stage s uses buffer s % NBUF
     const double* base = A + (int64_t)part * g.Nz * 5 * bs;
     const int S = 2 * g.Nz - 1;                // stages: forward 1..Nz-1, backward Nz-1..0
     auto stage_src = [&](int s) -> const double* {
@@ -607,15 +606,13 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
         return (uint32_t)(((s < g.Nz - 1) ? 2 : 3) * bs * sizeof(double));
     };
     if (tid == 0) {
-        mbar_init(smem_u32(&bars[0]), 1);
-        mbar_init(smem_u32(&bars[1]), 1);
+        for (int q = 0; q < NBUF; ++q) mbar_init(smem_u32(&bars[q]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0) {
-        bulk_load(smem_u32(buf0), stage_src(0), stage_bytes(0), smem_u32(&bars[0]));
-        if (S > 1) bulk_load(smem_u32(buf1), stage_src(1), stage_bytes(1), smem_u32(&bars[1]));
-    }
+    if (tid == 0)                                // the first NBUF stages are in flight from the start
+        for (int q = 0; q < NBUF && q < S; ++q)
+            bulk_load(smem_u32(buf0 + (int64_t)q * 3 * bs), stage_src(q), stage_bytes(q), smem_u32(&bars[q]));
     const int fcol = F.V ? *F.col : 0;
     const double fscale = F.V ? *F.scale : 0.0;
     const double* fsrc = (fcol == 0) ? F.src0 : F.src1;
@@ -635,19 +632,33 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
         }
         xs[q] = v;
     }
-    if (tid < LD) tv[tid] = 0.0;
+    for (int q = tid; q < g.Nz * LD; q += blockDim.x) xb[q] = 0.0;
     __syncthreads();
     const int lane = tid % PA_LANES;
     const int r = tid / PA_LANES;              // one row per 8 lanes: 64 rows (nb <= 64)
     bool ok = true;
+    int s_fail = S;
+    int issued = (S < NBUF) ? S : NBUF;        // stages whose copies have been issued
+    // One barrier per stage: it publishes the previous stage's rows and frees its buffer, which is
+    // refilled right after it.  Forward rows overwrite b_k by z_k in xs (each row reads and writes
+    // only its own entry of plane k); backward rows go to xb, as every row reads all of z_k.
     for (int s = 0; s < S; ++s) {
-        const int bi = s & 1;
-        const double* buf = bi ? buf1 : buf0;
-        const bool arrived = mbar_wait(smem_u32(&bars[bi]), (uint32_t)((s >> 1) & 1));
+        const int bi = s % NBUF;
+        double* buf = buf0 + (int64_t)bi * 3 * bs;
+        const bool arrived = mbar_wait(smem_u32(&bars[bi]), (uint32_t)((s / NBUF) & 1));
         if (!__syncthreads_and(arrived)) {       // uniform decision: no thread is left at a barrier
             ok = false;
+            s_fail = s;
             if (tid == 0) atomicOr(err, 1);
             break;
+        }
+        if (s >= 1 && s - 1 + NBUF < S) {        // the previous stage's buffer is free: refill it
+            if (tid == 0) {
+                const int sn = s - 1 + NBUF, bn = (s - 1) % NBUF;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                bulk_load(smem_u32(buf0 + (int64_t)bn * 3 * bs), stage_src(sn), stage_bytes(sn), smem_u32(&bars[bn]));
+            }
+            issued = s + NBUF;
         }
         const bool fwd = s < g.Nz - 1;
         const int k = fwd ? s + 1 : g.Nz - 1 - (s - (g.Nz - 1));
@@ -671,13 +682,13 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
                 for (int j = 0; j < NJ; ++j) acc += m0[lane + PA_LANES * j] * v0[lane + PA_LANES * j];
                 if (k + 1 < g.Nz) {
                     const double* m1 = buf + bs + r * LD;
-                    const double* v1 = xs + (int64_t)(k + 1) * LD;
+                    const double* v1 = xb + (int64_t)(k + 1) * LD;
 #pragma unroll
                     for (int j = 0; j < NJ; ++j) acc += m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
                 }
                 if (k + 2 < g.Nz) {
                     const double* m2 = buf + 2 * bs + r * LD;
-                    const double* v2 = xs + (int64_t)(k + 2) * LD;
+                    const double* v2 = xb + (int64_t)(k + 2) * LD;
 #pragma unroll
                     for (int j = 0; j < NJ; ++j) acc += m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
                 }
@@ -685,27 +696,23 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
         }
 #pragma unroll
         for (int off = PA_LANES / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, PA_LANES);
-        if (r < nb && lane == 0) tv[r] = fwd ? xs[(int64_t)k * LD + r] - acc : acc;
-        __syncthreads();                         // every thread is done with `buf` and with xs reads
-        if (tid < nb) xs[(int64_t)k * LD + tid] = tv[tid];
-        if (tid == 0 && s + 2 < S) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            bulk_load(smem_u32(buf), stage_src(s + 2), stage_bytes(s + 2), smem_u32(&bars[bi]));
+        if (r < nb && lane == 0) {
+            if (fwd) xs[(int64_t)k * LD + r] = xs[(int64_t)k * LD + r] - acc;
+            else xb[(int64_t)k * LD + r] = acc;
         }
-        __syncthreads();
     }
+    __syncthreads();                             // the last stage's rows
     double ss = 0.0;
     if (!ok) {                                   // drain copies still in flight (bounded) and leave x untouched
-        if (tid == 0) {
-            mbar_wait(smem_u32(&bars[0]), 0);
-            mbar_wait(smem_u32(&bars[1]), 0);
-        }
+        if (tid == 0)
+            for (int s2 = s_fail; s2 < issued; ++s2)
+                mbar_wait(smem_u32(&bars[s2 % NBUF]), (uint32_t)((s2 / NBUF) & 1));
     } else {
         for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
             const int k = q / LD, l = q - k * LD;
             if (l < nb) {
                 const int64_t gi = pc_glob(g, part, k, l);
-                const double xv = sc ? xs[q] / sc[gi] : xs[q];
+                const double xv = sc ? xb[q] / sc[gi] : xb[q];
                 x[gi] = xv;
                 ss += xv * xv;
             }
@@ -868,13 +875,42 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
     return DV_OK;
 }
 
+// shared memory of the sweep with an NBUF-deep ring: solution planes, one plane of scratch, buffers
+static size_t apply_smem(const PcGeom& g, int nbuf) {
+    return sizeof(double) * (size_t)(2 * (int64_t)g.Nz * g.ld + (int64_t)nbuf * 3 * g.bs);
+}
+
+// ring depth: three stages in flight when they fit in shared memory, else two
+static int apply_nbuf(const PcGeom& g) { return apply_smem(g, 3) <= (size_t)smem_optin() ? 3 : 2; }
+
+template <int NJ, int NBUF>
+static void launch_apply_k(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
+                           const PaFuse& F, bool count) {
+    const size_t dyn = apply_smem(g, NBUF);
+    if (count) {
+        if (dyn > 48 * 1024)
+            cudaFuncSetAttribute(k_pc_apply<NJ, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ, NBUF><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F));
+    } else {
+        k_pc_apply<NJ, NBUF><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F);
+    }
+}
+
 template <int NJ>
-static int launch_apply(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
-                        size_t dyn) {
-    if (dyn > 48 * 1024)
-        DV_CUDA(cudaFuncSetAttribute(k_pc_apply<NJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-    DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, PaFuse()));
-    return DV_OK;
+static void launch_apply_nj(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
+                            const PaFuse& F, bool count) {
+    if (apply_nbuf(g) == 3) launch_apply_k<NJ, 3>(g, m, b, sc, x, s, F, count);
+    else launch_apply_k<NJ, 2>(g, m, b, sc, x, s, F, count);
+}
+
+static void launch_apply(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
+                         const PaFuse& F, bool count) {
+    switch (g.ld / PA_LANES) {
+        case 1: launch_apply_nj<1>(g, m, b, sc, x, s, F, count); break;
+        case 3: launch_apply_nj<3>(g, m, b, sc, x, s, F, count); break;
+        case 5: launch_apply_nj<5>(g, m, b, sc, x, s, F, count); break;
+        default: launch_apply_nj<7>(g, m, b, sc, x, s, F, count); break;
+    }
 }
 
 int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s) {
@@ -883,17 +919,8 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
         return DV_ERR_ARG;
     }
     PcGeom g = geom_of(m, m->pc_mode);
-    const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
-    const int nj = g.ld / PA_LANES;
-    if (g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7)) {
-        int rc = DV_OK;
-        switch (nj) {
-            case 1: rc = launch_apply<1>(g, m, b, sc, x, s, dyn); break;
-            case 3: rc = launch_apply<3>(g, m, b, sc, x, s, dyn); break;
-            case 5: rc = launch_apply<5>(g, m, b, sc, x, s, dyn); break;
-            default: rc = launch_apply<7>(g, m, b, sc, x, s, dyn); break;
-        }
-        if (rc != DV_OK) return rc;
+    if (precond_apply_fusable(m)) {
+        launch_apply(g, m, b, sc, x, s, PaFuse(), true);
     } else {
         DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply_glob<<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work));
     }
@@ -903,23 +930,15 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
 
 bool precond_apply_fusable(dv_model* m) {
     PcGeom g = geom_of(m, m->pc_mode);
-    const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
     const int nj = g.ld / PA_LANES;
-    return g.nb <= 64 && dyn <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7);
+    return g.nb <= 64 && apply_smem(g, 2) <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7);
 }
 
 int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
                           const PaFuse& F) {
     PcGeom g = geom_of(m, m->pc_mode);
-    const size_t dyn = sizeof(double) * (size_t)((int64_t)g.Nz * g.ld + g.ld + 6 * g.bs);
-    const int nj = g.ld / PA_LANES;
     if (precond_apply_fusable(m)) {
-        switch (nj) {
-            case 1: k_pc_apply<1><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
-            case 3: k_pc_apply<3><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
-            case 5: k_pc_apply<5><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
-            default: k_pc_apply<7><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F); break;
-        }
+        launch_apply(g, m, b, sc, x, s, F, false);    // attributes were set by an earlier precond_apply
     } else {
         if (F.V || F.out) {
             set_error("fused sweep requested for a partition the shared-memory sweep does not take");
