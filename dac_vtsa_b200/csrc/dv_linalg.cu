@@ -247,75 +247,85 @@ static __device__ void sm_bd_right(const PcGeom& g, double alpha, const double* 
 
 // In-place Gauss-Jordan inverse (row-major, nb <= 64) with partial pivoting; returns 1 on a zero /
 // non-finite pivot (replaced by 1 so the factors stay finite; reported through the info flag).
-static __device__ int sm_inverse(int nb, int ld, double* A, int* perm, double* fcol, double* prow, int* sp) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int tx = tid % SM_T, ty = tid / SM_T;
+// In-place Gauss-Jordan inverse with partial pivoting of the nb x nb block *A (shared memory, nb <=
+// 64, 256 threads), ping-ponging between *A and *B (same size).  Thread t updates column t % 64 on
+// the rows congruent to t / 64 modulo 4 (coalesced row accesses, broadcast column-k reads); the
+// threads of column k+1 also keep the running maxima of its new entries (rows > k), so the next
+// pivot is known after the one barrier of the step.  The pivot is the largest |entry|, the
+// smallest row index among equal ones.  The row interchanges are undone at the end by a single
+// column gather.  On return *A holds the inverse (the pointers may have been exchanged).
+static __device__ int sm_inverse(int nb, int ld, double*& A, double*& B, int* perm, int* idx, double* pv, int* pi) {
+    const int tid = threadIdx.x;
+    const int cc = tid & 63, rq = tid >> 6;
+    constexpr int RPT = 16;                       // rows per thread for nb <= 64
     int bad = 0;
-    for (int k = 0; k < nb; ++k) {
-        if (warp == 0) {                          // pivot row: largest |A[i][k]|, i >= k
-            double best = -1.0;
-            int bi = k;
-            for (int i = k + lane; i < nb; i += 32) {
-                double v = fabs(A[i * ld + k]);
-                if (v > best) { best = v; bi = i; }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                double ov = __shfl_down_sync(0xffffffffu, best, off);
-                int oi = __shfl_down_sync(0xffffffffu, bi, off);
-                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-            }
-            if (lane == 0) { sp[0] = bi; perm[k] = bi; }
+    if (cc == 0) {                                // column 0: partial maxima per row group
+        double best = -1.0;
+        int bi = nb;
+        for (int i = rq; i < nb; i += 4) {
+            const double v = fabs(A[i * ld]);
+            if (v > best) { best = v; bi = i; }
         }
-        __syncthreads();
-        const int p = sp[0];
+        pv[rq] = best;
+        pi[rq] = bi;
+    }
+    __syncthreads();
+    for (int k = 0; k < nb; ++k) {
+        const double* cpv = pv + 4 * (k & 1);
+        const int* cpi = pi + 4 * (k & 1);
+        double best = cpv[0];
+        int p = cpi[0];
+#pragma unroll
+        for (int q = 1; q < 4; ++q)
+            if (cpv[q] > best || (cpv[q] == best && cpi[q] < p)) { best = cpv[q]; p = cpi[q]; }
+        if (tid == 0) perm[k] = p;
         double piv = A[p * ld + k];
         if (!(fabs(piv) > 0.0) || !isfinite(piv)) { bad = 1; piv = 1.0; }
         const double inv = 1.0 / piv;
-        if (tid < nb) {                           // scaled pivot row and old column k (rows k, p exchanged)
-            const int c = tid;
-            prow[c] = ((c == k) ? 1.0 : A[p * ld + c]) * inv;
-            const int i = tid;
-            const int src = (i == k) ? p : ((i == p) ? k : i);
-            fcol[i] = (i == k) ? 0.0 : A[src * ld + k];
-        }
-        __syncthreads();
-        double keep[SM_R][SM_R];
+        if (cc < nb) {
+            const double pr = ((cc == k) ? 1.0 : A[p * ld + cc]) * inv;     // scaled pivot row
+            const bool nextcol = (cc == k + 1);
+            double nbest = -1.0;
+            int nbi = nb;
 #pragma unroll
-        for (int a = 0; a < SM_R; ++a) {
-            const int i = ty + SM_T * a;
-            if (i >= nb) continue;
-            const int src = (i == k) ? p : ((i == p) ? k : i);
-#pragma unroll
-            for (int b = 0; b < SM_R; ++b) {
-                const int c = tx + SM_T * b;
-                if (c >= nb) continue;
-                if (i == k) keep[a][b] = prow[c];
-                else keep[a][b] = ((c == k) ? 0.0 : A[src * ld + c]) - fcol[i] * prow[c];
+            for (int a = 0; a < RPT; ++a) {
+                const int i = rq + 4 * a;
+                if (i >= nb) break;
+                double val;
+                if (i == k) {
+                    val = pr;
+                } else {
+                    const int src = (i == p) ? k : i;                      // rows k and p exchanged
+                    const double fc = A[src * ld + k];                     // old column k
+                    val = ((cc == k) ? 0.0 : A[src * ld + cc]) - fc * pr;
+                }
+                B[i * ld + cc] = val;
+                if (nextcol && i > k) {
+                    const double v = fabs(val);
+                    if (v > nbest) { nbest = v; nbi = i; }
+                }
+            }
+            if (nextcol) {
+                pv[4 * ((k + 1) & 1) + rq] = nbest;
+                pi[4 * ((k + 1) & 1) + rq] = nbi;
             }
         }
         __syncthreads();
-#pragma unroll
-        for (int a = 0; a < SM_R; ++a) {
-            const int i = ty + SM_T * a;
-            if (i >= nb) continue;
-#pragma unroll
-            for (int b = 0; b < SM_R; ++b) {
-                const int c = tx + SM_T * b;
-                if (c < nb) A[i * ld + c] = keep[a][b];
-            }
-        }
-        __syncthreads();
+        double* t = A; A = B; B = t;
     }
-    for (int k = nb - 1; k >= 0; --k) {           // undo the row interchanges as column interchanges
-        const int p = perm[k];
-        if (p != k && tid < nb) {
-            double t = A[tid * ld + k];
-            A[tid * ld + k] = A[tid * ld + p];
-            A[tid * ld + p] = t;
+    if (tid == 0) {                               // the row interchanges, undone as column interchanges
+        for (int c = 0; c < nb; ++c) idx[c] = c;
+        for (int k = nb - 1; k >= 0; --k) {
+            const int q = perm[k], t = idx[k];
+            idx[k] = idx[q];
+            idx[q] = t;
         }
-        __syncthreads();
     }
+    __syncthreads();
+    if (cc < nb)
+        for (int i = rq; i < nb; i += 4) B[i * ld + cc] = A[i * ld + idx[cc]];
+    __syncthreads();
+    double* t = A; A = B; B = t;
     return bad;
 }
 
@@ -327,9 +337,9 @@ static __device__ void cp_block(int64_t n, const double* src, double* dst) {
 __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __restrict__ A, int* __restrict__ info) {
     const PcGeom g = pc_part(gin, (int)blockIdx.x);
     extern __shared__ __align__(16) double dsm[];
-    __shared__ int perm[64];
-    __shared__ double fcol[64], prow[64];
-    __shared__ int sp[1];
+    __shared__ int perm[64], idx[64];
+    __shared__ double pv[8];
+    __shared__ int pi[8];
     const int nb = g.nb, ld = g.ld;
     const int n2 = nb * ld;
     double* buf[9];
@@ -365,7 +375,7 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
             sm_gemm(nb, ld, -1.0, S1, U11, 1.0, S2);                           // D -= L1 U1_{k-1}
             sm_bd_right(g, -1.0, S1, U2_1, 1.0, S3);                           // U1 = A(k,k+1) - L1 U2_{k-1}
         }
-        bad |= sm_inverse(nb, ld, S2, perm, fcol, prow, sp);
+        bad |= sm_inverse(nb, ld, S2, T, perm, idx, pv, pi);              // (T: ping-pong buffer)
         sm_gemm(nb, ld, -1.0, S2, S3, 0.0, T);                                 // -Uinv_k U1_k
         if (k >= 2) cp_block(n2, S0, Ak);
         if (k >= 1) cp_block(n2, S1, Ak + g.bs);
