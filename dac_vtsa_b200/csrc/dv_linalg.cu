@@ -156,42 +156,59 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
 #define SM_T 16
 #define SM_R 4
 
-// C = beta C + alpha A B (all row-major in shared memory, leading dimension ld, nb <= 64)
+// D = A B + D on the FP64 tensor cores: one 8x8x4 product per warp instruction.  Fragments
+// (lane = 4 g + t): a = A[g][t], b = B[t][g], d = D[g][2t .. 2t+1].
+static __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// C = beta C + alpha A B (row-major in shared memory, leading dimension ld, nb <= 64, alpha = +-1):
+// 8x8 output tiles dealt round-robin to the warps; a warp accumulates all of its tiles together
+// (independent DMMA chains) over k in steps of 4; entries beyond nb read as zero, are not written.
 static __device__ void sm_gemm(int nb, int ld, double alpha, const double* A, const double* B, double beta,
                                double* C) {
-    const int tx = threadIdx.x % SM_T, ty = threadIdx.x / SM_T;
-    double acc[SM_R][SM_R];
+    constexpr int TPW = 8;                        // tiles per warp: 64 tiles of nb <= 64 over 8 warps
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int nt = (nb + 7) >> 3;
+    const int ntile = nt * nt;
+    int ra[TPW], cbv[TPW];                        // this lane's A row offset and B column per tile (-1: none)
+    double d[TPW][2];
 #pragma unroll
-    for (int a = 0; a < SM_R; ++a)
+    for (int q = 0; q < TPW; ++q) {
+        const int tile = warp + q * nw;
+        const int ti = tile / nt, tj = tile - ti * nt;
+        const int r = 8 * ti + g, cb = 8 * tj + g;
+        ra[q] = (tile < ntile && r < nb) ? r * ld : -1;
+        cbv[q] = (tile < ntile && cb < nb) ? cb : -1;
+        d[q][0] = d[q][1] = 0.0;
+    }
+    const int nq = (ntile - warp + nw - 1) / nw;  // tiles of this warp
+    for (int kk = 0; kk < nb; kk += 4) {
+        const int ka = kk + t4;
+        const bool kin = ka < nb;
+        const double* Bk = B + ka * ld;
 #pragma unroll
-        for (int b = 0; b < SM_R; ++b) acc[a][b] = 0.0;
-    for (int q = 0; q < nb; ++q) {
-        double av[SM_R], bv[SM_R];
-#pragma unroll
-        for (int a = 0; a < SM_R; ++a) {
-            const int r = ty + SM_T * a;
-            av[a] = (r < nb) ? A[r * ld + q] : 0.0;
+        for (int q = 0; q < TPW; ++q) {
+            if (q < nq) {
+                const double a = (kin && ra[q] >= 0) ? alpha * A[ra[q] + ka] : 0.0;
+                const double b = (kin && cbv[q] >= 0) ? Bk[cbv[q]] : 0.0;
+                dmma_884(d[q][0], d[q][1], a, b);
+            }
         }
-#pragma unroll
-        for (int b = 0; b < SM_R; ++b) {
-            const int c = tx + SM_T * b;
-            bv[b] = (c < nb) ? B[q * ld + c] : 0.0;
-        }
-#pragma unroll
-        for (int a = 0; a < SM_R; ++a)
-#pragma unroll
-            for (int b = 0; b < SM_R; ++b) acc[a][b] += av[a] * bv[b];
     }
 #pragma unroll
-    for (int a = 0; a < SM_R; ++a) {
-        const int r = ty + SM_T * a;
-        if (r >= nb) continue;
-#pragma unroll
-        for (int b = 0; b < SM_R; ++b) {
-            const int c = tx + SM_T * b;
-            if (c >= nb) continue;
-            double* cp = C + r * ld + c;
-            *cp = (beta == 0.0) ? alpha * acc[a][b] : beta * (*cp) + alpha * acc[a][b];
+    for (int q = 0; q < TPW; ++q) {
+        if (q >= nq) continue;
+        const int tile = warp + q * nw;
+        const int ti = tile / nt, tj = tile - ti * nt;
+        const int r = 8 * ti + g, c0 = 8 * tj + 2 * t4;
+        if (r < nb) {
+            double* cp = C + r * ld + c0;
+            if (c0 < nb) cp[0] = (beta == 0.0) ? d[q][0] : beta * cp[0] + d[q][0];
+            if (c0 + 1 < nb) cp[1] = (beta == 0.0) ? d[q][1] : beta * cp[1] + d[q][1];
         }
     }
     __syncthreads();
@@ -254,7 +271,7 @@ static __device__ void sm_bd_right(const PcGeom& g, double alpha, const double* 
 // pivot is known after the one barrier of the step.  The pivot is the largest |entry|, the
 // smallest row index among equal ones.  The row interchanges are undone at the end by a single
 // column gather.  On return *A holds the inverse (the pointers may have been exchanged).
-static __device__ int sm_inverse(int nb, int ld, double*& A, double*& B, int* perm, int* idx, double* pv, int* pi) {
+static __device__ int sm_inverse_unb(int nb, int ld, double*& A, double*& B, int* perm, int* idx, double* pv, int* pi) {
     const int tid = threadIdx.x;
     const int cc = tid & 63, rq = tid >> 6;
     constexpr int RPT = 16;                       // rows per thread for nb <= 64
@@ -327,6 +344,158 @@ static __device__ int sm_inverse(int nb, int ld, double*& A, double*& B, int* pe
     __syncthreads();
     double* t = A; A = B; B = t;
     return bad;
+}
+
+// Blocked Gauss-Jordan inverse with partial pivoting of the nb x nb block *A (shared memory, nb <=
+// 64, 256 threads, leading dimension ld); *B (same size) is scratch.  Columns are processed in
+// panels of 8: the pivot steps of a panel run on a small column-major copy of its columns (one
+// barrier per step, the next pivot found by the warp that updates its column), then the panel's
+// row interchanges are applied to the other columns, the panel's pivot rows are set aside and the
+// other columns receive the panel's combined transformation as one rank-8 DMMA update:
+//   x <- [x with the pivot rows zeroed] + Panel * x(pivot rows).
+// The pivot is the largest |entry|, the smallest row index among equal ones.  The row
+// interchanges are undone at the end by one column gather.  On return *A holds the inverse (the
+// pointers may have been exchanged).
+static __device__ int sm_inverse_blk(int nb, int ld, double*& A, double*& B, int* perm, int* idx, int* pi) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* P0 = B;                               // panel copies: [8][nb] column-major, ping-pong
+    double* P1 = B + nb * 8;
+    double* Bs = B + 2 * nb * 8;                  // the panel's pivot rows: [8][ld] (fits: see sm_inverse)
+    int bad = 0;
+    for (int j0 = 0; j0 < nb; j0 += 8) {
+        const int jb = min(8, nb - j0);
+        for (int q = tid; q < nb * 8; q += blockDim.x) {       // panel copy
+            const int cq = q / nb, i = q - cq * nb;
+            P0[q] = (cq < jb) ? A[i * ld + j0 + cq] : 0.0;
+        }
+        if (warp == 0) {                          // pivot of the panel's first column
+            double best = -1.0;
+            int bi = nb;
+            for (int i = j0 + lane; i < nb; i += 32) {
+                const double v = fabs(A[i * ld + j0]);
+                if (v > best) { best = v; bi = i; }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, off);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) pi[0] = bi;
+        }
+        __syncthreads();
+        double* Pc = P0;
+        double* Pn = P1;
+        for (int kq = 0; kq < jb; ++kq) {         // pivot steps of the panel: warp w updates column w
+            const int k = j0 + kq;
+            const int p = pi[kq & 1];
+            if (tid == 0) perm[k] = p;
+            double piv = Pc[kq * nb + p];
+            if (!(fabs(piv) > 0.0) || !isfinite(piv)) { bad = 1; piv = 1.0; }
+            const double inv = 1.0 / piv;
+            const int cq = warp;
+            double best = -1.0;
+            int bi = nb;
+            if (cq < jb) {
+                const double pr = ((cq == kq) ? 1.0 : Pc[cq * nb + p]) * inv;
+                for (int i = lane; i < nb; i += 32) {
+                    double val;
+                    if (i == k) {
+                        val = pr;
+                    } else {
+                        const int src = (i == p) ? k : i;
+                        val = ((cq == kq) ? 0.0 : Pc[cq * nb + src]) - Pc[kq * nb + src] * pr;
+                    }
+                    Pn[cq * nb + i] = val;
+                    if (cq == kq + 1 && i > k) {
+                        const double v = fabs(val);
+                        if (v > best) { best = v; bi = i; }
+                    }
+                }
+            }
+            if (cq == kq + 1) {                   // the next pivot (warp-uniform branch)
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    const double ov = __shfl_down_sync(0xffffffffu, best, off);
+                    const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+                }
+                if (lane == 0) pi[(kq + 1) & 1] = bi;
+            }
+            __syncthreads();
+            double* t = Pc; Pc = Pn; Pn = t;
+        }
+        if (tid < nb && (tid < j0 || tid >= j0 + jb)) {    // the panel's row interchanges elsewhere
+            const int c = tid;
+            for (int kq = 0; kq < jb; ++kq) {
+                const int k = j0 + kq, p = perm[k];
+                if (p != k) {
+                    const double t = A[k * ld + c];
+                    A[k * ld + c] = A[p * ld + c];
+                    A[p * ld + c] = t;
+                }
+            }
+        }
+        __syncthreads();
+        for (int q = tid; q < 8 * ld; q += blockDim.x) {   // set the pivot rows aside
+            const int kq = q / ld, c = q - kq * ld;
+            double v = 0.0;
+            if (kq < jb && c < nb && (c < j0 || c >= j0 + jb)) {
+                v = A[(j0 + kq) * ld + c];
+                A[(j0 + kq) * ld + c] = 0.0;
+            }
+            Bs[q] = v;
+        }
+        __syncthreads();
+        {                                         // other columns += Panel * Bs; panel columns <- Panel
+            const int g = lane >> 2, t4 = lane & 3;
+            const int nt = (nb + 7) >> 3;
+            for (int tile = warp; tile < nt * nt; tile += (int)(blockDim.x >> 5)) {
+                const int ti = tile / nt, tj = tile - ti * nt;
+                const int r = 8 * ti + g, cb = 8 * tj + g, c0 = 8 * tj + 2 * t4;
+                double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < 8; kk += 4) {
+                    const double a = (r < nb && kk + t4 < jb) ? Pc[(kk + t4) * nb + r] : 0.0;
+                    const double b = (cb < nb) ? Bs[(kk + t4) * ld + cb] : 0.0;
+                    dmma_884(d0, d1, a, b);
+                }
+                if (r < nb) {
+                    double* cp = A + r * ld;
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int c = c0 + e;
+                        if (c >= nb) continue;
+                        if (c >= j0 && c < j0 + jb) cp[c] = Pc[(c - j0) * nb + r];
+                        else cp[c] += (e == 0) ? d0 : d1;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {                               // the row interchanges, undone as column interchanges
+        for (int c = 0; c < nb; ++c) idx[c] = c;
+        for (int k = nb - 1; k >= 0; --k) {
+            const int q = perm[k], t = idx[k];
+            idx[k] = idx[q];
+            idx[q] = t;
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < nb * nb; q += blockDim.x) {
+        const int i = q / nb, c = q - i * nb;
+        B[i * ld + c] = A[i * ld + idx[c]];
+    }
+    __syncthreads();
+    double* t = A; A = B; B = t;
+    return bad;
+}
+
+// Inverse of the nb x nb block *A: blocked when *B can hold the panel copies and pivot rows.
+static __device__ int sm_inverse(int nb, int ld, double*& A, double*& B, int* perm, int* idx, double* pv, int* pi) {
+    if (16 * nb + 8 * ld <= nb * ld) return sm_inverse_blk(nb, ld, A, B, perm, idx, pi);
+    return sm_inverse_unb(nb, ld, A, B, perm, idx, pv, pi);
 }
 
 static __device__ void cp_block(int64_t n, const double* src, double* dst) {
