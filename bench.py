@@ -139,6 +139,22 @@ def reference_arm(a, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------- ranks
+def max_over_ranks(x, dist=None, device=None):
+    """Max of a per-rank number over all ranks (a job's time is its slowest rank's)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, cycles, seconds):
+    """Whole-job bed-seconds per wall-second: every rank runs `cycles` independent cycles."""
+    return world * cycles * CYCLE_BED_S / seconds
+
+
 # ---------------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
@@ -277,11 +293,8 @@ def gpu_arm(a, rank, world, local_rank):
     barrier()
     launches = _lib.launch_count() - launches0
     clocks = sampler.stop()
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    value = world * a.steps * CYCLE_BED_S / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, dist, dev)
+    value = replica_throughput(world, a.steps, total_ms / 1e3)
     # ---- e2e: public step-runner API, host states, outlet recording per accepted step
     counters.reset()
     barrier()
@@ -292,11 +305,8 @@ def gpu_arm(a, rank, world, local_rank):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     nE = max(1, a.e2e_steps)
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_s = float(t.item())
-    e2e = {"value": world * nE * CYCLE_BED_S / e2e_s, "unit": "bed-s/wall-s",
+    e2e_s = max_over_ranks(e2e_s, dist, dev)
+    e2e = {"value": replica_throughput(world, nE, e2e_s), "unit": "bed-s/wall-s",
            "h2d_bytes_per_step": counters.TRAFFIC["h2d"] // nE, "d2h_bytes_per_step": counters.TRAFFIC["d2h"] // nE,
            "path": "runner.run_cycle (steps/_runner.py-compatible run_step per cycle step, outlet recorded at "
                    "every accepted step)"}

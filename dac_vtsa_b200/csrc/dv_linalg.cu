@@ -165,50 +165,30 @@ static __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a
 }
 
 // C = beta C + alpha A B (row-major in shared memory, leading dimension ld, nb <= 64, alpha = +-1):
-// 8x8 output tiles dealt round-robin to the warps; a warp accumulates all of its tiles together
-// (independent DMMA chains) over k in steps of 4; entries beyond nb read as zero, are not written.
+// 8x8 output tiles spread over the warps, each accumulated by DMMA over k in steps of 4; entries
+// beyond nb read as zero and are not written.  (Accumulating all of a warp's tiles together
+// measured slower on B200: 5.8 us against 3.7 us for nb = 48.)
 static __device__ void sm_gemm(int nb, int ld, double alpha, const double* A, const double* B, double beta,
                                double* C) {
-    constexpr int TPW = 8;                        // tiles per warp: 64 tiles of nb <= 64 over 8 warps
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int g = lane >> 2, t4 = lane & 3;
     const int nt = (nb + 7) >> 3;
-    const int ntile = nt * nt;
-    int ra[TPW], cbv[TPW];                        // this lane's A row offset and B column per tile (-1: none)
-    double d[TPW][2];
-#pragma unroll
-    for (int q = 0; q < TPW; ++q) {
-        const int tile = warp + q * nw;
+    for (int tile = warp; tile < nt * nt; tile += nw) {
         const int ti = tile / nt, tj = tile - ti * nt;
-        const int r = 8 * ti + g, cb = 8 * tj + g;
-        ra[q] = (tile < ntile && r < nb) ? r * ld : -1;
-        cbv[q] = (tile < ntile && cb < nb) ? cb : -1;
-        d[q][0] = d[q][1] = 0.0;
-    }
-    const int nq = (ntile - warp + nw - 1) / nw;  // tiles of this warp
-    for (int kk = 0; kk < nb; kk += 4) {
-        const int ka = kk + t4;
-        const bool kin = ka < nb;
-        const double* Bk = B + ka * ld;
-#pragma unroll
-        for (int q = 0; q < TPW; ++q) {
-            if (q < nq) {
-                const double a = (kin && ra[q] >= 0) ? alpha * A[ra[q] + ka] : 0.0;
-                const double b = (kin && cbv[q] >= 0) ? Bk[cbv[q]] : 0.0;
-                dmma_884(d[q][0], d[q][1], a, b);
-            }
+        const int r = 8 * ti + g;                 // row of A and C held by this lane
+        const int cb = 8 * tj + g;                // column of B in the b fragment
+        const int c0 = 8 * tj + 2 * t4;           // columns of C in the d fragment
+        double d0 = 0.0, d1 = 0.0;
+        for (int kk = 0; kk < nb; kk += 4) {
+            const int ka = kk + t4;
+            const double a = (r < nb && ka < nb) ? alpha * A[r * ld + ka] : 0.0;
+            const double b = (ka < nb && cb < nb) ? B[ka * ld + cb] : 0.0;
+            dmma_884(d0, d1, a, b);
         }
-    }
-#pragma unroll
-    for (int q = 0; q < TPW; ++q) {
-        if (q >= nq) continue;
-        const int tile = warp + q * nw;
-        const int ti = tile / nt, tj = tile - ti * nt;
-        const int r = 8 * ti + g, c0 = 8 * tj + 2 * t4;
         if (r < nb) {
             double* cp = C + r * ld + c0;
-            if (c0 < nb) cp[0] = (beta == 0.0) ? d[q][0] : beta * cp[0] + d[q][0];
-            if (c0 + 1 < nb) cp[1] = (beta == 0.0) ? d[q][1] : beta * cp[1] + d[q][1];
+            if (c0 < nb) cp[0] = (beta == 0.0) ? d0 : beta * cp[0] + d0;
+            if (c0 + 1 < nb) cp[1] = (beta == 0.0) ? d1 : beta * cp[1] + d1;
         }
     }
     __syncthreads();

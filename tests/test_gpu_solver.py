@@ -152,3 +152,23 @@ def test_results_do_not_depend_on_unwritten_memory(monkeypatch):
     for y, n_steps, n_krylov, stats in runs[1:]:
         assert np.array_equal(y, runs[0][0])
         assert (n_steps, n_krylov, stats) == runs[0][1:]
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_step_statistics_track_the_reference(k):
+    """Free-running adsorption (200 s), blowdown (10 s) and heating (100 s) of the 4x4x16 bed take
+    about as many accepted and rejected steps as the reference did on the same input: the GPU
+    preconditioner is not SuperLU's, so GMRES counts differ, but a solver fault (a wrong matvec, a
+    stale norm) shows up as many more steps, rejections or Newton failures."""
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.solver import TRBDF2
+    d, m, cfg, meta = _c0_model(TVSAModel, k)
+    dur = meta["duration"]
+    integ = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur)
+    res = integ.integrate(d[f"s{k}_y0"], dur, [dur])
+    ref_steps, ref_rej, ref_fail = (int(v) for v in d[f"s{k}_stats"][:3])
+    ref_gmres = int(d[f"s{k}_stats"][6])
+    assert abs(res.n_steps - ref_steps) <= max(5, 0.15 * ref_steps), (res.n_steps, ref_steps)
+    assert res.n_reject <= ref_rej + 5, (res.n_reject, ref_rej)
+    assert res.n_newton_fail <= ref_fail + 3, (res.n_newton_fail, ref_fail)
+    assert integ.stats["gmres_iters"] <= 2 * ref_gmres + 50, (integ.stats["gmres_iters"], ref_gmres)
