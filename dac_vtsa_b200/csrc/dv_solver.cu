@@ -1067,13 +1067,25 @@ static int gmres_graph_collect(Work& W, dv_model* m, int* info, int64_t* inner) 
     return check_device_error(m);
 }
 
+// DVTSA_GMRES_GRAPH=0 in the environment runs GMRES host-driven (read once per process; for tools
+// that want plain kernel launches, such as a kernel-by-kernel profiler).
+static bool gmres_graph_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("DVTSA_GMRES_GRAPH");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 // The graph when it applies; the host-driven loop while launches are being profiled one by one.
 // With *pending set on return the graph is still running: call gmres_graph_collect after the
 // next synchronisation of the stream.
 static int gmres_start(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
                        int64_t* inner, bool* pending, cudaStream_t st) {
     *pending = false;
-    if (g_prof_on || b != W.b || op.z != W.z || op.f != W.f || op.s != W.s || kdim > GM_KMAX)
+    if (g_prof_on || !gmres_graph_enabled() || b != W.b || op.z != W.z || op.f != W.f || op.s != W.s ||
+        kdim > GM_KMAX)
         return gmres(W, op, b, rtol, atol, kdim, info, inner, st);
     DV_TRY(gmres_graph(W, op, b, rtol, atol, kdim, info, inner, st));
     *pending = true;

@@ -222,3 +222,54 @@ def _pressure_host(cfg, grid, props, y):
     Hq = rho_b * (th.dH_ads_co2 * q[0] + th.dH_ads_h2o * q[1])
     T = (e - Hq + A * th.T_ref) / (A - B)
     return (c[0] + c[1] + c[2]) * R_GAS * T
+
+
+# ---------------------------------------------------------------------------- command line
+# Operating point of the cycle benchmark (jackets 288 K, heating 373 K, vacuum 10 kPa, feed 288 K
+# at 50 % RH) on top of the reference defaults.
+BENCH_POINT = {"solver.scheme": "trbdf2", "operation.T_adsorption_jacket": 288.0, "operation.T_cool": 288.0,
+               "operation.T_heat": 373.0, "operation.P_vacuum": 1e4, "feed.T": 288.0, "feed.RH": 0.5,
+               "ambient.T": 288.0}
+
+
+def main(argv=None):
+    """Run one cycle step (or a window of it) of a bed from the seeded constant-pressure state on
+    the GPU and print its solver statistics as JSON, like the reference's per-step command lines
+    (steps/_runner.py:244): ``python -m dac_vtsa_b200.runner --grid 8 8 32 --step adsorption
+    --duration 600``."""
+    import argparse
+    import json
+    from .config import load_config
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--grid", type=int, nargs=3, default=(8, 8, 32), metavar=("NR", "NTHETA", "NZ"))
+    ap.add_argument("--step", default="adsorption", help="name of a step of the configured cycle")
+    ap.add_argument("--duration", type=float, default=None, help="bed-seconds to integrate (default: whole step)")
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args(argv)
+    over = dict(BENCH_POINT, **{"grid.Nr": a.grid[0], "grid.Ntheta": a.grid[1], "grid.Nz": a.grid[2]})
+    cfg = load_config(override_dict=over)
+    grid = host.Grid.from_config(cfg)
+    props = host.get_backend(cfg)
+    st = host.seeded_state(cfg, grid, props, seed=a.seed)
+    steps = {s["name"]: s for s in cfg.cycle}
+    if a.step not in steps:
+        raise SystemExit(f"unknown step {a.step!r}; the cycle has {sorted(steps)}")
+    step = dict(steps[a.step])
+    full = float(step["duration"])
+    dur = full if a.duration is None else min(a.duration, full)
+    model = TVSAModel(cfg, grid, props, step, st)
+    integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * full)
+    y0 = torch.from_numpy(model.pack(st)).to(model.device)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = integ.integrate(y0, dur, np.array([dur]), keep_on_device=True)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    print(json.dumps({"grid": list(a.grid), "step": a.step, "bed_s": res.t, "wall_s": wall,
+                      "bed_s_per_wall_s": res.t / wall, "steps": res.n_steps, "rejected": res.n_reject,
+                      "jac": res.n_jac, "lu": res.n_lu, "nfev": res.nfev, **integ.stats}))
+
+
+if __name__ == "__main__":
+    main()
+
