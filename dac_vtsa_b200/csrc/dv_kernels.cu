@@ -331,12 +331,16 @@ static __device__ __forceinline__ double matvec_sig(const double* scal) {
     return 1.4901161193847656e-08 * scal[1] / scal[0];
 }
 
+// Two warps per 32 cells: warp 0 evaluates the transport properties of its cells, warp 1 the
+// temperature, isotherms and LDF rates of the same cells (the two halves of the per-cell chain run
+// side by side; uptake reads only the clipped temperature of the properties).
 template <int MODE>
 __global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
                                                const double* __restrict__ u, const double* __restrict__ sc,
                                                const double* __restrict__ scal) {
     const int64_t nc = S.nc;
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c = (int64_t)blockIdx.x * 32 + (threadIdx.x & 31);
+    const bool half = (threadIdx.x >> 5) != 0;             // warp-uniform
     if (c >= nc) return;
     Cell s;
     if (MODE == M_MATVEC) {
@@ -347,29 +351,34 @@ __global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const 
         LoadPlain ld{y};
         load_cell(ld, nc, c, s);
     }
-    Props o;
-    cell_props(p, s, o);
-    double rate[DV_NA], qstar[DV_NA];
-    uptake(p, s, o, rate, qstar);
     double* a = S.cell;
+    if (!half) {
+        Props o;
+        cell_props(p, s, o);
 #pragma unroll
-    for (int q = 0; q < DV_NG; ++q) {
-        a[(SP_C0 + q) * nc + c] = s.c[q];
-        a[(SP_Y0 + q) * nc + c] = o.y[q];
-    }
-    a[SP_T * nc + c] = o.T;
-    a[SP_P * nc + c] = o.P;
-    a[SP_CPOS * nc + c] = o.Cpos;
-    a[SP_MU * nc + c] = o.mu;
-    a[SP_KG * nc + c] = o.kg;
-    a[SP_RHO * nc + c] = o.rho;
-    a[SP_CPM * nc + c] = o.cpm;
-    a[SP_DM * nc + c] = o.Dm;
-    a[SP_LAM0 * nc + c] = o.lam0;
+        for (int q = 0; q < DV_NG; ++q) {
+            a[(SP_C0 + q) * nc + c] = s.c[q];
+            a[(SP_Y0 + q) * nc + c] = o.y[q];
+        }
+        a[SP_T * nc + c] = o.T;
+        a[SP_P * nc + c] = o.P;
+        a[SP_CPOS * nc + c] = o.Cpos;
+        a[SP_MU * nc + c] = o.mu;
+        a[SP_KG * nc + c] = o.kg;
+        a[SP_RHO * nc + c] = o.rho;
+        a[SP_CPM * nc + c] = o.cpm;
+        a[SP_DM * nc + c] = o.Dm;
+        a[SP_LAM0 * nc + c] = o.lam0;
+    } else {
+        Props o;                            // uptake reads o.Tp only (same expression as cell_props)
+        o.Tp = npclip(cell_T(p, s), 150.0, 1500.0);
+        double rate[DV_NA], qstar[DV_NA];
+        uptake(p, s, o, rate, qstar);
 #pragma unroll
-    for (int q = 0; q < DV_NA; ++q) {
-        a[(SP_RATE0 + q) * nc + c] = rate[q];
-        a[(SP_QS0 + q) * nc + c] = qstar[q];
+        for (int q = 0; q < DV_NA; ++q) {
+            a[(SP_RATE0 + q) * nc + c] = rate[q];
+            a[(SP_QS0 + q) * nc + c] = qstar[q];
+        }
     }
 }
 
@@ -567,7 +576,7 @@ static int split_residual(dv_model* m, const Rec& rec, double t, const double* y
     const Split S = split_of(p, m->d_split);
     const int64_t ncol = (int64_t)p.Nr * p.Nth;
     const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
-    DV_LAUNCH(kind, s, k_cprops<MODE><<<nblk(m->nc, 64), 64, 0, s>>>(p, S, y, u, sc, scal));
+    DV_LAUNCH(kind, s, k_cprops<MODE><<<nblk(m->nc, 32), 64, 0, s>>>(p, S, y, u, sc, scal));
     DV_LAUNCH(kind, s, k_faces<REC><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t,
                                                                   MODE == M_MATVEC ? scal : nullptr, nullptr));
     DV_LAUNCH(kind, s, k_assemble<MODE, REC><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t, y, u, sc, f0,
@@ -616,7 +625,7 @@ int matvec_capture(dv_model* m, const double* dargs, const double* z, const doub
     const Rec rec = make_rec(m->rl, m->d_rec);
     const int64_t ncol = (int64_t)p.Nr * p.Nth;
     const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
-    k_cprops<M_MATVEC><<<nblk(m->nc, 64), 64, 0, s>>>(p, S, z, u, sc, scal);
+    k_cprops<M_MATVEC><<<nblk(m->nc, 32), 64, 0, s>>>(p, S, z, u, sc, scal);
     k_faces<false><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, scal, dargs);
     k_assemble<M_MATVEC, false><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, z, u, sc, f0, scal, 0.0,
                                                              out, dargs);

@@ -252,37 +252,67 @@ __global__ void k_combine(int64_t n, int m, const double* __restrict__ V, int64_
     }
 }
 
-// conservation sums: out[0..3] = W R (species moles + energy), out[4..7] = W s (core/residual.py:146-168)
-__global__ void k_cons(dv_step_params p, const double* __restrict__ R, const double* __restrict__ s,
-                       double* __restrict__ out) {
-    __shared__ double sh[VB];
+// conservation sums: out[0..3] = W R (species moles + energy), out[4..7] = W s (core/residual.py:146-168).
+// Grid-stride over cells; each block sums its eight values, the last block to finish adds the
+// block sums in block order (deterministic) and resets the ticket.
+__global__ void __launch_bounds__(VB) k_cons(dv_step_params p, const double* __restrict__ R,
+                                             const double* __restrict__ s, double* __restrict__ part,
+                                             unsigned* ticket, double* __restrict__ out) {
+    __shared__ double sh[VB / 32][8];
+    __shared__ bool last;
     const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz, nw = p.wall_on ? (int64_t)p.Nth * p.Nz : 0;
-    for (int which = 0; which < 2; ++which) {
-        const double* x = which ? s : R;
-        for (int m = 0; m <= DV_NG; ++m) {
-            double acc = 0.0;
-            for (int64_t c = threadIdx.x; c < nc; c += blockDim.x) {
-                const int i = (int)(c / ((int64_t)p.Nth * p.Nz));
-                const double V = p.V[i];
-                if (m < DV_NG) {
-                    acc += p.eps_t * V * x[m * nc + c];
-                    if (m < DV_NA) acc += p.rho_b * V * x[(DV_NG + m) * nc + c];
-                } else {
-                    acc += V * x[(int64_t)(DV_NG + DV_NA) * nc + c];      // e block
-                }
+    const int64_t ncz = (int64_t)p.Nth * p.Nz;
+    double acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const double V = p.V[(int)(c / ncz)];
+#pragma unroll
+        for (int which = 0; which < 2; ++which) {
+            const double* x = which ? s : R;
+#pragma unroll
+            for (int m = 0; m < DV_NG; ++m) {
+                double v = p.eps_t * V * x[m * nc + c];
+                if (m < DV_NA) v += p.rho_b * V * x[(DV_NG + m) * nc + c];
+                acc[which * 4 + m] += v;
             }
-            if (m == DV_NG)
-                for (int64_t w = threadIdx.x; w < nw; w += blockDim.x) acc += p.wall_C * x[(int64_t)DV_NV * nc + w];
-            sh[threadIdx.x] = acc;
-            __syncthreads();
-            for (int st = VB / 2; st > 0; st >>= 1) {
-                if (threadIdx.x < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-                __syncthreads();
-            }
-            if (threadIdx.x == 0) out[which * 4 + m] = sh[0];
-            __syncthreads();
+            acc[which * 4 + DV_NG] += V * x[(int64_t)(DV_NG + DV_NA) * nc + c];      // e block
         }
     }
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
+        acc[DV_NG] += p.wall_C * R[(int64_t)DV_NV * nc + w];
+        acc[4 + DV_NG] += p.wall_C * s[(int64_t)DV_NV * nc + w];
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        double v = acc[q];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0) sh[wid][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        double t = 0.0;
+        for (int w2 = 0; w2 < VB / 32; ++w2) t += sh[w2][threadIdx.x];
+        part[(int64_t)blockIdx.x * 8 + threadIdx.x] = t;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last && threadIdx.x < 8) {
+        __threadfence();
+        double t = 0.0;
+        for (int b = 0; b < (int)gridDim.x; ++b) t += ((volatile const double*)part)[(int64_t)b * 8 + threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    if (last && threadIdx.x == 0) *ticket = 0u;
+}
+
+static unsigned cons_grid(int64_t nc) {
+    const int64_t b = (nc + VB - 1) / VB;
+    return (unsigned)(b < 1 ? 1 : (b > 64 ? 64 : b));
 }
 
 // err scale: sc = atol + rtol max(|y|, |z|)  (core/solver.py:461)
@@ -1156,7 +1186,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
     auto cons_ok = [&](const double* R, const double* z, bool* ok) -> int {
         if (C.o.cons_tol <= 0.0) { *ok = true; return DV_OK; }
         scale(z, W.tmp);
-        DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<1, VB, 0, st>>>(m->p, R, W.tmp, W.scal));
+        DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<cons_grid(m->nc), VB, 0, st>>>(m->p, R, W.tmp, W.apart, W.tickets + 5, W.scal));
         DV_CUDA(cudaGetLastError());
         double v[8];
         DV_TRY(fetch(W, W.scal, 8, v, st));
@@ -1190,7 +1220,8 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         if (C.o.cons_tol > 0.0) {
             scale(W.zt, W.w);
             // into scal[16..23]: scal[0..1] still feed the matvec of a GMRES rerun after a refresh
-            DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<1, VB, 0, st>>>(m->p, W.Rt, W.w, W.scal + 16));
+            DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<cons_grid(m->nc), VB, 0, st>>>(m->p, W.Rt, W.w, W.apart, W.tickets + 5,
+                                                                                  W.scal + 16));
         }
         DV_CUDA(cudaMemcpyAsync(W.hpin + 16, W.scal, sizeof(double) * 32, cudaMemcpyDeviceToHost, st));
         return DV_OK;
