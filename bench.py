@@ -295,6 +295,32 @@ def gpu_arm(a, rank, world, local_rank):
     clocks = sampler.stop()
     total_ms = max_over_ranks(total_ms, dist, dev)
     value = replica_throughput(world, a.steps, total_ms / 1e3)
+    # ---- mixed precision (gpu.krylov_precision = fp32: FP32 factor storage in the preconditioner
+    # sweep), the same cycle, one warm-up and one timed cycle; state difference to the FP64 cycle
+    mixed = None
+    if not a.no_mixed:
+        from dac_vtsa_b200.config import load_config
+        cfg32 = load_config(override_dict=dict(overrides(WORKLOADS[a.workload]["grid"]),
+                                               **{"gpu.krylov_precision": "fp32"}))
+        run_cycle_device(y0_dev.clone(), cfg32, grid, props)
+        flush.fill_(1.0)
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        y32, st32, _ = run_cycle_device(y0_dev.clone(), cfg32, grid, props)
+        e1.record(stream)
+        e1.synchronize()
+        ms32 = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        y64h, y32h = y_end.double().cpu().numpy(), y32.double().cpu().numpy()
+        sc = m0.atol + cfg.solver.rtol * np.abs(y64h)
+        dev_scaled = (y32h - y64h) / sc
+        mixed = {"value": replica_throughput(world, 1, ms32 / 1e3), "unit": "bed-s/wall-s", "ms_per_step": ms32,
+                 "precision": "FP32 preconditioner factors, FP64 residual/Jacobian/Newton/GMRES vectors",
+                 "state_diff_vs_fp64_scaled_rms": float(np.sqrt(np.mean(dev_scaled ** 2))),
+                 "state_diff_vs_fp64_scaled_max": float(np.abs(dev_scaled).max()),
+                 "state_diff_vs_fp64_rel_max": float(np.max(np.abs(y32h - y64h) / (np.abs(y64h) + m0.atol))),
+                 "solver": st32}
     # ---- e2e: public step-runner API, host states, outlet recording per accepted step
     counters.reset()
     barrier()
@@ -355,6 +381,7 @@ def gpu_arm(a, rank, world, local_rank):
                            "l2": "flushed between timed cycles (256 MB write)",
                            "parallelism": f"{world} independent replicas (one per GPU)"},
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
+                "mixed_precision": mixed,
                 "clocks": clocks, "solver": stats_last}
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -371,6 +398,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cycle_8x8x32")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision cycle")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")

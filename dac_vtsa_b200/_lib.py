@@ -88,7 +88,7 @@ class DvNewtonResult(C.Structure):
 
 class DvSolverOpts(C.Structure):
     _fields_ = [("scheme", I32), ("max_newton_iter", I32), ("jacobian_max_age", I32), ("gmres_refresh", I32),
-                ("precond_mode", I32), ("pad_", I32), ("max_steps", I64),
+                ("precond_mode", I32), ("krylov_fp32", I32), ("max_steps", I64),
                 ("rtol", D), ("newton_kappa", D), ("refactor_ratio", D), ("conservation_tol", D),
                 ("h_max", D), ("h_init", D)]
 
@@ -122,6 +122,7 @@ SIGNATURES = [
     ("dv_fd_jacobian", C.c_int, [P, D, P, P, P, P]),
     ("dv_precond_factor", C.c_int, [P, P, D, I32, P]),
     ("dv_precond_solve", C.c_int, [P, P, P, P]),
+    ("dv_model_set_krylov_fp32", C.c_int, [P, I32]),
     ("dv_newton_stage", C.c_int, [P, D, P, P, D, C.POINTER(DvNewtonOpts), P, C.POINTER(DvNewtonResult), P]),
     ("dv_integrator_create", C.c_int, [P, C.POINTER(DvSolverOpts), C.POINTER(P)]),
     ("dv_integrator_destroy", C.c_int, [P]),

@@ -110,6 +110,11 @@ __global__ void k_pc_zero(double* __restrict__ A, int64_t n) {
         A[q] = 0.0;
 }
 
+__global__ void k_pc_to_f32(const double* __restrict__ A, float* __restrict__ B, int64_t n) {
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        B[q] = (float)A[q];
+}
+
 __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, double* __restrict__ A) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nc) return;
@@ -739,8 +744,8 @@ static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) 
 // j < NJ, are a fixed, fully unrolled batch of loads (padding columns hold zeros).
 #define PA_THREADS 512
 #define PA_LANES 8
-template <int NJ, int NBUF>
-__global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const double* __restrict__ A,
+template <int NJ, int NBUF, typename TS>
+__global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
                                                          double* __restrict__ x, int* __restrict__ err, PaFuse F) {
     extern __shared__ __align__(128) double dsm[];
@@ -753,16 +758,16 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
     const int64_t bs = g.bs;
     double* xs = dsm;                          // [Nz][LD]: b, then z (forward sweep, in place)
     double* xb = xs + (int64_t)g.Nz * LD;      // [Nz][LD]: x (backward sweep); padding columns zero
-    double* buf0 = xb + (int64_t)g.Nz * LD;    // NBUF ring buffers of [3 bs]: stage s uses buffer s % NBUF
-    const double* base = A + (int64_t)part * g.Nz * 5 * bs;
+    TS* buf0 = reinterpret_cast<TS*>(xb + (int64_t)g.Nz * LD);   // NBUF ring buffers of [3 bs]: stage s uses s % NBUF
+    const TS* base = A + (int64_t)part * g.Nz * 5 * bs;
     const int S = 2 * g.Nz - 1;                // stages: forward 1..Nz-1, backward Nz-1..0
-    auto stage_src = [&](int s) -> const double* {
+    auto stage_src = [&](int s) -> const TS* {
         if (s < g.Nz - 1) return base + (int64_t)(s + 1) * 5 * bs;
         const int k = g.Nz - 1 - (s - (g.Nz - 1));
         return base + ((int64_t)k * 5 + 2) * bs;
     };
     auto stage_bytes = [&](int s) -> uint32_t {
-        return (uint32_t)(((s < g.Nz - 1) ? 2 : 3) * bs * sizeof(double));
+        return (uint32_t)(((s < g.Nz - 1) ? 2 : 3) * bs * sizeof(TS));
     };
     if (tid == 0) {
         for (int q = 0; q < NBUF; ++q) mbar_init(smem_u32(&bars[q]), 1);
@@ -803,7 +808,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
     // only its own entry of plane k); backward rows go to xb, as every row reads all of z_k.
     for (int s = 0; s < S; ++s) {
         const int bi = s % NBUF;
-        double* buf = buf0 + (int64_t)bi * 3 * bs;
+        TS* buf = buf0 + (int64_t)bi * 3 * bs;
         const bool arrived = mbar_wait(smem_u32(&bars[bi]), (uint32_t)((s / NBUF) & 1));
         if (!__syncthreads_and(arrived)) {       // uniform decision: no thread is left at a barrier
             ok = false;
@@ -824,32 +829,32 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
         double acc = 0.0;
         if (r < nb) {
             if (fwd) {                           // [L1 | L2] . [z_{k-1} ; z_{k-2}]
-                const double* m1 = buf + bs + r * LD;
+                const TS* m1 = buf + bs + r * LD;
                 const double* v1 = xs + (int64_t)(k - 1) * LD;
 #pragma unroll
-                for (int j = 0; j < NJ; ++j) acc += m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
+                for (int j = 0; j < NJ; ++j) acc += (double)m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
                 if (k >= 2) {
-                    const double* m2 = buf + r * LD;
+                    const TS* m2 = buf + r * LD;
                     const double* v2 = xs + (int64_t)(k - 2) * LD;
 #pragma unroll
-                    for (int j = 0; j < NJ; ++j) acc += m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
+                    for (int j = 0; j < NJ; ++j) acc += (double)m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
                 }
             } else {                             // [Uinv | -W1 | -W2] . [z_k ; x_{k+1} ; x_{k+2}]
-                const double* m0 = buf + r * LD;
+                const TS* m0 = buf + r * LD;
                 const double* v0 = xs + (int64_t)k * LD;
 #pragma unroll
-                for (int j = 0; j < NJ; ++j) acc += m0[lane + PA_LANES * j] * v0[lane + PA_LANES * j];
+                for (int j = 0; j < NJ; ++j) acc += (double)m0[lane + PA_LANES * j] * v0[lane + PA_LANES * j];
                 if (k + 1 < g.Nz) {
-                    const double* m1 = buf + bs + r * LD;
+                    const TS* m1 = buf + bs + r * LD;
                     const double* v1 = xb + (int64_t)(k + 1) * LD;
 #pragma unroll
-                    for (int j = 0; j < NJ; ++j) acc += m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
+                    for (int j = 0; j < NJ; ++j) acc += (double)m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
                 }
                 if (k + 2 < g.Nz) {
-                    const double* m2 = buf + 2 * bs + r * LD;
+                    const TS* m2 = buf + 2 * bs + r * LD;
                     const double* v2 = xb + (int64_t)(k + 2) * LD;
 #pragma unroll
-                    for (int j = 0; j < NJ; ++j) acc += m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
+                    for (int j = 0; j < NJ; ++j) acc += (double)m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
                 }
             }
         }
@@ -904,7 +909,8 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const doubl
 
 // Sweep for partitions too large for the shared-memory pipeline: same fused stages, operands read
 // from global memory (L2).
-__global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const double* __restrict__ A,
+template <typename TS>
+__global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const TS* __restrict__ A,
                                                        const double* __restrict__ b, const double* __restrict__ sc,
                                                        double* __restrict__ x, double* __restrict__ xs_all) {
     __shared__ double tv[512];
@@ -914,7 +920,7 @@ __global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const double*
     const int tid = threadIdx.x;
     const int64_t bs = g.bs;
     double* xs = xs_all + (int64_t)part * g.Nz * ld;
-    const double* base = A + (int64_t)part * g.Nz * 5 * bs;
+    const TS* base = A + (int64_t)part * g.Nz * 5 * bs;
     for (int64_t q = tid; q < (int64_t)g.Nz * nb; q += blockDim.x) {
         int k = (int)(q / nb), l = (int)(q % nb);
         int64_t gi = pc_glob(g, part, k, l);
@@ -925,19 +931,19 @@ __global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const double*
     for (int s = 0; s < S; ++s) {
         const bool fwd = s < g.Nz - 1;
         const int k = fwd ? s + 1 : g.Nz - 1 - (s - (g.Nz - 1));
-        const double* Ak = base + (int64_t)k * 5 * bs;
-        const double* M0 = fwd ? Ak + bs : Ak + 2 * bs;
+        const TS* Ak = base + (int64_t)k * 5 * bs;
+        const TS* M0 = fwd ? Ak + bs : Ak + 2 * bs;
         const double* v0 = fwd ? xs + (int64_t)(k - 1) * ld : xs + (int64_t)k * ld;
-        const double* M1 = fwd ? ((k >= 2) ? Ak : nullptr) : ((k + 1 < g.Nz) ? Ak + 3 * bs : nullptr);
+        const TS* M1 = fwd ? ((k >= 2) ? Ak : nullptr) : ((k + 1 < g.Nz) ? Ak + 3 * bs : nullptr);
         const double* v1 = fwd ? ((k >= 2) ? xs + (int64_t)(k - 2) * ld : nullptr)
                                : ((k + 1 < g.Nz) ? xs + (int64_t)(k + 1) * ld : nullptr);
-        const double* M2 = (!fwd && k + 2 < g.Nz) ? Ak + 4 * bs : nullptr;
+        const TS* M2 = (!fwd && k + 2 < g.Nz) ? Ak + 4 * bs : nullptr;
         const double* v2 = (!fwd && k + 2 < g.Nz) ? xs + (int64_t)(k + 2) * ld : nullptr;
         for (int r = tid; r < nb; r += blockDim.x) {
             double acc = 0.0;
-            for (int c = 0; c < nb; ++c) acc += M0[(int64_t)r * ld + c] * v0[c];
-            if (M1) for (int c = 0; c < nb; ++c) acc += M1[(int64_t)r * ld + c] * v1[c];
-            if (M2) for (int c = 0; c < nb; ++c) acc += M2[(int64_t)r * ld + c] * v2[c];
+            for (int c = 0; c < nb; ++c) acc += (double)M0[(int64_t)r * ld + c] * v0[c];
+            if (M1) for (int c = 0; c < nb; ++c) acc += (double)M1[(int64_t)r * ld + c] * v1[c];
+            if (M2) for (int c = 0; c < nb; ++c) acc += (double)M2[(int64_t)r * ld + c] * v2[c];
             tv[r] = fwd ? xs[(int64_t)k * ld + r] - acc : acc;
         }
         __syncthreads();
@@ -1026,6 +1032,10 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
             DV_CUDA(cudaFuncSetAttribute(k_pc_factor_glob, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_glob<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_work, m->d_pc_info, use_smem));
     }
+    if (m->pc_fp32) {               // the sweep streams an FP32 copy of the factors
+        const int64_t tot = (int64_t)g.nparts * g.Nz * 5 * g.bs;
+        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_to_f32<<<std::min<int64_t>((tot + 255) / 256, 4096), 256, 0, s>>>(m->d_pc, m->d_pc32, tot));
+    }
     DV_CUDA(cudaGetLastError());
     m->pc_mode = g.mode;
     m->pc_nb = g.nb;
@@ -1035,31 +1045,39 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
 }
 
 // shared memory of the sweep with an NBUF-deep ring: solution planes, one plane of scratch, buffers
-static size_t apply_smem(const PcGeom& g, int nbuf) {
-    return sizeof(double) * (size_t)(2 * (int64_t)g.Nz * g.ld + (int64_t)nbuf * 3 * g.bs);
+// shared memory of the sweep with an NBUF-deep ring of factor blocks stored as `tsize`-byte values
+static size_t apply_smem(const PcGeom& g, int nbuf, size_t tsize) {
+    return sizeof(double) * (size_t)(2 * (int64_t)g.Nz * g.ld) + tsize * (size_t)((int64_t)nbuf * 3 * g.bs);
 }
 
-// ring depth: three stages in flight when they fit in shared memory, else two
-static int apply_nbuf(const PcGeom& g) { return apply_smem(g, 3) <= (size_t)smem_optin() ? 3 : 2; }
+static size_t pc_tsize(const dv_model* m) { return m->pc_fp32 ? sizeof(float) : sizeof(double); }
 
-template <int NJ, int NBUF>
-static void launch_apply_k(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
-                           const PaFuse& F, bool count) {
-    const size_t dyn = apply_smem(g, NBUF);
+// ring depth: three stages in flight when they fit in shared memory, else two
+static int apply_nbuf(const PcGeom& g, size_t tsize) { return apply_smem(g, 3, tsize) <= (size_t)smem_optin() ? 3 : 2; }
+
+template <int NJ, int NBUF, typename TS>
+static void launch_apply_k(const PcGeom& g, dv_model* m, const TS* A, const double* b, const double* sc, double* x,
+                           cudaStream_t s, const PaFuse& F, bool count) {
+    const size_t dyn = apply_smem(g, NBUF, sizeof(TS));
     if (count) {
         if (dyn > 48 * 1024)
-            cudaFuncSetAttribute(k_pc_apply<NJ, NBUF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ, NBUF><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F));
+            cudaFuncSetAttribute(k_pc_apply<NJ, NBUF, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ, NBUF, TS><<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F));
     } else {
-        k_pc_apply<NJ, NBUF><<<g.nparts, PA_THREADS, dyn, s>>>(g, m->d_pc, b, sc, x, m->d_err, F);
+        k_pc_apply<NJ, NBUF, TS><<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F);
     }
 }
 
 template <int NJ>
 static void launch_apply_nj(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
                             const PaFuse& F, bool count) {
-    if (apply_nbuf(g) == 3) launch_apply_k<NJ, 3>(g, m, b, sc, x, s, F, count);
-    else launch_apply_k<NJ, 2>(g, m, b, sc, x, s, F, count);
+    if (m->pc_fp32) {               // factors stored in FP32 (mixed-precision Krylov), products in FP64
+        if (apply_nbuf(g, sizeof(float)) == 3) launch_apply_k<NJ, 3, float>(g, m, m->d_pc32, b, sc, x, s, F, count);
+        else launch_apply_k<NJ, 2, float>(g, m, m->d_pc32, b, sc, x, s, F, count);
+    } else {
+        if (apply_nbuf(g, sizeof(double)) == 3) launch_apply_k<NJ, 3, double>(g, m, m->d_pc, b, sc, x, s, F, count);
+        else launch_apply_k<NJ, 2, double>(g, m, m->d_pc, b, sc, x, s, F, count);
+    }
 }
 
 static void launch_apply(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
@@ -1081,7 +1099,11 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
     if (precond_apply_fusable(m)) {
         launch_apply(g, m, b, sc, x, s, PaFuse(), true);
     } else {
-        DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply_glob<<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work));
+        if (m->pc_fp32) {
+            DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply_glob<float><<<g.nparts, 512, 0, s>>>(g, m->d_pc32, b, sc, x, m->d_pc_work));
+        } else {
+            DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply_glob<double><<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work));
+        }
     }
     DV_CUDA(cudaGetLastError());
     return DV_OK;
@@ -1090,7 +1112,8 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
 bool precond_apply_fusable(dv_model* m) {
     PcGeom g = geom_of(m, m->pc_mode);
     const int nj = g.ld / PA_LANES;
-    return g.nb <= 64 && apply_smem(g, 2) <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7);
+    return g.nb <= 64 && apply_smem(g, 2, pc_tsize(m)) <= (size_t)smem_optin() &&
+           (nj == 1 || nj == 3 || nj == 5 || nj == 7);
 }
 
 int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
@@ -1103,7 +1126,8 @@ int precond_apply_capture(dv_model* m, const double* b, const double* sc, double
             set_error("fused sweep requested for a partition the shared-memory sweep does not take");
             return DV_ERR_ARG;
         }
-        k_pc_apply_glob<<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work);
+        if (m->pc_fp32) k_pc_apply_glob<float><<<g.nparts, 512, 0, s>>>(g, m->d_pc32, b, sc, x, m->d_pc_work);
+        else k_pc_apply_glob<double><<<g.nparts, 512, 0, s>>>(g, m->d_pc, b, sc, x, m->d_pc_work);
     }
     DV_CUDA(cudaGetLastError());
     return DV_OK;

@@ -1058,6 +1058,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     W.gm_mode = m->pc_mode;
     W.gm_nb = m->pc_nb;
     W.gm_nparts = m->pc_nparts;
+    W.gm_fp32 = m->pc_fp32;
     for (int k = 0; k < K_NKIND; ++k) {
         W.gm_fixed[k] = fixed[k];
         W.gm_iter[k] = iter[k];
@@ -1071,7 +1072,7 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
                        int64_t* inner, cudaStream_t st) {
     dv_model* m = op.m;
     if (!W.gm_exec || W.gm_kdim != kdim || W.gm_mode != m->pc_mode || W.gm_nb != m->pc_nb ||
-        W.gm_nparts != m->pc_nparts)
+        W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32)
         DV_TRY(gm_build(m, W, kdim));
     GmHost* hst = (GmHost*)W.gm_host;
     hst->args[0] = op.t;
@@ -1484,9 +1485,18 @@ int dv_device_count(int* n) {
     return DV_OK;
 }
 
+int dv_model_set_krylov_fp32(dv_model* m, int32_t on) {
+    if (!m) { set_error("null argument"); return DV_ERR_ARG; }
+    if (m->pc_fp32 != (on ? 1 : 0)) {
+        m->pc_fp32 = on ? 1 : 0;
+        m->pc_ready = 0;                // the next dv_precond_factor builds the copy the sweep reads
+    }
+    return DV_OK;
+}
+
 int dv_model_destroy(dv_model* m) {
     if (!m) return DV_OK;
-    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_acc, m->d_pc, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
+    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_acc, m->d_pc, m->d_pc32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
                     m->d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -1532,6 +1542,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
                 cudaMalloc((void**)&m->d_split, sizeof(double) * split_doubles(*p)) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_pc32, sizeof(float) * pc_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts) != cudaSuccess ||
@@ -1546,6 +1557,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     debug_fill(m->d_split, sizeof(double) * split_doubles(*p), 1);
     debug_fill(m->d_acc, sizeof(double) * DV_NACC, 1);
     debug_fill(m->d_pc, sizeof(double) * pc_need, 1);
+    debug_fill(m->d_pc32, sizeof(float) * pc_need, 1);
     debug_fill(m->d_pc_work, sizeof(double) * work_need, 1);
     debug_fill(m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb, 1);
     debug_fill(m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts, 1);
@@ -1660,6 +1672,10 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
     g->o = *o;
     g->n = m->n;
     g->log_refactor = std::log(o->refactor_ratio);
+    if (m->pc_fp32 != (o->krylov_fp32 ? 1 : 0)) {   // factors must be rebuilt in the requested storage
+        m->pc_fp32 = o->krylov_fp32 ? 1 : 0;
+        m->pc_ready = 0;
+    }
     double** vecs[] = {&g->y, &g->fn, &g->slope, &g->z1, &g->z2, &g->f1, &g->f2, &g->rhs1, &g->rhs2, &g->pred, &g->ev, &g->es};
     for (double** v : vecs) {
         if (cudaMalloc((void**)v, sizeof(double) * g->n) != cudaSuccess) {

@@ -295,6 +295,14 @@ class TVSAModel:
                 "R_bed": (1.0 / self.cfg.transport.lumped_U) if self.params.lumped else Rb.copy()}
 
     # ------------------------------------------------------------------ linear algebra entry points
+    def set_krylov_precision(self, precision: str):
+        """"fp64" (default) or "fp32": storage of the preconditioner factors the sweep streams
+        (products stay FP64); takes effect at the next factorisation."""
+        if precision not in ("fp64", "fp32"):
+            raise ValueError(f"krylov precision must be fp64 or fp32, not {precision!r}")
+        check(self.lib.dv_model_set_krylov_fp32(self.handle, 1 if precision == "fp32" else 0),
+              "dv_model_set_krylov_fp32")
+
     def precond_factor(self, J_block: torch.Tensor, dh: float, mode: str = "theta_block"):
         """Factorise I - dh J (block layout J) along z per partition: "theta_block" (the innermost ring
         of all sectors as one partition, rings 1.. of each sector as the others), "sector" (whole

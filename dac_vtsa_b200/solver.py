@@ -91,8 +91,11 @@ class TRBDF2:
         o.conservation_tol = float(s.conservation_tol or 0.0)
         o.h_max = h_max
         o.h_init = self.h_init
-        self.opts = o
+        # gpu.krylov_precision: fp64 (default, the parity path) or fp32 (factors streamed in FP32)
         self.krylov_precision = gpu_option(cfg, "krylov_precision", "fp64")
+        o.krylov_fp32 = 1 if self.krylov_precision == "fp32" else 0
+        self.opts = o
+
         h = C.c_void_p()
         check(self.lib.dv_integrator_create(model.handle, C.byref(o), C.byref(h)), "dv_integrator_create")
         self.handle = h

@@ -172,3 +172,44 @@ def test_step_statistics_track_the_reference(k):
     assert res.n_reject <= ref_rej + 5, (res.n_reject, ref_rej)
     assert res.n_newton_fail <= ref_fail + 3, (res.n_newton_fail, ref_fail)
     assert integ.stats["gmres_iters"] <= 2 * ref_gmres + 50, (integ.stats["gmres_iters"], ref_gmres)
+
+
+def test_fp32_factors_solve_to_single_precision():
+    """The sweep over FP32-stored factors (mixed-precision Krylov) solves the same partition system
+    as the FP64 one to single-precision accuracy."""
+    import torch
+    from dac_vtsa_b200.jacobian import FDJacobian
+    from dac_vtsa_b200.model import TVSAModel
+    d = golden("jacobian_3x4x6.npz")
+    m, _ = build(TVSAModel, {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6}, 0, d["P0"])
+    J = FDJacobian(m).block(5.0, d["y"])
+    b = np.random.default_rng(11).standard_normal(m.n_core) * m.atol
+    m.precond_factor(J, 2.1)
+    x64 = m.precond_solve(b)
+    m.set_krylov_precision("fp32")
+    m.precond_factor(J, 2.1)
+    x32 = m.precond_solve(b)
+    rel = np.abs(x32 - x64).max() / np.abs(x64).max()
+    assert 0.0 < rel < 1e-4, rel
+
+
+def test_mixed_precision_adsorption_stays_within_solver_tolerance():
+    """Free-running 200 s adsorption of the 4x4x16 bed with gpu.krylov_precision = fp32: the end
+    state matches the FP64 run within the solver's own error scale (atol + rtol |y|) and the
+    step count stays close; only the preconditioner changes, the Newton tolerance judges."""
+    from dac_vtsa_b200.config import load_config
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.solver import TRBDF2
+    d, m, cfg, meta = _c0_model(TVSAModel)
+    dur = meta["duration"]
+    r64 = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur).integrate(d["s0_y0"], dur, [dur])
+    over = json.loads(str(d["over"]))
+    over["gpu.krylov_precision"] = "fp32"
+    d2, m2, cfg2, _ = _c0_model(TVSAModel)
+    cfg32 = load_config(override_dict=over)
+    integ = TRBDF2(m2, cfg32, h_max=cfg32.solver.h_max_fraction * dur)
+    r32 = integ.integrate(d["s0_y0"], dur, [dur])
+    sc = m.atol + cfg.solver.rtol * np.abs(r64.y)
+    err = np.sqrt(np.mean(((r32.y - r64.y) / sc) ** 2))
+    assert err < 1.0, err
+    assert abs(r32.n_steps - r64.n_steps) <= max(5, 0.15 * r64.n_steps), (r32.n_steps, r64.n_steps)
