@@ -52,7 +52,7 @@ struct Work {
     cudaGraph_t gm_graph = nullptr;
     cudaGraphExec_t gm_exec = nullptr;
     cudaStream_t gm_cs = nullptr;             // capture stream
-    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1;
+    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1;
     int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
@@ -87,6 +87,7 @@ struct dv_model {
     int64_t jac_doubles;
     // preconditioner: block-pentadiagonal LU along z per partition
     int pc_mode, pc_nparts, pc_nb, pc_ready;
+    int pc_zs;                      // twisted factorisation: first separator plane (0: top-down only)
     int pc_fp32;                    // sweep reads an FP32 copy of the factors (mixed-precision Krylov)
     float* d_pc32;                  // that copy, same layout as d_pc
     int pc_cap_nb, pc_cap_parts;

@@ -27,6 +27,7 @@ namespace dv {
 
 struct PcGeom {
     int Nr, Nth, Nz, wall, mode, nb, nparts, ld;
+    int zs;                // twisted factorisation: separator planes zs, zs+1 (0: one direction, top-down)
     int ncv;               // cell unknowns (6 per cell) of the partition; nb - ncv wall nodes follow
     int64_t nc, bs;        // bs: block stride in doubles (nb*ld rounded up to even: 16-byte multiple)
 };
@@ -487,32 +488,75 @@ static __device__ void cp_block(int64_t n, const double* src, double* dst) {
     for (int64_t q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[q];
 }
 
-// One CTA per partition, every working block resident in shared memory (nb <= PC_SMEM_NB).
+// ---------------------------------------------------------------- clusters of two CTAs
+static __device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+static __device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// a value in the shared memory of CTA `rank` of this cluster, at the address of *p in this CTA
+static __device__ __forceinline__ double ld_peer_cta(const double* p, uint32_t rank) {
+    uint32_t ra;
+    double v;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(smem_u32(p)), "r"(rank));
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(ra) : "memory");
+    return v;
+}
+static __device__ __forceinline__ int ld_peer_cta(const int* p, uint32_t rank) {
+    uint32_t ra;
+    int v;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(smem_u32(p)), "r"(rank));
+    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(ra) : "memory");
+    return v;
+}
+
+// One CTA per partition (TW: per direction of a partition, a cluster of two), every working block
+// resident in shared memory (nb <= PC_SMEM_NB).  The elimination runs in the CTA's local plane
+// frame: rank 0 top-down over planes 0..zs-1, rank 1 bottom-up over planes Nz-1..zs+2, local
+// slot sl of local plane t being global slot 4 - sl of plane Nz-1-t for rank 1.  TW: after its n
+// planes each rank also forms the multipliers of the separator planes n, n+1 and their Schur contributions Q = -(couplings through
+// the eliminated planes); rank 0 adds both ranks' Q to the separator blocks (read through
+// distributed shared memory) and factorises the 2 nb x 2 nb separator matrix S = [S11 S12; S21 S22]
+// as two more planes of the same block elimination (the inverse is not multiplied out, which loses
+// accuracy when S11 is poorly conditioned):
+//   plane zs:   slot 2 Dm^-1 = S11^-1,  slot 3 -Dm^-1 S12
+//   plane zs+1: slot 1 S21 Dm^-1,       slot 2 Dn^-1 = (S22 - S21 Dm^-1 S12)^-1
+template <bool TW>
 __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __restrict__ A, int* __restrict__ info) {
-    const PcGeom g = pc_part(gin, (int)blockIdx.x);
-    extern __shared__ __align__(16) double dsm[];
+    const int rank = TW ? (int)(blockIdx.x & 1u) : 0;
+    const int part = TW ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+    const PcGeom g = pc_part(gin, part);
+    extern __shared__ __align__(128) double dsm[];
     __shared__ int perm[64], idx[64];
     __shared__ double pv[8];
     __shared__ int pi[8];
+    __shared__ int qoff[4], sbad;
     const int nb = g.nb, ld = g.ld;
     const int n2 = nb * ld;
+    const int Nz = g.Nz;
+    const int n = TW ? (rank == 0 ? g.zs : Nz - g.zs - 2) : Nz;
     double* buf[9];
     for (int q = 0; q < 9; ++q) buf[q] = dsm + (int64_t)q * n2;
     double *S0 = buf[0], *S1 = buf[1], *S2 = buf[2], *S3 = buf[3], *T = buf[4];
     double *Ui1 = buf[5], *Ui2 = buf[6], *U11 = buf[7], *U12 = buf[8];
     for (int64_t q = threadIdx.x; q < 9 * (int64_t)n2; q += blockDim.x) dsm[q] = 0.0;   // zero padding columns
     __syncthreads();
-    double* base = A + (int64_t)blockIdx.x * g.Nz * 5 * g.bs;
+    double* base = A + (int64_t)part * Nz * 5 * g.bs;
+    // block (local plane t, local slot sl)
+    auto B = [&](int t, int sl) -> double* {
+        const int P = (rank == 0) ? t : Nz - 1 - t;
+        return base + ((int64_t)P * 5 + ((rank == 0) ? sl : 4 - sl)) * g.bs;
+    };
     int bad = 0;
-    for (int k = 0; k < g.Nz; ++k) {
-        double* Ak = base + (int64_t)k * 5 * g.bs;
-        if (k >= 2) cp_block(n2, Ak, S0);
-        if (k >= 1) cp_block(n2, Ak + g.bs, S1);
-        cp_block(n2, Ak + 2 * g.bs, S2);
-        cp_block(n2, Ak + 3 * g.bs, S3);
+    for (int k = 0; k < n; ++k) {
+        if (k >= 2) cp_block(n2, B(k, 0), S0);
+        if (k >= 1) cp_block(n2, B(k, 1), S1);
+        cp_block(n2, B(k, 2), S2);
+        cp_block(n2, B(k, 3), S3);
         __syncthreads();
         if (k >= 2) {
-            double* U2_2 = base + ((int64_t)(k - 2) * 5 + 4) * g.bs;        // A(k-2, k), block diagonal
+            double* U2_2 = B(k - 2, 4);                                        // A(k-2, k), block diagonal
             sm_bd_left(g, 1.0, S0, Ui2, 0.0, T);                               // L2 = A(k,k-2) Uinv_{k-2}
             double* t = S0; S0 = T; T = t;
             sm_gemm(nb, ld, -1.0, S0, U12, 1.0, S1);                           // A(k,k-1) -= L2 U1_{k-2}
@@ -522,7 +566,7 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
             __syncthreads();
         }
         if (k >= 1) {
-            const double* U2_1 = base + ((int64_t)(k - 1) * 5 + 4) * g.bs;   // A(k-1, k+1), block diagonal
+            const double* U2_1 = B(k - 1, 4);                                  // A(k-1, k+1), block diagonal
             if (k == 1) sm_bd_left(g, 1.0, S1, Ui1, 0.0, T);                  // L1 = A(1,0) Uinv_0
             else sm_gemm(nb, ld, 1.0, S1, Ui1, 0.0, T);                        // L1 = (...) Uinv_{k-1}
             double* t = S1; S1 = T; T = t;
@@ -531,17 +575,89 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
         }
         bad |= sm_inverse(nb, ld, S2, T, perm, idx, pv, pi);              // (T: ping-pong buffer)
         sm_gemm(nb, ld, -1.0, S2, S3, 0.0, T);                                 // -Uinv_k U1_k
-        if (k >= 2) cp_block(n2, S0, Ak);
-        if (k >= 1) cp_block(n2, S1, Ak + g.bs);
-        cp_block(n2, S2, Ak + 2 * g.bs);
-        cp_block(n2, T, Ak + 3 * g.bs);
+        if (k >= 2) cp_block(n2, S0, B(k, 0));
+        if (k >= 1) cp_block(n2, S1, B(k, 1));
+        cp_block(n2, S2, B(k, 2));
+        cp_block(n2, T, B(k, 3));
         __syncthreads();
         // rotate: Uinv_{k-2} <- Uinv_{k-1} <- Uinv_k ; U1 likewise; freed blocks become S2 / S3
         double* fi = Ui2; Ui2 = Ui1; Ui1 = S2; S2 = fi;
         double* fu = U12; U12 = U11; U11 = S3; S3 = fu;
     }
-    // slot 4 of the last two planes: U2_k = A(k, k+2) = 0 for k >= Nz-2 (zeroed at assembly)
-    if (threadIdx.x == 0) info[blockIdx.x] = bad;
+    if constexpr (!TW) {
+        // slot 4 of the last two planes: U2_k = A(k, k+2) = 0 for k >= Nz-2 (zeroed at assembly)
+        if (threadIdx.x == 0) info[part] = bad;
+    } else {
+        // separator plane n: coupled to planes n-2 and n-1
+        cp_block(n2, B(n, 0), S0);                                             // A(n, n-2)
+        cp_block(n2, B(n, 1), S1);                                             // A(n, n-1)
+        __syncthreads();
+        double* U2_2 = B(n - 2, 4);                                            // A(n-2, n)
+        double* U2_1 = B(n - 1, 4);                                            // A(n-1, n+1)
+        sm_bd_left(g, 1.0, S0, Ui2, 0.0, T);                                   // L2_n = A(n,n-2) Uinv_{n-2}
+        { double* t = S0; S0 = T; T = t; }
+        sm_gemm(nb, ld, -1.0, S0, U12, 1.0, S1);                               // A(n,n-1) - L2 U1_{n-2}
+        sm_bd_right(g, -1.0, S0, U2_2, 0.0, S2);                               // Q(n,n) = -L2 U2_{n-2}
+        sm_bd_right(g, -1.0, Ui2, U2_2, 0.0, T);                               // -Uinv_{n-2} U2_{n-2}
+        cp_block(n2, T, U2_2);
+        __syncthreads();
+        sm_gemm(nb, ld, 1.0, S1, Ui1, 0.0, T);                                 // L1_n = (...) Uinv_{n-1}
+        { double* t = S1; S1 = T; T = t; }
+        sm_gemm(nb, ld, -1.0, S1, U11, 1.0, S2);                               // Q(n,n) -= L1 U1_{n-1}
+        sm_bd_right(g, -1.0, S1, U2_1, 0.0, S3);                               // Q(n,n+1) = -L1 U2_{n-1}
+        cp_block(n2, S0, B(n, 0));
+        cp_block(n2, S1, B(n, 1));
+        __syncthreads();
+        // separator plane n+1: coupled to plane n-1 only
+        cp_block(n2, B(n + 1, 0), S0);                                         // A(n+1, n-1)
+        __syncthreads();
+        sm_bd_left(g, 1.0, S0, Ui1, 0.0, T);                                   // L2_{n+1} = A(n+1,n-1) Uinv_{n-1}
+        { double* t = S0; S0 = T; T = t; }
+        double* Q10 = Ui2;                                                     // (Uinv_{n-2}, U1_{n-2}: done)
+        double* Q11 = U12;
+        sm_gemm(nb, ld, -1.0, S0, U11, 0.0, Q10);                              // Q(n+1,n) = -L2 U1_{n-1}
+        sm_bd_right(g, -1.0, S0, U2_1, 0.0, Q11);                              // Q(n+1,n+1) = -L2 U2_{n-1}
+        sm_bd_right(g, -1.0, Ui1, U2_1, 0.0, T);                               // -Uinv_{n-1} U2_{n-1}
+        cp_block(n2, T, U2_1);
+        cp_block(n2, S0, B(n + 1, 0));
+        if (threadIdx.x == 0) {
+            qoff[0] = (int)(S2 - dsm);
+            qoff[1] = (int)(S3 - dsm);
+            qoff[2] = (int)(Q10 - dsm);
+            qoff[3] = (int)(Q11 - dsm);
+            sbad = bad;
+        }
+        __syncthreads();
+        cluster_sync_all();                                                    // both ranks hold Q
+        // rank 0: S = A_sep + Q(rank 0) + Q(rank 1); rank 1's local block (a, b) is separator (1-a, 1-b)
+        double* Sb[4] = {S2, S3, Q10, Q11};                                    // separator (0,0) (0,1) (1,0) (1,1)
+        if (rank == 0) {
+            int ro[4];
+            for (int q = 0; q < 4; ++q) ro[q] = ld_peer_cta(&qoff[3 - q], 1u);
+            const double* Ab[4] = {B(n, 2), B(n, 3), B(n + 1, 1), B(n + 1, 2)};
+            for (int q = 0; q < 4; ++q)
+                for (int e = threadIdx.x; e < n2; e += blockDim.x)
+                    Sb[q][e] = (Ab[q][e] + Sb[q][e]) + ld_peer_cta(dsm + ro[q] + e, 1u);
+            if (threadIdx.x == 0) bad |= ld_peer_cta(&sbad, 1u);
+        }
+        __syncthreads();
+        cluster_sync_all();                                                    // rank 1's blocks have been read
+        if (rank == 0) {
+            double *S11 = Sb[0], *S12 = Sb[1], *S21 = Sb[2], *S22 = Sb[3];
+            double* Xn = S0;                                                   // free: S0, S1, Ui1, U11 (+ T)
+            double* Y = S1;
+            bad |= sm_inverse(nb, ld, S11, T, perm, idx, pv, pi);             // Dm^-1
+            sm_gemm(nb, ld, -1.0, S11, S12, 0.0, Xn);                          // -Dm^-1 S12
+            sm_gemm(nb, ld, 1.0, S21, S11, 0.0, Y);                            // S21 Dm^-1
+            sm_gemm(nb, ld, 1.0, S21, Xn, 1.0, S22);                           // S22 - S21 Dm^-1 S12
+            bad |= sm_inverse(nb, ld, S22, T, perm, idx, pv, pi);             // Dn^-1
+            cp_block(n2, S11, B(n, 2));
+            cp_block(n2, Xn, B(n, 3));
+            cp_block(n2, Y, B(n + 1, 1));
+            cp_block(n2, S22, B(n + 1, 2));
+            if (threadIdx.x == 0) info[part] = bad;
+        }
+    }
 }
 
 // ---------------------------------------------------------------- global-memory fallback (large blocks)
@@ -714,16 +830,8 @@ __global__ void __launch_bounds__(256) k_pc_factor_glob(PcGeom gin, double* __re
 }
 
 // ---------------------------------------------------------------- sweeps
-static __device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
 static __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-static __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
 }
 static __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     uint32_t ok;
@@ -738,36 +846,90 @@ static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) 
     return false;
 }
 
-// x = diag(1/sc) M^-1 diag(sc) b for all partitions: one CTA (512 threads, 8 lanes per row) per
-// partition.  The factor blocks of the next plane stream into a second shared buffer (cp.async.bulk
-// with an mbarrier) while the current plane is swept.  NJ = ld / 8: each lane's columns lane + 8j,
-// j < NJ, are a fixed, fully unrolled batch of loads (padding columns hold zeros).
-#define PA_THREADS 512
+// Plane frame of one elimination direction.  TW = false: planes 0..Nz-1 top-down (the whole
+// partition).  TW = true (twisted factorisation, a cluster of two CTAs per partition): rank 0
+// eliminates planes 0..zs-1 top-down, rank 1 planes Nz-1..zs+2 bottom-up, and the separator
+// planes zs, zs+1 are solved as one dense 2 nb system.  In its local frame each rank sees planes
+// t = 0, 1, .. (global gp(t)) with slot sl holding the coupling to local plane t + sl - 2, which is
+// global slot gs(sl): bottom-up, A(t, t-1) local is A(p, p+1) global, and so on.  The local
+// eliminated planes are 0..n-1; local n and n+1 are the separator planes.
+struct PcFrame {
+    int rank, n, Nz;
+    __device__ __forceinline__ int gp(int t) const { return rank == 0 ? t : Nz - 1 - t; }
+    __device__ __forceinline__ int gs(int sl) const { return rank == 0 ? sl : 4 - sl; }
+};
+
+// x = diag(1/sc) M^-1 diag(sc) b for all partitions: one CTA (256 threads; 8 lanes per group, two
+// rows per group) per partition, or per direction of a partition (TW).  The factor blocks of the
+// next planes stream into an NBUF-deep shared ring (cp.async.bulk with an mbarrier) while the
+// current plane is swept.  NJ = ld / 8: each lane's columns lane + 8j, j < NJ, are a fixed, fully
+// unrolled batch of loads (padding columns hold zeros).
+// Stages of one CTA (local frame):
+//   F(t), t = 1..n-1:   z_t = b_t - L1_t z_{t-1} - L2_t z_{t-2}                  (slots 0, 1)
+//   TW only:
+//   X:                  p_n = b_n - L1_n z_{n-1} - L2_n z_{n-2},  p_{n+1} = b_{n+1} - L2_{n+1} z_{n-1}
+//                       (b of the separator read by rank 0 only); the two ranks' p are summed
+//                       through distributed shared memory into r
+//   C0, C1, C2:         the separator's block LU (both ranks; r_m, r_m1: global planes zs, zs+1)
+//                       C0: r_m1 -= (S21 Dm^-1) r_m;  C1: x_m1 = Dn^-1 r_m1;
+//                       C2: x_m = Dm^-1 r_m + (-Dm^-1 S12) x_m1
+//   B(t), t = n-1..0:   x_t = Uinv_t z_t + (-Uinv_t U1_t) x_{t+1} + (-Uinv_t U2_t) x_{t+2}  (slots 2..4)
+// Without TW the backward stages run t = Nz-1..0 (couplings beyond the last plane are absent).
+#define PA_THREADS 256
 #define PA_LANES 8
-template <int NJ, int NBUF, typename TS>
+template <int NJ, int NBUF, typename TS, bool TW>
 __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
                                                          double* __restrict__ x, int* __restrict__ err, PaFuse F) {
     extern __shared__ __align__(128) double dsm[];
     __shared__ __align__(8) uint64_t bars[NBUF];
     constexpr int LD = NJ * PA_LANES;
-    const int part = blockIdx.x;
+    const int rank = TW ? (int)(blockIdx.x & 1u) : 0;
+    const int part = TW ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
     const PcGeom g = pc_part(gin, part);
-    const int nb = g.nb;
+    const int nb = g.nb, Nz = g.Nz;
     const int tid = threadIdx.x;
     const int64_t bs = g.bs;
-    double* xs = dsm;                          // [Nz][LD]: b, then z (forward sweep, in place)
-    double* xb = xs + (int64_t)g.Nz * LD;      // [Nz][LD]: x (backward sweep); padding columns zero
-    TS* buf0 = reinterpret_cast<TS*>(xb + (int64_t)g.Nz * LD);   // NBUF ring buffers of [3 bs]: stage s uses s % NBUF
-    const TS* base = A + (int64_t)part * g.Nz * 5 * bs;
-    const int S = 2 * g.Nz - 1;                // stages: forward 1..Nz-1, backward Nz-1..0
-    auto stage_src = [&](int s) -> const TS* {
-        if (s < g.Nz - 1) return base + (int64_t)(s + 1) * 5 * bs;
-        const int k = g.Nz - 1 - (s - (g.Nz - 1));
-        return base + ((int64_t)k * 5 + 2) * bs;
-    };
-    auto stage_bytes = [&](int s) -> uint32_t {
-        return (uint32_t)(((s < g.Nz - 1) ? 2 : 3) * bs * sizeof(TS));
+    const PcFrame fr{rank, TW ? (rank == 0 ? g.zs : Nz - g.zs - 2) : Nz, Nz};
+    const int n = fr.n;
+    double* xs = dsm;                          // [Nz][LD] local planes: b, then z (forward, in place); r on the separator
+    double* xb = xs + (int64_t)Nz * LD;        // [Nz][LD]: x (backward sweep); padding columns zero
+    double* xch = xb + (int64_t)Nz * LD;       // [2][LD]: this rank's partial right-hand sides of the separator (TW)
+    TS* buf0 = reinterpret_cast<TS*>(xch + 2 * LD);   // NBUF ring buffers of [3 bs]
+    const TS* base = A + (int64_t)part * Nz * 5 * bs;
+    const int S = TW ? 2 * n + 3 : 2 * Nz - 1;
+    // local planes whose b this CTA reads and whose x it writes
+    const int nio = TW ? (rank == 0 ? n + 2 : n) : Nz;
+    auto blk = [&](int t, int sl) -> const TS* { return base + ((int64_t)fr.gp(t) * 5 + fr.gs(sl)) * bs; };
+    // the stage's copies: one contiguous run of slots, plus (TW stage X) one more block
+    auto issue = [&](int s, uint32_t dst, uint32_t bar) {
+        const uint32_t b1 = (uint32_t)(bs * sizeof(TS));
+        const TS* src;
+        uint32_t nblk;
+        const TS* src2 = nullptr;
+        if (s < n - 1) {                                   // F(t): slots 0, 1
+            src = (fr.rank == 0) ? blk(s + 1, 0) : blk(s + 1, 1);
+            nblk = 2;
+        } else if (TW && s == n - 1) {                     // X: plane n slots 0, 1; plane n+1 slot 0
+            src = (fr.rank == 0) ? blk(n, 0) : blk(n, 1);
+            nblk = 2;
+            src2 = blk(n + 1, 0);
+        } else if (TW && s <= n + 2) {                     // C0, C1: plane zs+1 slot 1, 2; C2: plane zs slots 2, 3
+            const int i = s - n;
+            src = (i < 2) ? base + ((int64_t)(g.zs + 1) * 5 + 1 + i) * bs : base + ((int64_t)g.zs * 5 + 2) * bs;
+            nblk = (i < 2) ? 1 : 2;
+        } else {                                           // B(t): slots 2..4
+            const int t = TW ? n - 1 - (s - (n + 3)) : Nz - 1 - (s - (Nz - 1));
+            src = (fr.rank == 0) ? blk(t, 2) : blk(t, 4);
+            nblk = 3;
+        }
+        const uint32_t tot = (nblk + (src2 ? 1u : 0u)) * b1;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tot) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(dst), "l"(src), "r"(nblk * b1), "r"(bar) : "memory");
+        if (src2)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(dst + nblk * b1), "l"(src2), "r"(b1), "r"(bar) : "memory");
     };
     if (tid == 0) {
         for (int q = 0; q < NBUF; ++q) mbar_init(smem_u32(&bars[q]), 1);
@@ -775,16 +937,15 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
     }
     __syncthreads();
     if (tid == 0)                                // the first NBUF stages are in flight from the start
-        for (int q = 0; q < NBUF && q < S; ++q)
-            bulk_load(smem_u32(buf0 + (int64_t)q * 3 * bs), stage_src(q), stage_bytes(q), smem_u32(&bars[q]));
+        for (int q = 0; q < NBUF && q < S; ++q) issue(q, smem_u32(buf0 + (int64_t)q * 3 * bs), smem_u32(&bars[q]));
     const int fcol = F.V ? *F.col : 0;
     const double fscale = F.V ? *F.scale : 0.0;
     const double* fsrc = (fcol == 0) ? F.src0 : F.src1;
-    for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
-        const int k = q / LD, l = q - k * LD;
+    for (int q = tid; q < Nz * LD; q += blockDim.x) {
+        const int t = q / LD, l = q - t * LD;
         double v = 0.0;
-        if (l < nb) {
-            const int64_t gi = pc_glob(g, part, k, l);
+        if (l < nb && t < nio) {
+            const int64_t gi = pc_glob(g, part, fr.gp(t), l);
             double bv;
             if (F.V) {                           // normalise the basis vector on the way in
                 bv = fscale * fsrc[gi];
@@ -796,75 +957,149 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         }
         xs[q] = v;
     }
-    for (int q = tid; q < g.Nz * LD; q += blockDim.x) xb[q] = 0.0;
+    for (int q = tid; q < Nz * LD; q += blockDim.x) xb[q] = 0.0;
     __syncthreads();
     const int lane = tid % PA_LANES;
-    const int r = tid / PA_LANES;              // one row per 8 lanes: 64 rows (nb <= 64)
-    bool ok = true;
-    int s_fail = S;
+    const int grp = tid / PA_LANES;            // 8 lanes per group, two rows per group: r0 and r0 + rh
+    const int rh = (nb + 1) >> 1;
+    const int r0 = grp, r1 = grp + rh;
+    const bool act0 = r0 < rh, act1 = act0 && r1 < nb;
     int issued = (S < NBUF) ? S : NBUF;        // stages whose copies have been issued
+    int bi = 0, pb = NBUF - 1;                 // this stage's ring buffer, the previous stage's
+    uint32_t par = 0;
+    // one block times one solution plane for both rows of the group (the vector loads are shared)
+    auto dot2 = [&](const TS* M, const double* v, double& acc0, double& acc1) {
+        const TS* ma = M + r0 * LD;
+        const TS* mb = M + (act1 ? r1 : r0) * LD;
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const double vv = v[lane + PA_LANES * j];
+            acc0 += (double)ma[lane + PA_LANES * j] * vv;
+            acc1 += (double)mb[lane + PA_LANES * j] * vv;
+        }
+    };
+    auto reduce = [&](double& acc0, double& acc1) {
+#pragma unroll
+        for (int off = PA_LANES / 2; off > 0; off >>= 1) {
+            acc0 += __shfl_xor_sync(0xffffffffu, acc0, off, PA_LANES);
+            acc1 += __shfl_xor_sync(0xffffffffu, acc1, off, PA_LANES);
+        }
+    };
+    auto put = [&](double* row, double a0, double a1, bool sub) {
+        if (lane == 0 && act0) {
+            row[r0] = sub ? row[r0] - a0 : a0;
+            if (act1) row[r1] = sub ? row[r1] - a1 : a1;
+        }
+    };
     // One barrier per stage: it publishes the previous stage's rows and frees its buffer, which is
-    // refilled right after it.  Forward rows overwrite b_k by z_k in xs (each row reads and writes
-    // only its own entry of plane k); backward rows go to xb, as every row reads all of z_k.
-    for (int s = 0; s < S; ++s) {
-        const int bi = s % NBUF;
+    // refilled right after it.  Forward rows overwrite b_t by z_t in xs (each row reads and writes
+    // only its own entry of plane t); backward rows go to xb, as every row reads all of z_t.  Warp 0
+    // alone polls the copy's mbarrier; the barrier carries its answer to the others.
+    auto stage = [&](int s) -> bool {
         TS* buf = buf0 + (int64_t)bi * 3 * bs;
-        const bool arrived = mbar_wait(smem_u32(&bars[bi]), (uint32_t)((s / NBUF) & 1));
+        const bool arrived = (tid < 32) ? mbar_wait(smem_u32(&bars[bi]), par) : true;
         if (!__syncthreads_and(arrived)) {       // uniform decision: no thread is left at a barrier
-            ok = false;
-            s_fail = s;
             if (tid == 0) atomicOr(err, 1);
-            break;
+            return false;
         }
         if (s >= 1 && s - 1 + NBUF < S) {        // the previous stage's buffer is free: refill it
             if (tid == 0) {
-                const int sn = s - 1 + NBUF, bn = (s - 1) % NBUF;
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                bulk_load(smem_u32(buf0 + (int64_t)bn * 3 * bs), stage_src(sn), stage_bytes(sn), smem_u32(&bars[bn]));
+                issue(s - 1 + NBUF, smem_u32(buf0 + (int64_t)pb * 3 * bs), smem_u32(&bars[pb]));
             }
             issued = s + NBUF;
         }
-        const bool fwd = s < g.Nz - 1;
-        const int k = fwd ? s + 1 : g.Nz - 1 - (s - (g.Nz - 1));
-        double acc = 0.0;
-        if (r < nb) {
-            if (fwd) {                           // [L1 | L2] . [z_{k-1} ; z_{k-2}]
-                const TS* m1 = buf + bs + r * LD;
-                const double* v1 = xs + (int64_t)(k - 1) * LD;
-#pragma unroll
-                for (int j = 0; j < NJ; ++j) acc += (double)m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
-                if (k >= 2) {
-                    const TS* m2 = buf + r * LD;
-                    const double* v2 = xs + (int64_t)(k - 2) * LD;
-#pragma unroll
-                    for (int j = 0; j < NJ; ++j) acc += (double)m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
+        const int64_t oL2 = (fr.rank == 0) ? 0 : bs, oL1 = (fr.rank == 0) ? bs : 0;
+        double a0 = 0.0, a1 = 0.0;
+        if (s < n - 1) {                                       // F(t)
+            const int t = s + 1;
+            if (act0) {
+                dot2(buf + oL1, xs + (int64_t)(t - 1) * LD, a0, a1);
+                if (t >= 2) dot2(buf + oL2, xs + (int64_t)(t - 2) * LD, a0, a1);
+            }
+            reduce(a0, a1);
+            put(xs + (int64_t)t * LD, a0, a1, true);
+        } else if (TW && s == n - 1) {                         // X: partial right-hand sides of the separator
+            if (act0) {
+                dot2(buf + oL1, xs + (int64_t)(n - 1) * LD, a0, a1);
+                dot2(buf + oL2, xs + (int64_t)(n - 2) * LD, a0, a1);
+            }
+            reduce(a0, a1);
+            if (lane == 0 && act0) {
+                xch[r0] = xs[(int64_t)n * LD + r0] - a0;
+                if (act1) xch[r1] = xs[(int64_t)n * LD + r1] - a1;
+            }
+            a0 = a1 = 0.0;
+            if (act0) dot2(buf + 2 * bs, xs + (int64_t)(n - 1) * LD, a0, a1);
+            reduce(a0, a1);
+            if (lane == 0 && act0) {
+                xch[LD + r0] = xs[(int64_t)(n + 1) * LD + r0] - a0;
+                if (act1) xch[LD + r1] = xs[(int64_t)(n + 1) * LD + r1] - a1;
+            }
+        } else if (TW && s <= n + 2) {                         // C0..C2: both ranks solve the separator
+            const int i = s - n;
+            const int lz0 = (fr.rank == 0) ? n : n + 1;        // local planes of global zs, zs+1
+            const int lz1 = 2 * n + 1 - lz0;
+            if (i == 0) {
+                if (act0) dot2(buf, xs + (int64_t)lz0 * LD, a0, a1);
+                reduce(a0, a1);
+                put(xs + (int64_t)lz1 * LD, a0, a1, true);
+            } else if (i == 1) {
+                if (act0) dot2(buf, xs + (int64_t)lz1 * LD, a0, a1);
+                reduce(a0, a1);
+                put(xb + (int64_t)lz1 * LD, a0, a1, false);
+            } else {
+                if (act0) {
+                    dot2(buf, xs + (int64_t)lz0 * LD, a0, a1);
+                    dot2(buf + bs, xb + (int64_t)lz1 * LD, a0, a1);
                 }
-            } else {                             // [Uinv | -W1 | -W2] . [z_k ; x_{k+1} ; x_{k+2}]
-                const TS* m0 = buf + r * LD;
-                const double* v0 = xs + (int64_t)k * LD;
-#pragma unroll
-                for (int j = 0; j < NJ; ++j) acc += (double)m0[lane + PA_LANES * j] * v0[lane + PA_LANES * j];
-                if (k + 1 < g.Nz) {
-                    const TS* m1 = buf + bs + r * LD;
-                    const double* v1 = xb + (int64_t)(k + 1) * LD;
-#pragma unroll
-                    for (int j = 0; j < NJ; ++j) acc += (double)m1[lane + PA_LANES * j] * v1[lane + PA_LANES * j];
-                }
-                if (k + 2 < g.Nz) {
-                    const TS* m2 = buf + 2 * bs + r * LD;
-                    const double* v2 = xb + (int64_t)(k + 2) * LD;
-#pragma unroll
-                    for (int j = 0; j < NJ; ++j) acc += (double)m2[lane + PA_LANES * j] * v2[lane + PA_LANES * j];
-                }
+                reduce(a0, a1);
+                put(xb + (int64_t)lz0 * LD, a0, a1, false);
+            }
+        } else {                                               // B(t)
+            const int t = TW ? n - 1 - (s - (n + 3)) : Nz - 1 - (s - (Nz - 1));
+            const int lim = TW ? n + 2 : Nz;
+            const int64_t oU = (fr.rank == 0) ? 0 : 2 * bs, oW2 = (fr.rank == 0) ? 2 * bs : 0;
+            if (act0) {
+                dot2(buf + oU, xs + (int64_t)t * LD, a0, a1);
+                if (t + 1 < lim) dot2(buf + bs, xb + (int64_t)(t + 1) * LD, a0, a1);
+                if (t + 2 < lim) dot2(buf + oW2, xb + (int64_t)(t + 2) * LD, a0, a1);
+            }
+            reduce(a0, a1);
+            put(xb + (int64_t)t * LD, a0, a1, false);
+        }
+        pb = bi;
+        if (++bi == NBUF) {
+            bi = 0;
+            par ^= 1u;
+        }
+        return true;
+    };
+    bool ok = true;
+    int s = 0;
+    const int s_x = TW ? n : S;                  // stages before the exchange
+    for (; s < s_x && ok; ++s) ok = stage(s);
+    if constexpr (TW) {
+        __syncthreads();                         // this rank's partials are in xch
+        cluster_sync_all();                      // ... and the other rank's (both ranks always arrive)
+        if (ok) {
+            const uint32_t other = (uint32_t)(fr.rank ^ 1);
+            for (int q = tid; q < 2 * LD; q += blockDim.x) {
+                const int c = q / LD, l = q - c * LD;   // separator plane zs + c, row l
+                if (l >= nb) continue;
+                // plane zs + c is slot c of rank 0's xch and slot 1 - c of rank 1's; the sum is
+                // taken in the same order on both ranks, so both hold the same r
+                const double* q0 = xch + c * LD + l;
+                const double* q1 = xch + (1 - c) * LD + l;
+                const double p0 = (fr.rank == 0) ? *q0 : ld_peer_cta(q0, other);
+                const double p1 = (fr.rank == 0) ? ld_peer_cta(q1, other) : *q1;
+                xs[(int64_t)(n + ((fr.rank == 0) ? c : 1 - c)) * LD + l] = p0 + p1;
             }
         }
-#pragma unroll
-        for (int off = PA_LANES / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off, PA_LANES);
-        if (r < nb && lane == 0) {
-            if (fwd) xs[(int64_t)k * LD + r] = xs[(int64_t)k * LD + r] - acc;
-            else xb[(int64_t)k * LD + r] = acc;
-        }
+        __syncthreads();
     }
+    for (; s < S && ok; ++s) ok = stage(s);
+    const int s_fail = ok ? S : s - 1;           // first stage whose data was not consumed
     __syncthreads();                             // the last stage's rows
     double ss = 0.0;
     if (!ok) {                                   // drain copies still in flight (bounded) and leave x untouched
@@ -872,10 +1107,10 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             for (int s2 = s_fail; s2 < issued; ++s2)
                 mbar_wait(smem_u32(&bars[s2 % NBUF]), (uint32_t)((s2 / NBUF) & 1));
     } else {
-        for (int q = tid; q < g.Nz * LD; q += blockDim.x) {
-            const int k = q / LD, l = q - k * LD;
-            if (l < nb) {
-                const int64_t gi = pc_glob(g, part, k, l);
+        for (int q = tid; q < Nz * LD; q += blockDim.x) {
+            const int t = q / LD, l = q - t * LD;
+            if (l < nb && t < nio) {
+                const int64_t gi = pc_glob(g, part, fr.gp(t), l);
                 const double xv = sc ? xb[q] / sc[gi] : xb[q];
                 x[gi] = xv;
                 ss += xv * xv;
@@ -892,7 +1127,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         if (tid == 0) {
             double t = 0.0;
             for (int w = 0; w < PA_THREADS / 32; ++w) t += wsum[w];
-            F.part[part] = t;
+            F.part[blockIdx.x] = t;
             __threadfence();
             last = (atomicAdd(F.ticket, 1u) == gridDim.x - 1);
         }
@@ -905,6 +1140,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             *F.ticket = 0u;
         }
     }
+    if constexpr (TW) cluster_sync_all();        // the other rank has finished reading this CTA's xch
 }
 
 // Sweep for partitions too large for the shared-memory pipeline: same fused stages, operands read
@@ -983,6 +1219,14 @@ static PcGeom geom_of(const dv_model* m, int mode) {
     }
     g.ld = pc_ld(g.nb);
     g.bs = (((int64_t)g.nb * g.ld + 1) / 2) * 2;
+    g.zs = 0;
+    return g;
+}
+
+// the geometry the current factors were computed with
+static PcGeom geom_factored(const dv_model* m) {
+    PcGeom g = geom_of(m, m->pc_mode);
+    g.zs = m->pc_zs;
     return g;
 }
 
@@ -1003,6 +1247,40 @@ int64_t precond_work_doubles(int nb, int nparts, int Nz) {
     return std::max((int64_t)nparts * 4 * (int64_t)nb * ld, (int64_t)nparts * Nz * (int64_t)ld);
 }
 
+// a launch of `kern` as clusters of two CTAs (grid = 2 x partitions)
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pair(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t dyn, cudaStream_t s,
+                               Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = dyn;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
+static size_t apply_smem(const PcGeom& g, int nbuf, size_t tsize);
+static bool apply_fusable(const PcGeom& g, size_t tsize);
+static size_t pc_tsize(const dv_model* m);
+
+// Twisted factorisation: the top-down and bottom-up eliminations run at the same time and meet at
+// the separator planes zs, zs+1, which halves the sequential plane chain of the factorisation and
+// of both sweeps.  Taken when each direction keeps at least three planes and both kernels run from
+// shared memory; DVTSA_PC_TWIST=0 keeps the one-directional form.
+static int pc_twist_zs(const PcGeom& g, size_t tsize, bool factor_smem) {
+    const char* e = getenv("DVTSA_PC_TWIST");
+    if (e && e[0] == '0') return 0;
+    if (g.Nz < 8 || !factor_smem || !apply_fusable(g, tsize)) return 0;
+    return (g.Nz - 2) / 2;
+}
+
 int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s) {
     PcGeom g = geom_of(m, mode);
     if (g.nb > m->pc_cap_nb || g.nparts > m->pc_cap_parts) {
@@ -1019,10 +1297,19 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
     DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_scatter<<<grid, 128, 0, s>>>(g, J, dh, m->d_pc));
     const int optin = smem_optin();
     const size_t n2b = (size_t)g.nb * g.ld * sizeof(double);
-    if (g.nb <= PC_SMEM_NB && 9 * n2b + 2048 <= (size_t)optin) {
+    const bool factor_smem = g.nb <= PC_SMEM_NB && 9 * n2b + 2048 <= (size_t)optin;
+    g.zs = pc_twist_zs(g, pc_tsize(m), factor_smem);
+    if (factor_smem && g.zs > 0) {
         size_t dyn = 9 * n2b;
-        if (dyn > 48 * 1024) DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_smem<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_info));
+        if (dyn > 48 * 1024)
+            DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        DV_LAUNCH(dv::K_PC_FACTOR, s,
+                  DV_CUDA(launch_pair(k_pc_factor_smem<true>, 2u * g.nparts, 256u, dyn, s, g, m->d_pc, m->d_pc_info)));
+    } else if (factor_smem) {
+        size_t dyn = 9 * n2b;
+        if (dyn > 48 * 1024)
+            DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_smem<false><<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_info));
     } else {
         const size_t static_smem = (2 * 1024 + 256) * sizeof(double) + 256 * sizeof(int);
         size_t need = (size_t)2 * g.nb * g.nb * sizeof(double);
@@ -1040,6 +1327,7 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
     m->pc_mode = g.mode;
     m->pc_nb = g.nb;
     m->pc_nparts = g.nparts;
+    m->pc_zs = g.zs;
     m->pc_ready = 1;
     return DV_OK;
 }
@@ -1047,7 +1335,7 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
 // shared memory of the sweep with an NBUF-deep ring: solution planes, one plane of scratch, buffers
 // shared memory of the sweep with an NBUF-deep ring of factor blocks stored as `tsize`-byte values
 static size_t apply_smem(const PcGeom& g, int nbuf, size_t tsize) {
-    return sizeof(double) * (size_t)(2 * (int64_t)g.Nz * g.ld) + tsize * (size_t)((int64_t)nbuf * 3 * g.bs);
+    return sizeof(double) * (size_t)(2 * (int64_t)g.Nz * g.ld + 2 * g.ld) + tsize * (size_t)((int64_t)nbuf * 3 * g.bs);
 }
 
 static size_t pc_tsize(const dv_model* m) { return m->pc_fp32 ? sizeof(float) : sizeof(double); }
@@ -1055,17 +1343,23 @@ static size_t pc_tsize(const dv_model* m) { return m->pc_fp32 ? sizeof(float) : 
 // ring depth: three stages in flight when they fit in shared memory, else two
 static int apply_nbuf(const PcGeom& g, size_t tsize) { return apply_smem(g, 3, tsize) <= (size_t)smem_optin() ? 3 : 2; }
 
+template <int NJ, int NBUF, typename TS, bool TW>
+static void launch_apply_tw(const PcGeom& g, dv_model* m, const TS* A, const double* b, const double* sc, double* x,
+                            cudaStream_t s, const PaFuse& F, bool count) {
+    const size_t dyn = apply_smem(g, NBUF, sizeof(TS));
+    auto kern = k_pc_apply<NJ, NBUF, TS, TW>;
+    if (count && dyn > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (count) prof_begin(dv::K_PC_APPLY, s);
+    if (TW) launch_pair(kern, 2u * g.nparts, PA_THREADS, dyn, s, g, A, b, sc, x, m->d_err, F);
+    else kern<<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F);
+    if (count) prof_end(dv::K_PC_APPLY, s);
+}
+
 template <int NJ, int NBUF, typename TS>
 static void launch_apply_k(const PcGeom& g, dv_model* m, const TS* A, const double* b, const double* sc, double* x,
                            cudaStream_t s, const PaFuse& F, bool count) {
-    const size_t dyn = apply_smem(g, NBUF, sizeof(TS));
-    if (count) {
-        if (dyn > 48 * 1024)
-            cudaFuncSetAttribute(k_pc_apply<NJ, NBUF, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        DV_LAUNCH(dv::K_PC_APPLY, s, k_pc_apply<NJ, NBUF, TS><<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F));
-    } else {
-        k_pc_apply<NJ, NBUF, TS><<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F);
-    }
+    if (g.zs > 0) launch_apply_tw<NJ, NBUF, TS, true>(g, m, A, b, sc, x, s, F, count);
+    else launch_apply_tw<NJ, NBUF, TS, false>(g, m, A, b, sc, x, s, F, count);
 }
 
 template <int NJ>
@@ -1095,7 +1389,7 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
         set_error("preconditioner applied before it was factorised");
         return DV_ERR_ARG;
     }
-    PcGeom g = geom_of(m, m->pc_mode);
+    PcGeom g = geom_factored(m);
     if (precond_apply_fusable(m)) {
         launch_apply(g, m, b, sc, x, s, PaFuse(), true);
     } else {
@@ -1109,16 +1403,16 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
     return DV_OK;
 }
 
-bool precond_apply_fusable(dv_model* m) {
-    PcGeom g = geom_of(m, m->pc_mode);
+static bool apply_fusable(const PcGeom& g, size_t tsize) {
     const int nj = g.ld / PA_LANES;
-    return g.nb <= 64 && apply_smem(g, 2, pc_tsize(m)) <= (size_t)smem_optin() &&
-           (nj == 1 || nj == 3 || nj == 5 || nj == 7);
+    return g.nb <= 64 && apply_smem(g, 2, tsize) <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7);
 }
+
+bool precond_apply_fusable(dv_model* m) { return apply_fusable(geom_factored(m), pc_tsize(m)); }
 
 int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
                           const PaFuse& F) {
-    PcGeom g = geom_of(m, m->pc_mode);
+    PcGeom g = geom_factored(m);
     if (precond_apply_fusable(m)) {
         launch_apply(g, m, b, sc, x, s, F, false);    // attributes were set by an earlier precond_apply
     } else {

@@ -1058,6 +1058,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     W.gm_mode = m->pc_mode;
     W.gm_nb = m->pc_nb;
     W.gm_nparts = m->pc_nparts;
+    W.gm_zs = m->pc_zs;
     W.gm_fp32 = m->pc_fp32;
     for (int k = 0; k < K_NKIND; ++k) {
         W.gm_fixed[k] = fixed[k];
@@ -1072,7 +1073,7 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
                        int64_t* inner, cudaStream_t st) {
     dv_model* m = op.m;
     if (!W.gm_exec || W.gm_kdim != kdim || W.gm_mode != m->pc_mode || W.gm_nb != m->pc_nb ||
-        W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32)
+        W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32 || W.gm_zs != m->pc_zs)
         DV_TRY(gm_build(m, W, kdim));
     GmHost* hst = (GmHost*)W.gm_host;
     hst->args[0] = op.t;
