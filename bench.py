@@ -216,11 +216,25 @@ class ClockSampler:
 ALG_BYTES_DOC = {
     "matvec": "FD matvec residual: reads z, u, s, f (4 n_core) + writes n_core doubles",
     "residual": "residual: reads y (+ rhs_known) and writes f: 2 n_core doubles",
-    "precond_apply": "sweep: reads the 5 factor blocks of every plane of every partition + 3 n_core doubles",
+    "precond_apply": "sweep: reads the 5 nb x nb factor blocks of every plane of every partition + 3 n_core doubles",
     "fd_jacobian": "reads y, f0 (2 n_core) + writes the 9*49*ncell block layout",
     "precond_factor": "assembly + factorisation: writes and re-reads 5 blocks per plane",
     "vector": "Krylov vector kernels: ~3 n_core doubles per launch (average)",
 }
+
+
+def partition_sizes(m):
+    """Unknowns per z-partition of the preconditioner the solver builds for model m (block nb of
+    each partition): theta_block with >= 1 coupled ring = the innermost ring of all sectors plus
+    rings 1.. of each sector with its wall node; theta_block with 0 rings = whole sectors; full =
+    one partition (also for a single sector)."""
+    g, s, w = m.grid, m.cfg.solver, (1 if m.n_w else 0)
+    mode = s.preconditioner if g.Nth > 1 else "full"
+    if mode == "theta_block" and s.precond_theta_rings >= 1 and g.Nr >= 2:
+        return [6 * (g.Nr - 1) + w] * g.Nth + [6 * g.Nth]
+    if mode == "theta_block":
+        return [6 * g.Nr + w] * g.Nth
+    return [6 * g.Nr * g.Nth + w * g.Nth]
 
 
 def alg_bytes_per_launch(kind, m):
@@ -231,9 +245,7 @@ def alg_bytes_per_launch(kind, m):
         return 2 * n * 8
     if kind == "fd_jacobian":
         return (2 * n + m.jac_doubles) * 8
-    nb = 6 * m.grid.Nr + (1 if m.n_w else 0)
-    parts = m.grid.Nth
-    blocks = parts * m.grid.Nz * 5 * nb * nb * 8
+    blocks = m.grid.Nz * 5 * sum(nb * nb for nb in partition_sizes(m)) * 8
     if kind == "precond_apply":
         return blocks + 3 * n * 8
     if kind == "precond_factor":
@@ -366,6 +378,11 @@ def gpu_arm(a, rank, world, local_rank):
                 "alg_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
                 "alg_bytes_rule": ALG_BYTES_DOC.get(dom, ""),
                 "kernel_share": {k: round(v[2] / sum(x[2] for x in kinds.values()), 4) for k, v in kinds.items()},
+                # device time of the profiled cycle summed over its timed launches (each bracketed by
+                # events, so it slightly overstates); the rest of ms_per_step is host work and gaps
+                "kernel_ms_per_cycle": round(sum(x[2] for x in kinds.values()), 1),
+                "timed_launches": int(sum(x[1] for x in kinds.values())),
+                "launches_per_cycle": int(sum(x[0] for x in kinds.values())),
                 "kernel_avg_us": {k: round(1e3 * v[2] / v[1], 3) for k, v in kinds.items()}}
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:

@@ -20,6 +20,7 @@
 //   forward  z_k = b_k - L1_k z_{k-1} - L2_k z_{k-2}
 //   backward x_k = Uinv_k z_k + (-Uinv_k U1_k) x_{k+1} + (-Uinv_k U2_k) x_{k+2}
 #include <algorithm>
+#include <type_traits>
 #include "dv_internal.h"
 #include "dv_physics.cuh"
 
@@ -52,12 +53,17 @@ static __device__ __forceinline__ int pc_part_of(const PcGeom& g, int i, int j) 
 
 #define PC_SMEM_NB 56      // largest block the shared-memory factorisation keeps resident (9 blocks)
 
-// leading dimension: nb rounded up to 8 and kept == 8 (mod 16) so the 4 rows a warp reads in the
-// sweep fall on alternating shared-memory bank halves
-static inline int pc_ld(int nb) {
-    int ld = (nb + 7) / 8 * 8;
-    if (ld % 16 == 0) ld += 8;
-    return ld;
+// leading dimension of the stored blocks: nb rounded up to 16, so a row is a whole number of
+// 16-column groups that the sweep's 8 lanes read as 16-byte column pairs
+static inline int pc_ld(int nb) { return (nb + 15) / 16 * 16; }
+
+// leading dimension of the blocks the factorisation keeps in shared memory: nb rounded up to 4 and
+// made == 4 (mod 8), so the 8 rows of a DMMA A fragment (and the 4 rows of a B fragment) start on
+// different 8-bank groups; without that padding when nine blocks would not fit
+static inline int pc_lds(int nb, size_t budget) {
+    const int l4 = (nb + 3) / 4 * 4;
+    const int l = (l4 % 8 == 0) ? l4 + 4 : l4;
+    return (size_t)9 * nb * l * sizeof(double) <= budget ? l : l4;
 }
 
 static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int k, int l) {
@@ -200,10 +206,11 @@ static __device__ void sm_gemm(int nb, int ld, double alpha, const double* A, co
     __syncthreads();
 }
 
-// C = beta C + alpha Bd X with Bd block diagonal (cell blocks) in shared memory.
-static __device__ void sm_bd_left(const PcGeom& g, double alpha, const double* Bd, const double* X, double beta,
-                                  double* C) {
-    const int nb = g.nb, ld = g.ld;
+// C = beta C + alpha Bd X with Bd block diagonal (cell blocks); all three in shared memory with
+// leading dimension ld.
+static __device__ void sm_bd_left(const PcGeom& g, int ld, double alpha, const double* Bd, const double* X,
+                                  double beta, double* C) {
+    const int nb = g.nb;
     const int tx = threadIdx.x % SM_T, ty = threadIdx.x / SM_T;
 #pragma unroll
     for (int a = 0; a < SM_R; ++a) {
@@ -224,10 +231,11 @@ static __device__ void sm_bd_left(const PcGeom& g, double alpha, const double* B
     __syncthreads();
 }
 
-// C = beta C + alpha X Bd with Bd block diagonal (any memory space).
-static __device__ void sm_bd_right(const PcGeom& g, double alpha, const double* X, const double* Bd, double beta,
-                                   double* C) {
-    const int nb = g.nb, ld = g.ld;
+// C = beta C + alpha X Bd with Bd block diagonal (any memory space, leading dimension ldb); X and C
+// in shared memory with leading dimension ld.
+static __device__ void sm_bd_right(const PcGeom& g, int ld, double alpha, const double* X, const double* Bd,
+                                   int ldb, double beta, double* C) {
+    const int nb = g.nb;
     const int tx = threadIdx.x % SM_T, ty = threadIdx.x / SM_T;
 #pragma unroll
     for (int b = 0; b < SM_R; ++b) {
@@ -240,7 +248,7 @@ static __device__ void sm_bd_right(const PcGeom& g, double alpha, const double* 
             const int r = ty + SM_T * a;
             if (r >= nb) continue;
             double acc = 0.0;
-            for (int q = b0; q < b0 + bsz; ++q) acc += X[r * ld + q] * Bd[q * ld + c];
+            for (int q = b0; q < b0 + bsz; ++q) acc += X[r * ld + q] * Bd[q * ldb + c];
             double* cp = C + r * ld + c;
             *cp = (beta == 0.0) ? alpha * acc : beta * (*cp) + alpha * acc;
         }
@@ -484,8 +492,39 @@ static __device__ int sm_inverse(int nb, int ld, double*& A, double*& B, int* pe
     return sm_inverse_unb(nb, ld, A, B, perm, idx, pv, pi);
 }
 
-static __device__ void cp_block(int64_t n, const double* src, double* dst) {
-    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) dst[q] = src[q];
+// rows x columns < nb of a block, global (leading dimension ld) <-> shared memory (lds); the
+// padding columns keep the zeros they were given.  256 threads, nb <= PC_SMEM_NB: thread t moves
+// the entries t + 256 i (row-major over nb x nb), i < CP_K, stepping (row, column) without a
+// division; cp_in issues all of its global loads before the first shared store, so one copy
+// costs one L2 round trip.
+#define CP_K 13                                  // 13 * 256 >= 56 * 56
+static __device__ void cp_in(int nb, int ld, int lds, const double* __restrict__ src, double* __restrict__ dst) {
+    const int dr = 256 / nb, dc = 256 - dr * nb;
+    int r = threadIdx.x / nb, c = threadIdx.x - r * nb;
+    double v[CP_K];
+    int off[CP_K];
+#pragma unroll
+    for (int i = 0; i < CP_K; ++i) {
+        off[i] = (r < nb) ? r * lds + c : -1;
+        v[i] = (r < nb) ? src[r * ld + c] : 0.0;
+        r += dr;
+        c += dc;
+        if (c >= nb) { c -= nb; ++r; }
+    }
+#pragma unroll
+    for (int i = 0; i < CP_K; ++i)
+        if (off[i] >= 0) dst[off[i]] = v[i];
+}
+static __device__ void cp_out(int nb, int ld, int lds, const double* __restrict__ src, double* __restrict__ dst) {
+    const int dr = 256 / nb, dc = 256 - dr * nb;
+    int r = threadIdx.x / nb, c = threadIdx.x - r * nb;
+#pragma unroll
+    for (int i = 0; i < CP_K; ++i) {
+        if (r < nb) dst[r * ld + c] = src[r * lds + c];
+        r += dr;
+        c += dc;
+        if (c >= nb) { c -= nb; ++r; }
+    }
 }
 
 // ---------------------------------------------------------------- clusters of two CTAs
@@ -523,7 +562,7 @@ static __device__ __forceinline__ int ld_peer_cta(const int* p, uint32_t rank) {
 //   plane zs:   slot 2 Dm^-1 = S11^-1,  slot 3 -Dm^-1 S12
 //   plane zs+1: slot 1 S21 Dm^-1,       slot 2 Dn^-1 = (S22 - S21 Dm^-1 S12)^-1
 template <bool TW>
-__global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __restrict__ A, int* __restrict__ info) {
+__global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __restrict__ A, int* __restrict__ info, int lds) {
     const int rank = TW ? (int)(blockIdx.x & 1u) : 0;
     const int part = TW ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
     const PcGeom g = pc_part(gin, part);
@@ -533,7 +572,7 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
     __shared__ int pi[8];
     __shared__ int qoff[4], sbad;
     const int nb = g.nb, ld = g.ld;
-    const int n2 = nb * ld;
+    const int n2 = nb * lds;                   // one shared-memory block
     const int Nz = g.Nz;
     const int n = TW ? (rank == 0 ? g.zs : Nz - g.zs - 2) : Nz;
     double* buf[9];
@@ -550,35 +589,35 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
     };
     int bad = 0;
     for (int k = 0; k < n; ++k) {
-        if (k >= 2) cp_block(n2, B(k, 0), S0);
-        if (k >= 1) cp_block(n2, B(k, 1), S1);
-        cp_block(n2, B(k, 2), S2);
-        cp_block(n2, B(k, 3), S3);
+        if (k >= 2) cp_in(nb, ld, lds, B(k, 0), S0);
+        if (k >= 1) cp_in(nb, ld, lds, B(k, 1), S1);
+        cp_in(nb, ld, lds, B(k, 2), S2);
+        cp_in(nb, ld, lds, B(k, 3), S3);
         __syncthreads();
         if (k >= 2) {
             double* U2_2 = B(k - 2, 4);                                        // A(k-2, k), block diagonal
-            sm_bd_left(g, 1.0, S0, Ui2, 0.0, T);                               // L2 = A(k,k-2) Uinv_{k-2}
+            sm_bd_left(g, lds, 1.0, S0, Ui2, 0.0, T);                               // L2 = A(k,k-2) Uinv_{k-2}
             double* t = S0; S0 = T; T = t;
-            sm_gemm(nb, ld, -1.0, S0, U12, 1.0, S1);                           // A(k,k-1) -= L2 U1_{k-2}
-            sm_bd_right(g, -1.0, S0, U2_2, 1.0, S2);                           // D -= L2 U2_{k-2}
-            sm_bd_right(g, -1.0, Ui2, U2_2, 0.0, T);                           // -Uinv_{k-2} U2_{k-2}
-            cp_block(n2, T, U2_2);                                             // (U2_{k-2} is not needed again)
+            sm_gemm(nb, lds, -1.0, S0, U12, 1.0, S1);                           // A(k,k-1) -= L2 U1_{k-2}
+            sm_bd_right(g, lds, -1.0, S0, U2_2, ld, 1.0, S2);                           // D -= L2 U2_{k-2}
+            sm_bd_right(g, lds, -1.0, Ui2, U2_2, ld, 0.0, T);                           // -Uinv_{k-2} U2_{k-2}
+            cp_out(nb, ld, lds, T, U2_2);                                             // (U2_{k-2} is not needed again)
             __syncthreads();
         }
         if (k >= 1) {
             const double* U2_1 = B(k - 1, 4);                                  // A(k-1, k+1), block diagonal
-            if (k == 1) sm_bd_left(g, 1.0, S1, Ui1, 0.0, T);                  // L1 = A(1,0) Uinv_0
-            else sm_gemm(nb, ld, 1.0, S1, Ui1, 0.0, T);                        // L1 = (...) Uinv_{k-1}
+            if (k == 1) sm_bd_left(g, lds, 1.0, S1, Ui1, 0.0, T);                  // L1 = A(1,0) Uinv_0
+            else sm_gemm(nb, lds, 1.0, S1, Ui1, 0.0, T);                        // L1 = (...) Uinv_{k-1}
             double* t = S1; S1 = T; T = t;
-            sm_gemm(nb, ld, -1.0, S1, U11, 1.0, S2);                           // D -= L1 U1_{k-1}
-            sm_bd_right(g, -1.0, S1, U2_1, 1.0, S3);                           // U1 = A(k,k+1) - L1 U2_{k-1}
+            sm_gemm(nb, lds, -1.0, S1, U11, 1.0, S2);                           // D -= L1 U1_{k-1}
+            sm_bd_right(g, lds, -1.0, S1, U2_1, ld, 1.0, S3);                           // U1 = A(k,k+1) - L1 U2_{k-1}
         }
-        bad |= sm_inverse(nb, ld, S2, T, perm, idx, pv, pi);              // (T: ping-pong buffer)
-        sm_gemm(nb, ld, -1.0, S2, S3, 0.0, T);                                 // -Uinv_k U1_k
-        if (k >= 2) cp_block(n2, S0, B(k, 0));
-        if (k >= 1) cp_block(n2, S1, B(k, 1));
-        cp_block(n2, S2, B(k, 2));
-        cp_block(n2, T, B(k, 3));
+        bad |= sm_inverse(nb, lds, S2, T, perm, idx, pv, pi);              // (T: ping-pong buffer)
+        sm_gemm(nb, lds, -1.0, S2, S3, 0.0, T);                                 // -Uinv_k U1_k
+        if (k >= 2) cp_out(nb, ld, lds, S0, B(k, 0));
+        if (k >= 1) cp_out(nb, ld, lds, S1, B(k, 1));
+        cp_out(nb, ld, lds, S2, B(k, 2));
+        cp_out(nb, ld, lds, T, B(k, 3));
         __syncthreads();
         // rotate: Uinv_{k-2} <- Uinv_{k-1} <- Uinv_k ; U1 likewise; freed blocks become S2 / S3
         double* fi = Ui2; Ui2 = Ui1; Ui1 = S2; S2 = fi;
@@ -589,37 +628,37 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
         if (threadIdx.x == 0) info[part] = bad;
     } else {
         // separator plane n: coupled to planes n-2 and n-1
-        cp_block(n2, B(n, 0), S0);                                             // A(n, n-2)
-        cp_block(n2, B(n, 1), S1);                                             // A(n, n-1)
+        cp_in(nb, ld, lds, B(n, 0), S0);                                             // A(n, n-2)
+        cp_in(nb, ld, lds, B(n, 1), S1);                                             // A(n, n-1)
         __syncthreads();
         double* U2_2 = B(n - 2, 4);                                            // A(n-2, n)
         double* U2_1 = B(n - 1, 4);                                            // A(n-1, n+1)
-        sm_bd_left(g, 1.0, S0, Ui2, 0.0, T);                                   // L2_n = A(n,n-2) Uinv_{n-2}
+        sm_bd_left(g, lds, 1.0, S0, Ui2, 0.0, T);                                   // L2_n = A(n,n-2) Uinv_{n-2}
         { double* t = S0; S0 = T; T = t; }
-        sm_gemm(nb, ld, -1.0, S0, U12, 1.0, S1);                               // A(n,n-1) - L2 U1_{n-2}
-        sm_bd_right(g, -1.0, S0, U2_2, 0.0, S2);                               // Q(n,n) = -L2 U2_{n-2}
-        sm_bd_right(g, -1.0, Ui2, U2_2, 0.0, T);                               // -Uinv_{n-2} U2_{n-2}
-        cp_block(n2, T, U2_2);
+        sm_gemm(nb, lds, -1.0, S0, U12, 1.0, S1);                               // A(n,n-1) - L2 U1_{n-2}
+        sm_bd_right(g, lds, -1.0, S0, U2_2, ld, 0.0, S2);                               // Q(n,n) = -L2 U2_{n-2}
+        sm_bd_right(g, lds, -1.0, Ui2, U2_2, ld, 0.0, T);                               // -Uinv_{n-2} U2_{n-2}
+        cp_out(nb, ld, lds, T, U2_2);
         __syncthreads();
-        sm_gemm(nb, ld, 1.0, S1, Ui1, 0.0, T);                                 // L1_n = (...) Uinv_{n-1}
+        sm_gemm(nb, lds, 1.0, S1, Ui1, 0.0, T);                                 // L1_n = (...) Uinv_{n-1}
         { double* t = S1; S1 = T; T = t; }
-        sm_gemm(nb, ld, -1.0, S1, U11, 1.0, S2);                               // Q(n,n) -= L1 U1_{n-1}
-        sm_bd_right(g, -1.0, S1, U2_1, 0.0, S3);                               // Q(n,n+1) = -L1 U2_{n-1}
-        cp_block(n2, S0, B(n, 0));
-        cp_block(n2, S1, B(n, 1));
+        sm_gemm(nb, lds, -1.0, S1, U11, 1.0, S2);                               // Q(n,n) -= L1 U1_{n-1}
+        sm_bd_right(g, lds, -1.0, S1, U2_1, ld, 0.0, S3);                               // Q(n,n+1) = -L1 U2_{n-1}
+        cp_out(nb, ld, lds, S0, B(n, 0));
+        cp_out(nb, ld, lds, S1, B(n, 1));
         __syncthreads();
         // separator plane n+1: coupled to plane n-1 only
-        cp_block(n2, B(n + 1, 0), S0);                                         // A(n+1, n-1)
+        cp_in(nb, ld, lds, B(n + 1, 0), S0);                                         // A(n+1, n-1)
         __syncthreads();
-        sm_bd_left(g, 1.0, S0, Ui1, 0.0, T);                                   // L2_{n+1} = A(n+1,n-1) Uinv_{n-1}
+        sm_bd_left(g, lds, 1.0, S0, Ui1, 0.0, T);                                   // L2_{n+1} = A(n+1,n-1) Uinv_{n-1}
         { double* t = S0; S0 = T; T = t; }
         double* Q10 = Ui2;                                                     // (Uinv_{n-2}, U1_{n-2}: done)
         double* Q11 = U12;
-        sm_gemm(nb, ld, -1.0, S0, U11, 0.0, Q10);                              // Q(n+1,n) = -L2 U1_{n-1}
-        sm_bd_right(g, -1.0, S0, U2_1, 0.0, Q11);                              // Q(n+1,n+1) = -L2 U2_{n-1}
-        sm_bd_right(g, -1.0, Ui1, U2_1, 0.0, T);                               // -Uinv_{n-1} U2_{n-1}
-        cp_block(n2, T, U2_1);
-        cp_block(n2, S0, B(n + 1, 0));
+        sm_gemm(nb, lds, -1.0, S0, U11, 0.0, Q10);                              // Q(n+1,n) = -L2 U1_{n-1}
+        sm_bd_right(g, lds, -1.0, S0, U2_1, ld, 0.0, Q11);                              // Q(n+1,n+1) = -L2 U2_{n-1}
+        sm_bd_right(g, lds, -1.0, Ui1, U2_1, ld, 0.0, T);                               // -Uinv_{n-1} U2_{n-1}
+        cp_out(nb, ld, lds, T, U2_1);
+        cp_out(nb, ld, lds, S0, B(n + 1, 0));
         if (threadIdx.x == 0) {
             qoff[0] = (int)(S2 - dsm);
             qoff[1] = (int)(S3 - dsm);
@@ -636,8 +675,11 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
             for (int q = 0; q < 4; ++q) ro[q] = ld_peer_cta(&qoff[3 - q], 1u);
             const double* Ab[4] = {B(n, 2), B(n, 3), B(n + 1, 1), B(n + 1, 2)};
             for (int q = 0; q < 4; ++q)
-                for (int e = threadIdx.x; e < n2; e += blockDim.x)
-                    Sb[q][e] = (Ab[q][e] + Sb[q][e]) + ld_peer_cta(dsm + ro[q] + e, 1u);
+                for (int r = threadIdx.x >> 5; r < nb; r += blockDim.x >> 5)
+                    for (int c = threadIdx.x & 31; c < nb; c += 32) {
+                        const int es = r * lds + c;
+                        Sb[q][es] = (Ab[q][r * ld + c] + Sb[q][es]) + ld_peer_cta(dsm + ro[q] + es, 1u);
+                    }
             if (threadIdx.x == 0) bad |= ld_peer_cta(&sbad, 1u);
         }
         __syncthreads();
@@ -646,15 +688,15 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
             double *S11 = Sb[0], *S12 = Sb[1], *S21 = Sb[2], *S22 = Sb[3];
             double* Xn = S0;                                                   // free: S0, S1, Ui1, U11 (+ T)
             double* Y = S1;
-            bad |= sm_inverse(nb, ld, S11, T, perm, idx, pv, pi);             // Dm^-1
-            sm_gemm(nb, ld, -1.0, S11, S12, 0.0, Xn);                          // -Dm^-1 S12
-            sm_gemm(nb, ld, 1.0, S21, S11, 0.0, Y);                            // S21 Dm^-1
-            sm_gemm(nb, ld, 1.0, S21, Xn, 1.0, S22);                           // S22 - S21 Dm^-1 S12
-            bad |= sm_inverse(nb, ld, S22, T, perm, idx, pv, pi);             // Dn^-1
-            cp_block(n2, S11, B(n, 2));
-            cp_block(n2, Xn, B(n, 3));
-            cp_block(n2, Y, B(n + 1, 1));
-            cp_block(n2, S22, B(n + 1, 2));
+            bad |= sm_inverse(nb, lds, S11, T, perm, idx, pv, pi);             // Dm^-1
+            sm_gemm(nb, lds, -1.0, S11, S12, 0.0, Xn);                          // -Dm^-1 S12
+            sm_gemm(nb, lds, 1.0, S21, S11, 0.0, Y);                            // S21 Dm^-1
+            sm_gemm(nb, lds, 1.0, S21, Xn, 1.0, S22);                           // S22 - S21 Dm^-1 S12
+            bad |= sm_inverse(nb, lds, S22, T, perm, idx, pv, pi);             // Dn^-1
+            cp_out(nb, ld, lds, S11, B(n, 2));
+            cp_out(nb, ld, lds, Xn, B(n, 3));
+            cp_out(nb, ld, lds, Y, B(n + 1, 1));
+            cp_out(nb, ld, lds, S22, B(n + 1, 2));
             if (threadIdx.x == 0) info[part] = bad;
         }
     }
@@ -862,8 +904,9 @@ struct PcFrame {
 // x = diag(1/sc) M^-1 diag(sc) b for all partitions: one CTA (256 threads; 8 lanes per group, two
 // rows per group) per partition, or per direction of a partition (TW).  The factor blocks of the
 // next planes stream into an NBUF-deep shared ring (cp.async.bulk with an mbarrier) while the
-// current plane is swept.  NJ = ld / 8: each lane's columns lane + 8j, j < NJ, are a fixed, fully
-// unrolled batch of loads (padding columns hold zeros).
+// current plane is swept.  NJ = ld / 16: lane l reads the column pairs (2l + 16j, 2l + 16j + 1),
+// j < NJ, of a block row and of the solution plane with 16-byte loads (8-byte for FP32 blocks),
+// a fixed, fully unrolled batch; padding columns hold zeros.
 // Stages of one CTA (local frame):
 //   F(t), t = 1..n-1:   z_t = b_t - L1_t z_{t-1} - L2_t z_{t-2}                  (slots 0, 1)
 //   TW only:
@@ -883,7 +926,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
                                                          double* __restrict__ x, int* __restrict__ err, PaFuse F) {
     extern __shared__ __align__(128) double dsm[];
     __shared__ __align__(8) uint64_t bars[NBUF];
-    constexpr int LD = NJ * PA_LANES;
+    constexpr int LD = NJ * 2 * PA_LANES;
     const int rank = TW ? (int)(blockIdx.x & 1u) : 0;
     const int part = TW ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
     const PcGeom g = pc_part(gin, part);
@@ -968,14 +1011,19 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
     int bi = 0, pb = NBUF - 1;                 // this stage's ring buffer, the previous stage's
     uint32_t par = 0;
     // one block times one solution plane for both rows of the group (the vector loads are shared)
+    using TS2 = typename std::conditional<std::is_same<TS, float>::value, float2, double2>::type;
     auto dot2 = [&](const TS* M, const double* v, double& acc0, double& acc1) {
-        const TS* ma = M + r0 * LD;
-        const TS* mb = M + (act1 ? r1 : r0) * LD;
+        const TS2* ma = reinterpret_cast<const TS2*>(M + r0 * LD) + lane;
+        const TS2* mb = reinterpret_cast<const TS2*>(M + (act1 ? r1 : r0) * LD) + lane;
+        const double2* vp = reinterpret_cast<const double2*>(v) + lane;
 #pragma unroll
         for (int j = 0; j < NJ; ++j) {
-            const double vv = v[lane + PA_LANES * j];
-            acc0 += (double)ma[lane + PA_LANES * j] * vv;
-            acc1 += (double)mb[lane + PA_LANES * j] * vv;
+            const double2 vv = vp[PA_LANES * j];
+            const TS2 a = ma[PA_LANES * j], c = mb[PA_LANES * j];
+            acc0 += (double)a.x * vv.x;
+            acc1 += (double)c.x * vv.x;
+            acc0 += (double)a.y * vv.y;
+            acc1 += (double)c.y * vv.y;
         }
     };
     auto reduce = [&](double& acc0, double& acc1) {
@@ -1296,20 +1344,21 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
     dim3 grid((unsigned)((m->nc + 127) / 128), DV_NSLOT);
     DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_scatter<<<grid, 128, 0, s>>>(g, J, dh, m->d_pc));
     const int optin = smem_optin();
-    const size_t n2b = (size_t)g.nb * g.ld * sizeof(double);
-    const bool factor_smem = g.nb <= PC_SMEM_NB && 9 * n2b + 2048 <= (size_t)optin;
+    const size_t budget = (size_t)optin - 2048;             // static shared memory of the kernel
+    const int lds = pc_lds(g.nb, budget);
+    const size_t dyn = (size_t)9 * g.nb * lds * sizeof(double);
+    const bool factor_smem = g.nb <= PC_SMEM_NB && dyn <= budget;
     g.zs = pc_twist_zs(g, pc_tsize(m), factor_smem);
     if (factor_smem && g.zs > 0) {
-        size_t dyn = 9 * n2b;
         if (dyn > 48 * 1024)
             DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
         DV_LAUNCH(dv::K_PC_FACTOR, s,
-                  DV_CUDA(launch_pair(k_pc_factor_smem<true>, 2u * g.nparts, 256u, dyn, s, g, m->d_pc, m->d_pc_info)));
+                  DV_CUDA(launch_pair(k_pc_factor_smem<true>, 2u * g.nparts, 256u, dyn, s, g, m->d_pc, m->d_pc_info,
+                                      lds)));
     } else if (factor_smem) {
-        size_t dyn = 9 * n2b;
         if (dyn > 48 * 1024)
             DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_smem<false><<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_info));
+        DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_smem<false><<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_info, lds));
     } else {
         const size_t static_smem = (2 * 1024 + 256) * sizeof(double) + 256 * sizeof(int);
         size_t need = (size_t)2 * g.nb * g.nb * sizeof(double);
@@ -1376,11 +1425,11 @@ static void launch_apply_nj(const PcGeom& g, dv_model* m, const double* b, const
 
 static void launch_apply(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
                          const PaFuse& F, bool count) {
-    switch (g.ld / PA_LANES) {
+    switch (g.ld / (2 * PA_LANES)) {
         case 1: launch_apply_nj<1>(g, m, b, sc, x, s, F, count); break;
+        case 2: launch_apply_nj<2>(g, m, b, sc, x, s, F, count); break;
         case 3: launch_apply_nj<3>(g, m, b, sc, x, s, F, count); break;
-        case 5: launch_apply_nj<5>(g, m, b, sc, x, s, F, count); break;
-        default: launch_apply_nj<7>(g, m, b, sc, x, s, F, count); break;
+        default: launch_apply_nj<4>(g, m, b, sc, x, s, F, count); break;
     }
 }
 
@@ -1404,8 +1453,7 @@ int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cud
 }
 
 static bool apply_fusable(const PcGeom& g, size_t tsize) {
-    const int nj = g.ld / PA_LANES;
-    return g.nb <= 64 && apply_smem(g, 2, tsize) <= (size_t)smem_optin() && (nj == 1 || nj == 3 || nj == 5 || nj == 7);
+    return g.nb <= 64 && g.ld % (2 * PA_LANES) == 0 && apply_smem(g, 2, tsize) <= (size_t)smem_optin();
 }
 
 bool precond_apply_fusable(dv_model* m) { return apply_fusable(geom_factored(m), pc_tsize(m)); }

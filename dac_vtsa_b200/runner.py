@@ -11,6 +11,9 @@ at step start) are read back.
 """
 from __future__ import annotations
 
+import gzip
+import json
+import os
 import time
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
@@ -238,13 +241,15 @@ def main(argv=None):
     (steps/_runner.py:244): ``python -m dac_vtsa_b200.runner --grid 8 8 32 --step adsorption
     --duration 600``."""
     import argparse
-    import json
     from .config import load_config
     ap = argparse.ArgumentParser(description=main.__doc__)
     ap.add_argument("--grid", type=int, nargs=3, default=(8, 8, 32), metavar=("NR", "NTHETA", "NZ"))
     ap.add_argument("--step", default="adsorption", help="name of a step of the configured cycle")
     ap.add_argument("--duration", type=float, default=None, help="bed-seconds to integrate (default: whole step)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--trace", default=None, metavar="FILE",
+                    help="integrate once untraced, then again under a CUDA activity trace (torch.profiler) "
+                         "written to FILE (gzipped Chrome JSON); adds the GPU timeline summary to the output")
     a = ap.parse_args(argv)
     over = dict(BENCH_POINT, **{"grid.Nr": a.grid[0], "grid.Ntheta": a.grid[1], "grid.Nz": a.grid[2]})
     cfg = load_config(override_dict=over)
@@ -257,17 +262,69 @@ def main(argv=None):
     step = dict(steps[a.step])
     full = float(step["duration"])
     dur = full if a.duration is None else min(a.duration, full)
-    model = TVSAModel(cfg, grid, props, step, st)
-    integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * full)
-    y0 = torch.from_numpy(model.pack(st)).to(model.device)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res = integ.integrate(y0, dur, np.array([dur]), keep_on_device=True)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    print(json.dumps({"grid": list(a.grid), "step": a.step, "bed_s": res.t, "wall_s": wall,
-                      "bed_s_per_wall_s": res.t / wall, "steps": res.n_steps, "rejected": res.n_reject,
-                      "jac": res.n_jac, "lu": res.n_lu, "nfev": res.nfev, **integ.stats}))
+    def once():
+        model = TVSAModel(cfg, grid, props, step, st)
+        integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * full)
+        y0 = torch.from_numpy(model.pack(st)).to(model.device)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = integ.integrate(y0, dur, np.array([dur]), keep_on_device=True)
+        torch.cuda.synchronize()
+        return res, integ, time.perf_counter() - t0
+
+    res, integ, wall = once()
+    out = {"grid": list(a.grid), "step": a.step, "bed_s": res.t, "wall_s": wall, "bed_s_per_wall_s": res.t / wall,
+           "steps": res.n_steps, "rejected": res.n_reject, "jac": res.n_jac, "lu": res.n_lu, "nfev": res.nfev,
+           **integ.stats}
+    if a.trace:
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CPU, ProfilerActivity.CUDA]) as prof:
+            _, _, wall_t = once()
+        tmp = a.trace + ".tmp.json"
+        prof.export_chrome_trace(tmp)
+        with open(tmp, "rb") as f:
+            events = json.load(f)["traceEvents"]
+        with open(tmp, "rb") as f, gzip.open(a.trace, "wb") as g:
+            g.write(f.read())
+        os.remove(tmp)
+        out["trace"] = dict(timeline_summary(events), wall_s_traced=wall_t, file=a.trace)
+    print(json.dumps(out))
+
+
+def timeline_summary(events, top=8):
+    """GPU busy fraction and idle gaps of a CUDA activity trace (Chrome trace events), counted from
+    the first preconditioner sweep (model setup excluded): total kernel time, the idle time between
+    consecutive device activities by the pair of kernels around it, and the kernels by total time."""
+    acts = sorted((e for e in events if e.get("cat") in ("kernel", "gpu_memcpy", "gpu_memset")),
+                  key=lambda e: e["ts"])
+
+    def name(e):
+        if e.get("cat") != "kernel":
+            return e["cat"] + ":" + e["name"].split(" (")[0]
+        return e["name"].split("(")[0].replace("void ", "").replace("dv::", "")
+
+    start = next((e["ts"] for e in acts if "k_pc_apply" in e["name"]), acts[0]["ts"] if acts else 0.0)
+    acts = [e for e in acts if e["ts"] >= start]
+    if not acts:
+        return {}
+    span = acts[-1]["ts"] + acts[-1]["dur"] - start
+    busy = sum(e["dur"] for e in acts if e.get("cat") == "kernel")
+    gaps, per_kernel = {}, {}
+    for e0, e1 in zip(acts, acts[1:]):
+        gap = e1["ts"] - (e0["ts"] + e0["dur"])
+        if gap > 5.0:
+            key = name(e0) + " -> " + name(e1)
+            n, t = gaps.get(key, (0, 0.0))
+            gaps[key] = (n + 1, t + gap)
+    for e in acts:
+        if e.get("cat") == "kernel":
+            n, t = per_kernel.get(name(e), (0, 0.0))
+            per_kernel[name(e)] = (n + 1, t + e["dur"])
+    by_t = lambda d: sorted(d.items(), key=lambda kv: -kv[1][1])[:top]
+    return {"span_us": span, "kernel_us": busy, "busy_fraction": busy / span,
+            "idle_gaps_over_5us": [{"between": k, "count": n, "total_us": round(t)} for k, (n, t) in by_t(gaps)],
+            "kernels": [{"kernel": k, "count": n, "total_us": round(t), "avg_us": round(t / n, 2)}
+                        for k, (n, t) in by_t(per_kernel)]}
 
 
 if __name__ == "__main__":
