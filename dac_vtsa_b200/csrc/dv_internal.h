@@ -53,6 +53,7 @@ struct Work {
     cudaGraphExec_t gm_exec = nullptr;
     cudaStream_t gm_cs = nullptr;             // capture stream
     int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1;
+    int gm_prefix = 0;                        // Arnoldi steps captured ahead of the WHILE node
     int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
@@ -132,6 +133,7 @@ struct PaFuse {
     unsigned* ticket = nullptr;
     double* out = nullptr;
     int64_t n = 0;
+    const int* stop = nullptr;        // when *stop != 0 at launch: write *out = 0 and do nothing else
 };
 bool precond_apply_fusable(dv_model* m);
 // The same launches without launch accounting or attribute changes, for stream capture (the

@@ -924,6 +924,10 @@ template <int NJ, int NBUF, typename TS, bool TW>
 __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
                                                          double* __restrict__ x, int* __restrict__ err, PaFuse F) {
+    if (F.stop && *F.stop) {                   // an Arnoldi step after the solve stopped: a zero direction
+        if (blockIdx.x == 0 && threadIdx.x == 0 && F.out) *F.out = 0.0;
+        return;                                // (every CTA of the grid returns here: no barrier is left open)
+    }
     extern __shared__ __align__(128) double dsm[];
     __shared__ __align__(8) uint64_t bars[NBUF];
     constexpr int LD = NJ * 2 * PA_LANES;

@@ -767,6 +767,7 @@ __global__ void k_gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, 
 // Block sums of the first cnt entries of acc (VB threads) into part[blockIdx.x * GM_PS + q];
 // returns true in the block that finished last (after the other blocks' partials are visible).
 constexpr int GM_PS = GM_KMAX + 2;      // partial stride per block
+constexpr int GM_PREFIX = 4;            // Arnoldi steps of the GMRES graph ahead of its WHILE node
 __device__ __forceinline__ bool gm_block_partials(const double (&acc)[GM_KMAX + 1], int cnt, double* part,
                                                   unsigned* ticket) {
     __shared__ double sm[VB / 32][GM_PS];
@@ -810,6 +811,7 @@ __device__ __forceinline__ void gm_finish_partials(const double* part, int cnt, 
 __global__ void __launch_bounds__(VB) k_cgs_dots(int64_t n, const GmDev* __restrict__ st, const double* __restrict__ V,
                                                  int64_t ldv, const double* __restrict__ w, double* __restrict__ part,
                                                  unsigned* ticket, double* __restrict__ out) {
+    if (st->done) return;                  // a step after the solve stopped
     const int m = st->col + 1;
     double acc[GM_KMAX + 1];
 #pragma unroll
@@ -831,6 +833,7 @@ __global__ void __launch_bounds__(VB) k_cgs_orth_dots(int64_t n, const GmDev* __
                                                       const double* __restrict__ h, double* __restrict__ w,
                                                       double* __restrict__ part, unsigned* ticket,
                                                       double* __restrict__ out) {
+    if (st->done) return;                  // a step after the solve stopped
     const int m = st->col + 1;
     double acc[GM_KMAX + 1];
 #pragma unroll
@@ -852,6 +855,7 @@ __global__ void __launch_bounds__(VB) k_cgs_orth_norm(int64_t n, GmDev* st, cons
                                                       double* __restrict__ hh, double* __restrict__ w,
                                                       double* __restrict__ part, unsigned* ticket, int kdim,
                                                       cudaGraphConditionalHandle hnd) {
+    if (st->done) return;                  // a step after the solve stopped
     const int m = st->col + 1;
     const double* h2 = hh + (kdim + 2);
     double acc[GM_KMAX + 1];
@@ -923,6 +927,19 @@ struct GmHost {
     int res[6];                   // col, done, skip, iters, info, ncomb
 };
 
+// Arnoldi steps captured ahead of the WHILE node: GM_PREFIX, or DVTSA_GMRES_PREFIX=<0..8> from the
+// environment (read once per process; a tuning knob: more steps save WHILE relaunches of long
+// solves, but lengthen every graph launch on the host and run empty steps in short solves)
+static int gmres_prefix() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("DVTSA_GMRES_PREFIX");
+        v = GM_PREFIX;
+        if (e && e[0] >= '0' && e[0] <= '8' && e[1] == 0) v = e[0] - '0';
+    }
+    return v;
+}
+
 static int gm_build(dv_model* m, Work& W, int kdim) {
     if (W.gm_exec) { cudaGraphExecDestroy(W.gm_exec); W.gm_exec = nullptr; }
     if (W.gm_graph) { cudaGraphDestroy(W.gm_graph); W.gm_graph = nullptr; }
@@ -949,7 +966,42 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 9);
         k_gm_init<<<1, VB, 0, cs>>>(st, W.scal, kdim, hnd);
         fixed[K_VECTOR] += 3;
-        e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &ndeps);
+    }
+    const bool fused = precond_apply_fusable(m);
+    // One Arnoldi step of the fused form: sweep with normalisation prologue and rms epilogue,
+    // matvec, CGS2 in three kernels; every kernel returns at once when st->done is set.
+    auto arnoldi_step = [&](cudaStream_t c) -> int {
+        PaFuse F;
+        F.col = &st->col;
+        F.scale = &st->scale;
+        F.src0 = W.b;
+        F.src1 = W.wout;
+        F.V = W.V;
+        F.ldv = ldv;
+        F.part = W.apart;
+        F.ticket = W.tickets + 0;
+        F.out = W.scal + 0;
+        F.n = n;
+        F.stop = &st->done;
+        int rc = precond_apply_capture(m, W.vin, W.s, W.u, c, F);
+        if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, c);
+        k_cgs_dots<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.wout, W.part, W.tickets + 1, W.hbuf);
+        k_cgs_orth_dots<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 2, W.hbuf + (kdim + 2));
+        k_cgs_orth_norm<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 3, kdim, hnd);
+        return rc;
+    };
+    // The first GM_PREFIX steps are plain nodes ahead of the WHILE node: every solve takes at least
+    // two steps and most take five or more, and each pass through the WHILE body costs a device-side
+    // relaunch (~20 us on B200) that a plain node does not; a step after the stop returns at once.
+    const int prefix = fused ? std::min(gmres_prefix(), kdim) : 0;
+    if (e == cudaSuccess) {
+        for (int q = 0; q < prefix && e == cudaSuccess; ++q) {
+            if (arnoldi_step(cs) != DV_OK) e = cudaErrorUnknown;
+            fixed[K_PC_APPLY] += 1;
+            fixed[K_MATVEC] += 3;
+            fixed[K_VECTOR] += 3;
+        }
+        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &ndeps);
     }
     cudaGraphNode_t cnode = nullptr;
     cudaGraph_t body = nullptr;
@@ -963,30 +1015,13 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
     }
     if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(body_cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
-    const bool fused = precond_apply_fusable(m);
     if (e == cudaSuccess) {
         // body: one Arnoldi step
         int rc = DV_OK;
-        if (fused) {        // sweep with normalisation prologue and rms epilogue; CGS2 in three kernels
-            PaFuse F;
-            F.col = &st->col;
-            F.scale = &st->scale;
-            F.src0 = W.b;
-            F.src1 = W.wout;
-            F.V = W.V;
-            F.ldv = ldv;
-            F.part = W.apart;
-            F.ticket = W.tickets + 0;
-            F.out = W.scal + 0;
-            F.n = n;
-            rc = precond_apply_capture(m, W.vin, W.s, W.u, body_cs, F);
+        if (fused) {
+            rc = arnoldi_step(body_cs);
             iter[K_PC_APPLY] += 1;
-            if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, body_cs);
             iter[K_MATVEC] += 3;
-            k_cgs_dots<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.wout, W.part, W.tickets + 1, W.hbuf);
-            k_cgs_orth_dots<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 2,
-                                                   W.hbuf + (kdim + 2));
-            k_cgs_orth_norm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 3, kdim, hnd);
             iter[K_VECTOR] += 3;
         } else {
             k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
@@ -1059,6 +1094,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     W.gm_nb = m->pc_nb;
     W.gm_nparts = m->pc_nparts;
     W.gm_zs = m->pc_zs;
+    W.gm_prefix = prefix;
     W.gm_fp32 = m->pc_fp32;
     for (int k = 0; k < K_NKIND; ++k) {
         W.gm_fixed[k] = fixed[k];
@@ -1094,7 +1130,8 @@ static int gmres_graph_collect(Work& W, dv_model* m, int* info, int64_t* inner) 
     *info = hst->res[4];
     *inner += iters;
     m->nfev += iters + (skip ? 0 : 1);
-    for (int k = 0; k < K_NKIND; ++k) count_launches(k, W.gm_fixed[k] + W.gm_iter[k] * iters);
+    const int looped = std::max(iters - W.gm_prefix, 0);      // passes through the WHILE body
+    for (int k = 0; k < K_NKIND; ++k) count_launches(k, W.gm_fixed[k] + W.gm_iter[k] * looped);
     if (g_prof_on && !g_pending.empty()) prof_flush();
     return check_device_error(m);
 }
