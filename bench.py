@@ -378,10 +378,6 @@ def gpu_arm(a, rank, world, local_rank):
                 "alg_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
                 "alg_bytes_rule": ALG_BYTES_DOC.get(dom, ""),
                 "kernel_share": {k: round(v[2] / sum(x[2] for x in kinds.values()), 4) for k, v in kinds.items()},
-                # device time of the profiled cycle summed over its timed launches (each bracketed by
-                # events, so it slightly overstates); the rest of ms_per_step is host work and gaps
-                "kernel_ms_per_cycle": round(sum(x[2] for x in kinds.values()), 1),
-                "timed_launches": int(sum(x[1] for x in kinds.values())),
                 "launches_per_cycle": int(sum(x[0] for x in kinds.values())),
                 "kernel_avg_us": {k: round(1e3 * v[2] / v[1], 3) for k, v in kinds.items()}}
     cpu = None

@@ -57,6 +57,16 @@ struct Work {
     int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
+
+#ifdef __CUDACC__
+// sum of p[b * stride], b < nb, in index order: the deterministic finish of per-block partials
+// written by other SMs (volatile loads: never served from this SM's L1)
+__device__ __forceinline__ double sum_partials(const double* p, int nb, int64_t stride) {
+    double t = 0.0;
+    for (int b = 0; b < nb; ++b) t += ((volatile const double*)p)[(int64_t)b * stride];
+    return t;
+}
+#endif
 void work_free(Work& W);
 
 struct DevAux {

@@ -1186,9 +1186,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         __syncthreads();
         if (last && tid == 0) {
             __threadfence();
-            double t = 0.0;
-            for (int c = 0; c < (int)gridDim.x; ++c) t += ((volatile double*)F.part)[c];
-            *F.out = sqrt(t / (double)F.n);
+            *F.out = sqrt(sum_partials(F.part, (int)gridDim.x, 1) / (double)F.n);
             *F.ticket = 0u;
         }
     }

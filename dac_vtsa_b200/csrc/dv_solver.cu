@@ -303,9 +303,7 @@ __global__ void __launch_bounds__(VB) k_cons(dv_step_params p, const double* __r
     __syncthreads();
     if (last && threadIdx.x < 8) {
         __threadfence();
-        double t = 0.0;
-        for (int b = 0; b < (int)gridDim.x; ++b) t += ((volatile const double*)part)[(int64_t)b * 8 + threadIdx.x];
-        out[threadIdx.x] = t;
+        out[threadIdx.x] = sum_partials(part + threadIdx.x, (int)gridDim.x, 8);
     }
     if (last && threadIdx.x == 0) *ticket = 0u;
 }
@@ -626,7 +624,12 @@ __device__ void lartg_d(double f, double g, double& c, double& s, double& r) {
     }
 }
 
-__global__ void k_gm_init(GmDev* st, const double* __restrict__ scal, int kdim, cudaGraphConditionalHandle hnd) {
+__global__ void k_gm_init(GmDev* st, const double* __restrict__ scal, int kdim, cudaGraphConditionalHandle hnd,
+                          unsigned* bar) {
+    if (threadIdx.x == 0 && bar) {              // barrier words of k_cgs_fused: no arrivals pending
+        bar[0] = 0u;
+        bar[2] = 0u;
+    }
     for (int q = threadIdx.x; q < kdim * (kdim + 1); q += blockDim.x) st->H[q] = 0.0;
     for (int q = threadIdx.x; q <= kdim; q += blockDim.x) st->S[q] = 0.0;
     __syncthreads();
@@ -799,10 +802,7 @@ __device__ __forceinline__ bool gm_block_partials(const double (&acc)[GM_KMAX + 
 // out[q] = sum over blocks of part[.. q], q < cnt, in block order (called by the last block)
 __device__ __forceinline__ void gm_finish_partials(const double* part, int cnt, double* out, unsigned* ticket) {
     if ((int)threadIdx.x < cnt) {
-        double t = 0.0;
-        for (int b2 = 0; b2 < (int)gridDim.x; ++b2)
-            t += ((volatile const double*)part)[(int64_t)b2 * GM_PS + threadIdx.x];
-        out[threadIdx.x] = t;
+        out[threadIdx.x] = sum_partials(part + threadIdx.x, (int)gridDim.x, GM_PS);
     }
     if (threadIdx.x == 0) *ticket = 0u;
 }
@@ -869,12 +869,139 @@ __global__ void __launch_bounds__(VB) k_cgs_orth_norm(int64_t n, GmDev* st, cons
     }
     if (gm_block_partials(acc, 1, part, ticket)) {
         if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (int b2 = 0; b2 < (int)gridDim.x; ++b2) t += ((volatile const double*)part)[(int64_t)b2 * GM_PS];
-            hh[2 * (kdim + 2)] = sqrt(t);
+            hh[2 * (kdim + 2)] = sqrt(sum_partials(part, (int)gridDim.x, GM_PS));
             *ticket = 0u;
             gm_givens(st, hh, kdim, hnd);
         }
+    }
+}
+
+// ---- CGS2 of one Arnoldi step in a single cooperative launch
+// Barrier of a cooperative launch (all blocks co-resident): arrival counter + generation word in
+// global memory.  The wait is bounded: after ~2^24 polls the kernel records bit 4 in *err and
+// carries on (the step's results are then void, and the host sees the error).
+__device__ __forceinline__ void grid_sync_bounded(unsigned* cnt, unsigned* gen, int* err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vg = gen;
+        const unsigned g0 = *vg;
+        __threadfence();
+        if (atomicAdd(cnt, 1u) == gridDim.x - 1) {
+            *cnt = 0u;
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            for (int it = 0; *vg == g0; ++it) {
+                if (it > (1 << 24)) {
+                    atomicOr(err, 4);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// this block's sums of the first cnt entries of acc into part[blockIdx.x * GM_PS + q]
+__device__ __forceinline__ void gm_store_partials(const double (&acc)[GM_KMAX + 1], int cnt, double* part) {
+    __shared__ double sm[VB / 32][GM_PS];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q <= GM_KMAX; ++q) {
+        if (q < cnt) {
+            double v = acc[q];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if (lane == 0) sm[wid][q] = v;
+        }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < cnt) {
+        double t = 0.0;
+        for (int w2 = 0; w2 < VB / 32; ++w2) t += sm[w2][threadIdx.x];
+        part[(int64_t)blockIdx.x * GM_PS + threadIdx.x] = t;
+    }
+}
+
+// k_cgs_dots + k_cgs_orth_dots + k_cgs_orth_norm in one launch, with the same block partition and
+// the same summation order (so the same results): the two global sums between the passes are
+// grid barriers instead of kernel boundaries, and every block sums the partials itself in block
+// order.  Each pass has its own partials (a fast block never overwrites what a slow one reads).
+// hh receives h (pass 1, with w.w at hh[m]), h2 (pass 2) and ||w|| (pass 3); the last block of
+// pass 3 runs the Givens update and the stopping test.  bar: [0] arrivals, [1] generation,
+// [2] pass-3 ticket.
+__global__ void __launch_bounds__(VB) k_cgs_fused(int64_t n, GmDev* st, const double* __restrict__ V, int64_t ldv,
+                                                  double* __restrict__ hh, double* __restrict__ w,
+                                                  double* __restrict__ part, unsigned* bar, int kdim,
+                                                  cudaGraphConditionalHandle hnd, int* err) {
+    if (st->done) return;                  // a step after the solve stopped (uniform over the grid)
+    const int m = st->col + 1;
+    __shared__ double hs[GM_KMAX + 1];
+    __shared__ bool last;
+    const int64_t pstride = (int64_t)gridDim.x * GM_PS;
+    double* part1 = part;
+    double* part2 = part + pstride;
+    double* part3 = part + 2 * pstride;
+    double acc[GM_KMAX + 1];
+    // pass 1: V_q . w (q < m) and w . w
+#pragma unroll
+    for (int q = 0; q <= GM_KMAX; ++q) acc[q] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double wi = w[i];
+#pragma unroll
+        for (int q = 0; q <= GM_KMAX; ++q) {
+            if (q < m) acc[q] += V[q * ldv + i] * wi;
+            else if (q == m) acc[q] += wi * wi;
+        }
+    }
+    gm_store_partials(acc, m + 1, part1);
+    grid_sync_bounded(bar, bar + 1, err);
+    if ((int)threadIdx.x <= m) {
+        const double t = sum_partials(part1 + threadIdx.x, (int)gridDim.x, GM_PS);
+        hs[threadIdx.x] = t;
+        if (blockIdx.x == 0) hh[threadIdx.x] = t;
+    }
+    __syncthreads();
+    // pass 2: w -= sum_q h[q] V_q, then V_q . w
+#pragma unroll
+    for (int q = 0; q <= GM_KMAX; ++q) acc[q] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double o = 0.0;
+        for (int q = 0; q < m; ++q) o += hs[q] * V[q * ldv + i];
+        const double wi = w[i] - o;
+        w[i] = wi;
+#pragma unroll
+        for (int q = 0; q < GM_KMAX; ++q)
+            if (q < m) acc[q] += V[q * ldv + i] * wi;
+    }
+    gm_store_partials(acc, m, part2);
+    grid_sync_bounded(bar, bar + 1, err);
+    if ((int)threadIdx.x < m) {
+        const double t = sum_partials(part2 + threadIdx.x, (int)gridDim.x, GM_PS);
+        hs[threadIdx.x] = t;
+        if (blockIdx.x == 0) hh[(kdim + 2) + threadIdx.x] = t;
+    }
+    __syncthreads();
+    // pass 3: w -= sum_q h2[q] V_q, ||w||
+    acc[0] = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double o = 0.0;
+        for (int q = 0; q < m; ++q) o += hs[q] * V[q * ldv + i];
+        const double wi = w[i] - o;
+        w[i] = wi;
+        acc[0] += wi * wi;
+    }
+    gm_store_partials(acc, 1, part3);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(bar + 2, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        hh[2 * (kdim + 2)] = sqrt(sum_partials(part3, (int)gridDim.x, GM_PS));
+        bar[2] = 0u;
+        gm_givens(st, hh, kdim, hnd);
     }
 }
 
@@ -940,6 +1067,16 @@ static int gmres_prefix() {
     return v;
 }
 
+// DVTSA_GMRES_COOP=0 keeps the three-kernel CGS2 in the GMRES graph (read once per process)
+static bool gmres_coop_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("DVTSA_GMRES_COOP");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 static int gm_build(dv_model* m, Work& W, int kdim) {
     if (W.gm_exec) { cudaGraphExecDestroy(W.gm_exec); W.gm_exec = nullptr; }
     if (W.gm_graph) { cudaGraphDestroy(W.gm_graph); W.gm_graph = nullptr; }
@@ -964,10 +1101,18 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         // pre: ||b||, loop state
         k_sumsq<<<g, VB, 0, cs>>>(n, W.b, nullptr, W.part);
         k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 9);
-        k_gm_init<<<1, VB, 0, cs>>>(st, W.scal, kdim, hnd);
+        k_gm_init<<<1, VB, 0, cs>>>(st, W.scal, kdim, hnd, W.tickets + 8);
         fixed[K_VECTOR] += 3;
     }
     const bool fused = precond_apply_fusable(m);
+    // the cooperative CGS2 kernel takes at most one block per SM (all of them must be resident)
+    static bool coop_ok = true;               // cleared if the driver refuses a cooperative node
+    int nsm = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const unsigned gc = std::min<unsigned>(g, (unsigned)std::max(nsm, 1));
+    const bool coop = coop_ok && gmres_coop_enabled();
+    bool coop_failed = false;
     // One Arnoldi step of the fused form: sweep with normalisation prologue and rms epilogue,
     // matvec, CGS2 in three kernels; every kernel returns at once when st->done is set.
     auto arnoldi_step = [&](cudaStream_t c) -> int {
@@ -985,11 +1130,28 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         F.stop = &st->done;
         int rc = precond_apply_capture(m, W.vin, W.s, W.u, c, F);
         if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, c);
-        k_cgs_dots<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.wout, W.part, W.tickets + 1, W.hbuf);
-        k_cgs_orth_dots<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 2, W.hbuf + (kdim + 2));
-        k_cgs_orth_norm<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 3, kdim, hnd);
+        if (coop) {                          // CGS2 as one cooperative launch (co-resident blocks)
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(gc);
+            cfg.blockDim = dim3(VB);
+            cfg.stream = c;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeCooperative;
+            at[0].val.cooperative = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            if (cudaLaunchKernelEx(&cfg, k_cgs_fused, n, st, (const double*)W.V, ldv, W.hbuf, W.wout, W.part,
+                                   W.tickets + 8, kdim, hnd, m->d_err) != cudaSuccess)
+                coop_failed = true;
+        } else {
+            k_cgs_dots<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.wout, W.part, W.tickets + 1, W.hbuf);
+            k_cgs_orth_dots<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 2,
+                                             W.hbuf + (kdim + 2));
+            k_cgs_orth_norm<<<g, VB, 0, c>>>(n, st, W.V, ldv, W.hbuf, W.wout, W.part, W.tickets + 3, kdim, hnd);
+        }
         return rc;
     };
+    const int ncgs = coop ? 1 : 3;           // launches of the CGS2 part of a step
     // The first GM_PREFIX steps are plain nodes ahead of the WHILE node: every solve takes at least
     // two steps and most take five or more, and each pass through the WHILE body costs a device-side
     // relaunch (~20 us on B200) that a plain node does not; a step after the stop returns at once.
@@ -999,7 +1161,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
             if (arnoldi_step(cs) != DV_OK) e = cudaErrorUnknown;
             fixed[K_PC_APPLY] += 1;
             fixed[K_MATVEC] += 3;
-            fixed[K_VECTOR] += 3;
+            fixed[K_VECTOR] += ncgs;
         }
         if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &ndeps);
     }
@@ -1022,7 +1184,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
             rc = arnoldi_step(body_cs);
             iter[K_PC_APPLY] += 1;
             iter[K_MATVEC] += 3;
-            iter[K_VECTOR] += 3;
+            iter[K_VECTOR] += ncgs;
         } else {
             k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
             iter[K_VECTOR] += 1;
@@ -1082,6 +1244,12 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     cudaError_t e3 = cudaStreamEndCapture(cs, &graph);     // always end the capture
     if (e == cudaSuccess) e = e3;
     cudaStreamDestroy(body_cs);
+    if (coop_failed) {                        // build again with the three-kernel CGS2
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        coop_ok = false;
+        return gm_build(m, W, kdim);
+    }
     if (e != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
