@@ -279,3 +279,41 @@ def test_mixed_precision_adsorption_stays_within_solver_tolerance():
     err = np.sqrt(np.mean(((r32.y - r64.y) / sc) ** 2))
     assert err < 1.0, err
     assert abs(r32.n_steps - r64.n_steps) <= max(5, 0.15 * r64.n_steps), (r32.n_steps, r64.n_steps)
+
+
+_GRAPH_FORM_RUN = r"""
+import hashlib, json, sys
+import numpy as np
+sys.path.insert(0, {tests!r})
+from cases import golden
+from test_gpu_solver import _c0_model
+from dac_vtsa_b200.model import TVSAModel
+from dac_vtsa_b200.solver import TRBDF2
+d, m, cfg, meta = _c0_model(TVSAModel)
+dur = meta["duration"]
+integ = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur)
+r = integ.integrate(d["s0_y0"], dur, [dur])
+print(json.dumps({{"y": hashlib.sha256(np.ascontiguousarray(r.y).tobytes()).hexdigest(), "steps": r.n_steps,
+                  "gmres": integ.stats["gmres_iters"], "polish": integ.stats["gmres_polish"]}}))
+"""
+
+
+def test_gmres_graph_forms_give_identical_results():
+    """The GMRES graph's Arnoldi steps ahead of its WHILE node (DVTSA_GMRES_PREFIX) and its CGS2 as
+    one cooperative launch (DVTSA_GMRES_COOP) change where the same kernels' arithmetic runs, not
+    the arithmetic: a 200 s adsorption of the 4x4x16 bed ends in the bit-identical state with the
+    same step and GMRES counts in every form."""
+    import os
+    import subprocess
+    import sys
+    tests = os.path.dirname(os.path.abspath(__file__))
+    code = _GRAPH_FORM_RUN.format(tests=tests)
+    out = {}
+    for name, env in {"default": {}, "three_kernel_cgs": {"DVTSA_GMRES_COOP": "0"},
+                      "no_prefix": {"DVTSA_GMRES_PREFIX": "0"}}.items():
+        e = dict(os.environ, **env)
+        r = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True, text=True, timeout=600,
+                           cwd=os.path.dirname(tests))
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[name] = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["default"] == out["three_kernel_cgs"] == out["no_prefix"], out
