@@ -27,16 +27,16 @@ def _partition_of(m, mode):
     return np.zeros_like(idx)
 
 
-def _pc_model(Nz):
-    """3 x 4 x Nz bed and a state: the golden Jacobian state for Nz = 6, else a seeded state."""
+def _pc_model(Nz, Nr=3):
+    """Nr x 4 x Nz bed and a state: the golden Jacobian state for 3 x 4 x 6, else a seeded state."""
     from dac_vtsa_b200.model import TVSAModel
-    if Nz == 6:
+    if Nz == 6 and Nr == 3:
         d = golden("jacobian_3x4x6.npz")
         m, _ = build(TVSAModel, {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6}, 0, d["P0"])
         return m, d["y"]
     from dac_vtsa_b200 import host
     from dac_vtsa_b200.config import load_config
-    cfg = load_config(override_dict={"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": Nz})
+    cfg = load_config(override_dict={"grid.Nr": Nr, "grid.Ntheta": 4, "grid.Nz": Nz})
     g = host.Grid.from_config(cfg)
     props = host.get_backend(cfg)
     st = host.seeded_state(cfg, g, props, seed=3, amplitude=0.05)
@@ -73,7 +73,19 @@ def _dominant_jacobian(m, seed):
 def test_preconditioner_exact_on_dominant_system(mode, Nz):
     """dv_precond_solve == sparse LU solve of I - J restricted to the partition couplings, to
     rounding, on a diagonally dominant J that fills the whole stencil pattern."""
-    m, _ = _pc_model(Nz)
+    _check_dominant(mode, Nz, 3)
+
+
+# 8 rings: sector partitions of nb 49 (ld 64, two-deep ring, shared stride 52), theta_block
+# partitions of nb 43 / 24
+@pytest.mark.parametrize("mode", ["sector", "theta_block"])
+def test_preconditioner_exact_on_dominant_system_8_rings(mode):
+    """The same check on an 8-ring bed, whose sector blocks take the widest shared-memory layout."""
+    _check_dominant(mode, 12, 8)
+
+
+def _check_dominant(mode, Nz, Nr):
+    m, _ = _pc_model(Nz, Nr)
     Jd, Jc = _dominant_jacobian(m, 40 + Nz)
     m.precond_factor(Jd, 1.0, mode)
     M = _restricted(m, Jc, mode, 1.0)
