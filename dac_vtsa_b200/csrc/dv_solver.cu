@@ -178,6 +178,49 @@ __global__ void k_sumsq(int64_t n, const double* __restrict__ a, const double* _
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
+// k_sumsq then k_finish in one launch: the block that finishes last (ticket) sums the partials
+// with k_finish's own strided loop and tree, so the result is the same to the bit
+__global__ void k_sumsq_finish(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                               double* __restrict__ part, unsigned* ticket, int mode, double* __restrict__ out) {
+    __shared__ double sh[VB];
+    __shared__ bool last;
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = b ? a[i] / b[i] : a[i];
+        acc += v * v;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = VB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = sh[0];
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    acc = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) acc += ((volatile const double*)part)[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = VB / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double v = sh[0];
+        if (mode == 0) v = sqrt(v / (double)n);
+        else if (mode == 1) v = fmax(1.0, sqrt(v / (double)n));
+        else if (mode == 2) v = sqrt(v);
+        out[0] = v;
+        *ticket = 0u;
+    }
+}
+
 // out[slot] = mode 0: sqrt(sum/n); 1: max(1, sqrt(sum/n)); 2: sqrt(sum) ; 3: sum
 __global__ void k_finish(int nparts, const double* __restrict__ part, double n, int mode, double* __restrict__ out) {
     __shared__ double sh[VB];
@@ -412,8 +455,7 @@ void work_free(Work& W) {
 // reductions returning host values (synchronise)
 static int rms_ratio_dev(Work& W, int64_t n, const double* a, const double* b, int mode, double* dst, cudaStream_t s) {
     unsigned g = vgrid(n);
-    DV_LAUNCH(dv::K_VECTOR, s, k_sumsq<<<g, VB, 0, s>>>(n, a, b, W.part));
-    DV_LAUNCH(dv::K_VECTOR, s, k_finish<<<1, VB, 0, s>>>((int)g, W.part, (double)n, mode, dst));
+    DV_LAUNCH(dv::K_VECTOR, s, k_sumsq_finish<<<g, VB, 0, s>>>(n, a, b, W.part, W.tickets + 6, mode, dst));
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }
@@ -1099,10 +1141,9 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&hnd, cg, 0, cudaGraphCondAssignDefault);
     if (e == cudaSuccess) {
         // pre: ||b||, loop state
-        k_sumsq<<<g, VB, 0, cs>>>(n, W.b, nullptr, W.part);
-        k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 9);
+        k_sumsq_finish<<<g, VB, 0, cs>>>(n, W.b, nullptr, W.part, W.tickets + 6, 2, W.scal + 9);
         k_gm_init<<<1, VB, 0, cs>>>(st, W.scal, kdim, hnd, W.tickets + 8);
-        fixed[K_VECTOR] += 3;
+        fixed[K_VECTOR] += 2;
     }
     const bool fused = precond_apply_fusable(m);
     // the cooperative CGS2 kernel takes at most one block per SM (all of them must be resident)
@@ -1234,10 +1275,9 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.r, cs);
         fixed[K_MATVEC] += 3;
         k_axpby<<<g, VB, 0, cs>>>(n, 1.0, W.b, -1.0, W.r, W.r);
-        k_sumsq<<<g, VB, 0, cs>>>(n, W.r, nullptr, W.part);
-        k_finish<<<1, VB, 0, cs>>>((int)g, W.part, (double)n, 2, W.scal + 10);
+        k_sumsq_finish<<<g, VB, 0, cs>>>(n, W.r, nullptr, W.part, W.tickets + 6, 2, W.scal + 10);
         k_gm_info<<<1, 32, 0, cs>>>(st, W.scal);
-        fixed[K_VECTOR] += 4;
+        fixed[K_VECTOR] += 3;
         if (rc != DV_OK) e = cudaErrorUnknown;
     }
     cudaGraph_t graph = nullptr;
