@@ -920,6 +920,7 @@ struct PcFrame {
 // Without TW the backward stages run t = Nz-1..0 (couplings beyond the last plane are absent).
 #define PA_THREADS 256
 #define PA_LANES 8
+#define PA_IO 8            // entries per thread whose loads the prologue / epilogue batch
 template <int NJ, int NBUF, typename TS, bool TW>
 __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
@@ -987,22 +988,36 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         for (int q = 0; q < NBUF && q < S; ++q) issue(q, smem_u32(buf0 + (int64_t)q * 3 * bs), smem_u32(&bars[q]));
     const int fcol = F.V ? *F.col : 0;
     const double fscale = F.V ? *F.scale : 0.0;
-    const double* fsrc = (fcol == 0) ? F.src0 : F.src1;
-    for (int q = tid; q < Nz * LD; q += blockDim.x) {
-        const int t = q / LD, l = q - t * LD;
-        double v = 0.0;
-        if (l < nb && t < nio) {
-            const int64_t gi = pc_glob(g, part, fr.gp(t), l);
-            double bv;
-            if (F.V) {                           // normalise the basis vector on the way in
-                bv = fscale * fsrc[gi];
-                F.V[(int64_t)fcol * F.ldv + gi] = bv;
-            } else {
-                bv = b[gi];
-            }
-            v = sc ? bv * sc[gi] : bv;
+    const double* __restrict__ src = F.V ? ((fcol == 0) ? F.src0 : F.src1) : b;
+    // b (or the basis vector to normalise) into xs: PA_IO entries per thread at a time, all their
+    // loads issued before the first use
+    for (int q0 = tid; q0 < Nz * LD; q0 += PA_IO * PA_THREADS) {
+        int64_t gi[PA_IO];
+        double bv[PA_IO], sv[PA_IO];
+#pragma unroll
+        for (int u = 0; u < PA_IO; ++u) {
+            const int q = q0 + u * PA_THREADS;
+            const int t = q / LD, l = q - t * LD;
+            const bool in = q < Nz * LD && l < nb && t < nio;
+            gi[u] = in ? pc_glob(g, part, fr.gp(t), l) : -1;
+            bv[u] = in ? src[gi[u]] : 0.0;
+            sv[u] = (in && sc) ? sc[gi[u]] : 1.0;
         }
-        xs[q] = v;
+#pragma unroll
+        for (int u = 0; u < PA_IO; ++u) {
+            const int q = q0 + u * PA_THREADS;
+            if (q >= Nz * LD) break;
+            double v = 0.0;
+            if (gi[u] >= 0) {
+                double x0 = bv[u];
+                if (F.V) {                       // normalise the basis vector on the way in
+                    x0 = fscale * x0;
+                    F.V[(int64_t)fcol * F.ldv + gi[u]] = x0;
+                }
+                v = sc ? x0 * sv[u] : x0;
+            }
+            xs[q] = v;
+        }
     }
     for (int q = tid; q < Nz * LD; q += blockDim.x) xb[q] = 0.0;
     __syncthreads();
@@ -1158,13 +1173,24 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         if (tid == 0)
             for (int s2 = s_fail; s2 < issued; ++s2)
                 mbar_wait(smem_u32(&bars[s2 % NBUF]), (uint32_t)((s2 / NBUF) & 1));
-    } else {
-        for (int q = tid; q < Nz * LD; q += blockDim.x) {
-            const int t = q / LD, l = q - t * LD;
-            if (l < nb && t < nio) {
-                const int64_t gi = pc_glob(g, part, fr.gp(t), l);
-                const double xv = sc ? xb[q] / sc[gi] : xb[q];
-                x[gi] = xv;
+    } else {                                     // x out, PA_IO entries per thread at a time
+        for (int q0 = tid; q0 < Nz * LD; q0 += PA_IO * PA_THREADS) {
+            int64_t gi[PA_IO];
+            double sv[PA_IO];
+#pragma unroll
+            for (int u = 0; u < PA_IO; ++u) {
+                const int q = q0 + u * PA_THREADS;
+                const int t = q / LD, l = q - t * LD;
+                const bool in = q < Nz * LD && l < nb && t < nio;
+                gi[u] = in ? pc_glob(g, part, fr.gp(t), l) : -1;
+                sv[u] = (in && sc) ? sc[gi[u]] : 1.0;
+            }
+#pragma unroll
+            for (int u = 0; u < PA_IO; ++u) {
+                if (gi[u] < 0) continue;
+                const int q = q0 + u * PA_THREADS;
+                const double xv = sc ? xb[q] / sv[u] : xb[q];
+                x[gi[u]] = xv;
                 ss += xv * xv;
             }
         }
