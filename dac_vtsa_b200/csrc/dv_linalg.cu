@@ -19,6 +19,11 @@
 // so that both sweeps are one fused GEMV per plane:
 //   forward  z_k = b_k - L1_k z_{k-1} - L2_k z_{k-2}
 //   backward x_k = Uinv_k z_k + (-Uinv_k U1_k) x_{k+1} + (-Uinv_k U2_k) x_{k+2}
+// Twisted form (Nz >= 8, both kernels in shared memory): the same recurrences run top-down over
+// planes 0..zs-1 and, mirrored, bottom-up over planes Nz-1..zs+2 at the same time (a cluster of
+// two CTAs per partition); the separator planes zs, zs+1 (zs = (Nz-2)/2) take the Schur
+// contributions of both sides and are factorised as two more planes.  Half the sequential plane
+// chain of the one-directional form, for the same matrix.
 #include <algorithm>
 #include <type_traits>
 #include "dv_internal.h"
@@ -891,7 +896,8 @@ static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) 
 // Plane frame of one elimination direction.  TW = false: planes 0..Nz-1 top-down (the whole
 // partition).  TW = true (twisted factorisation, a cluster of two CTAs per partition): rank 0
 // eliminates planes 0..zs-1 top-down, rank 1 planes Nz-1..zs+2 bottom-up, and the separator
-// planes zs, zs+1 are solved as one dense 2 nb system.  In its local frame each rank sees planes
+// planes zs, zs+1 take both ranks' contributions and a two-plane block LU of their own.  In its
+// local frame each rank sees planes
 // t = 0, 1, .. (global gp(t)) with slot sl holding the coupling to local plane t + sl - 2, which is
 // global slot gs(sl): bottom-up, A(t, t-1) local is A(p, p+1) global, and so on.  The local
 // eliminated planes are 0..n-1; local n and n+1 are the separator planes.
