@@ -131,6 +131,7 @@ SIGNATURES = [
     ("dv_integrator_y", P, [P]),
     ("dv_integrator_copy_y", C.c_int, [P, P, P]),
     ("dv_rhs_acc_noalloc", C.c_int, [C.POINTER(DvStepParams), P, P, P, D, P, P, P, P]),
+    ("dv_selftest_wait_timeout", C.c_int, [I32, C.POINTER(I32)]),
 ]
 
 _lib = None

@@ -146,6 +146,8 @@ struct PaFuse {
     const int* stop = nullptr;        // when *stop != 0 at launch: write *out = 0 and do nothing else
 };
 bool precond_apply_fusable(dv_model* m);
+// bounded-wait self-test: one sweep-style mbarrier wait that nothing completes (bit 1 of *err)
+int selftest_mbar_timeout(int polls, int* err, cudaStream_t s);
 // The same launches without launch accounting or attribute changes, for stream capture (the
 // attributes are set by an earlier precond_apply).  Returns the number of kernels launched.
 int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,

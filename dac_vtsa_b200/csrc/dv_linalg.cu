@@ -886,11 +886,34 @@ static __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
                  : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
     return ok != 0;
 }
-// bounded wait: false after ~2^22 polls (each poll may itself suspend briefly)
-static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    for (int it = 0; it < (1 << 22); ++it)
+// bounded wait: false after `limit` polls (~2^22 by default; each poll may itself suspend briefly)
+static __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit = 1 << 22) {
+    for (int it = 0; it < limit; ++it)
         if (mbar_try(bar, parity)) return true;
     return false;
+}
+
+// Self-test of the bounded wait: an mbarrier that nothing arrives at, waited on by one warp with
+// `polls` polls; the timeout sets bit 1 of *err exactly as in the sweep, and the kernel returns.
+__global__ void k_selftest_mbar(int polls, int* err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    const bool arrived = mbar_wait(smem_u32(&bar), 0u, polls);
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        if (!arrived) atomicOr(err, 1);
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar)) : "memory");
+    }
+}
+
+int selftest_mbar_timeout(int polls, int* err, cudaStream_t s) {
+    k_selftest_mbar<<<1, 32, 0, s>>>(polls, err);
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
 }
 
 // Plane frame of one elimination direction.  TW = false: planes 0..Nz-1 top-down (the whole

@@ -630,6 +630,14 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
 
 static int check_device_error(dv_model* m);
 
+// the model's device error word: bit 1 a preconditioner sweep's bulk-copy wait timed out, bit 4 a
+// grid barrier of the cooperative Gram-Schmidt kernel timed out
+static const char* device_error_text(int e) {
+    if (e & 1) return "a bounded device wait (preconditioner bulk copy) timed out";
+    if (e & 4) return "a bounded device wait (GMRES grid barrier) timed out";
+    return "a bounded device wait timed out";
+}
+
 // ---------------------------------------------------------------- device-driven GMRES
 // The loop of gmres() above as a CUDA graph: the pre-loop kernels, a conditional WHILE node whose
 // body is one Arnoldi step (normalise the previous basis vector, precondition, FD matvec, two
@@ -922,7 +930,7 @@ __global__ void __launch_bounds__(VB) k_cgs_orth_norm(int64_t n, GmDev* st, cons
 // Barrier of a cooperative launch (all blocks co-resident): arrival counter + generation word in
 // global memory.  The wait is bounded: after ~2^24 polls the kernel records bit 4 in *err and
 // carries on (the step's results are then void, and the host sees the error).
-__device__ __forceinline__ void grid_sync_bounded(unsigned* cnt, unsigned* gen, int* err) {
+__device__ __forceinline__ void grid_sync_bounded(unsigned* cnt, unsigned* gen, int* err, int limit = 1 << 24) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned* vg = gen;
@@ -934,7 +942,7 @@ __device__ __forceinline__ void grid_sync_bounded(unsigned* cnt, unsigned* gen, 
             atomicAdd(gen, 1u);
         } else {
             for (int it = 0; *vg == g0; ++it) {
-                if (it > (1 << 24)) {
+                if (it > limit) {
                     atomicOr(err, 4);
                     break;
                 }
@@ -1047,6 +1055,14 @@ __global__ void __launch_bounds__(VB) k_cgs_fused(int64_t n, GmDev* st, const do
     }
 }
 
+// Self-test of the bounded grid barrier: a cooperative pair of blocks of which block 1 returns
+// without arriving; block 0's wait gives up after `polls` polls and sets bit 4 of *err exactly as
+// in k_cgs_fused, and the kernel returns.
+__global__ void k_selftest_grid(int polls, unsigned* bar, int* err) {
+    if (blockIdx.x != 0) return;
+    grid_sync_bounded(bar, bar + 1, err, polls);
+}
+
 // least squares by back substitution (as in gmres()); ybuf = y, ncomb = its length
 __global__ void k_gm_solve(GmDev* st, double* __restrict__ ybuf, int kdim) {
     if (threadIdx.x != 0) return;
@@ -1094,6 +1110,7 @@ __global__ void k_gm_info(GmDev* st, const double* __restrict__ scal) {
 struct GmHost {
     double args[4];               // t, dh, rtol, atol
     int res[6];                   // col, done, skip, iters, info, ncomb
+    int err;                      // the model's device error word, read back with the results
 };
 
 // Arnoldi steps captured ahead of the WHILE node: GM_PREFIX, or DVTSA_GMRES_PREFIX=<0..8> from the
@@ -1328,6 +1345,7 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
     DV_CUDA(cudaMemcpyAsync(dev, hst->args, sizeof(hst->args), cudaMemcpyHostToDevice, st));
     DV_CUDA(cudaGraphLaunch(W.gm_exec, st));
     DV_CUDA(cudaMemcpyAsync(hst->res, &dev->col, sizeof(hst->res), cudaMemcpyDeviceToHost, st));
+    DV_CUDA(cudaMemcpyAsync(&hst->err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     return DV_OK;
 }
 
@@ -1341,7 +1359,11 @@ static int gmres_graph_collect(Work& W, dv_model* m, int* info, int64_t* inner) 
     const int looped = std::max(iters - W.gm_prefix, 0);      // passes through the WHILE body
     for (int k = 0; k < K_NKIND; ++k) count_launches(k, W.gm_fixed[k] + W.gm_iter[k] * looped);
     if (g_prof_on && !g_pending.empty()) prof_flush();
-    return check_device_error(m);
+    if (hst->err != 0) {                  // (read back with the results: no extra round trip)
+        set_error(device_error_text(hst->err));
+        return DV_ERR_CUDA;
+    }
+    return DV_OK;
 }
 
 // DVTSA_GMRES_GRAPH=0 in the environment runs GMRES host-driven (read once per process; for tools
@@ -1687,7 +1709,7 @@ static int check_device_error(dv_model* m) {
     int e = 0;
     DV_CUDA(cudaMemcpy(&e, m->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e != 0) {
-        set_error("a bounded device wait (preconditioner TMA copy) timed out");
+        set_error(device_error_text(e));
         return DV_ERR_CUDA;
     }
     return DV_OK;
@@ -1698,6 +1720,33 @@ using namespace dv;
 extern "C" {
 
 int dv_abi_version(void) { return DV_ABI_VERSION; }
+
+int dv_selftest_wait_timeout(int32_t polls, int32_t* bits) {
+    if (!bits || polls < 1) { set_error("dv_selftest_wait_timeout: null bits or polls < 1"); return DV_ERR_ARG; }
+    int* d = nullptr;                          // [0] error word, [1..3] barrier words
+    DV_CUDA(cudaMalloc((void**)&d, 4 * sizeof(int)));
+    int rc = DV_OK;
+    cudaError_t e = cudaMemset(d, 0, 4 * sizeof(int));
+    if (e == cudaSuccess) rc = selftest_mbar_timeout(polls, d, 0);
+    if (e == cudaSuccess && rc == DV_OK) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2);
+        cfg.blockDim = dim3(32);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, k_selftest_grid, (int)polls, (unsigned*)(d + 1), d);
+    }
+    int h = 0;
+    if (e == cudaSuccess && rc == DV_OK) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (rc != DV_OK) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "dv_selftest_wait_timeout");
+    *bits = h;
+    return DV_OK;
+}
 
 int dv_profile_enable(int32_t on) {
     cudaDeviceSynchronize();

@@ -255,6 +255,14 @@ int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream);
 int dv_rhs_acc_noalloc(const dv_step_params* p, const double* feed_flux, const double* n_nom,
                        const double* coverage, double t, const double* y, double* f, double* acc, void* stream);
 
+/* Failure-detection self-test (no reference counterpart): runs the library's two bounded device
+ * waits against events that never happen -- the sweep's mbarrier wait on a barrier nothing arrives
+ * at, and the cooperative Gram-Schmidt kernel's grid barrier with one block that never arrives --
+ * each giving up after `polls` polls.  *bits receives the device error word they set (1: the
+ * bulk-copy wait, 4: the grid barrier; 5 when both timed out as they must).  The waits return,
+ * so the CUDA context stays usable.  Synchronous; allocates 16 bytes of device memory. */
+int dv_selftest_wait_timeout(int32_t polls, int32_t* bits);
+
 #ifdef __cplusplus
 }
 #endif
