@@ -1499,15 +1499,14 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
     DV_TRY(copy(z0, W.z));
     DV_TRY(stage(W.z, W.f, W.R));
     scale(W.z, W.s);
-    double rn;
-    DV_TRY(rms_ratio(W, n, W.R, W.s, &rn, st));
-    if (!std::isfinite(rn)) {
-        DV_TRY(copy(z0, zout));
-        r.rate = INFINITY;
-        return DV_OK;
-    }
-    double pn;
-    DV_TRY(pnorm(W.R, W.s, &pn));
+    // rms(R/s) and the preconditioned norm of R, queued into scal[24..25]: they come back with the
+    // first iteration's speculated scalars (one synchronisation fewer per stage solve and per
+    // norm); a non-finite rms then returns z0 as before, with the counters of that iteration undone
+    DV_TRY(rms_ratio_dev(W, n, W.R, W.s, 0, W.scal + 24, st));
+    DV_TRY(precond_apply(m, W.R, nullptr, W.tmp, st));
+    DV_TRY(rms_ratio_dev(W, n, W.tmp, W.s, 0, W.scal + 25, st));
+    double rn = 0.0, pn = 0.0;
+    const int64_t nfev0 = m->nfev;
     double step_prev = -1.0;     // < 0 : None
     int polish = 0;
     bool have_best = false;
@@ -1531,6 +1530,16 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         DV_TRY(speculate());
         DV_CUDA(cudaStreamSynchronize(st));
         if (pending) DV_TRY(gmres_graph_collect(W, m, &info, &inner));
+        if (it == 0) {                                       // the norms queued before the loop
+            rn = W.hpin[16 + 24];
+            pn = W.hpin[16 + 25];
+            if (!std::isfinite(rn)) {
+                m->nfev = nfev0;
+                DV_TRY(copy(z0, zout));
+                r.rate = INFINITY;
+                return DV_OK;
+            }
+        }
         bool spec_ok = true;
         if (polish) r.gmres_polish += inner;
         else { r.gmres_iters += inner; if (C.gm_counter) *C.gm_counter += inner; }
@@ -1695,6 +1704,7 @@ struct dv_integrator {
     int64_t n;
     double *y, *fn, *slope, *z1, *z2, *f1, *f2, *rhs1, *rhs2, *pred, *ev, *es, *d_g;   // device vectors
     double* h_g;                  // pinned: 3 x DV_NACC accumulator rates
+    int* h_err;                   // pinned: the model's device error word, read with the error norm
     double acc[DV_NACC], gn[DV_NACC];
     double t, t_end, h, h_cap, h_lu, log_refactor;
     bool have_J, have_lu, fresh, have_slope, started;
@@ -1954,6 +1964,7 @@ int dv_integrator_destroy(dv_integrator* g) {
     for (double* q : ptrs)
         if (q) cudaFree(q);
     if (g->h_g) cudaFreeHost(g->h_g);
+    if (g->h_err) cudaFreeHost(g->h_err);
     delete g;
     return DV_OK;
 }
@@ -1980,7 +1991,8 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
         }
     }
     if (cudaMalloc((void**)&g->d_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
-        cudaMallocHost((void**)&g->h_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess) {
+        cudaMallocHost((void**)&g->h_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
+        cudaMallocHost((void**)&g->h_err, sizeof(int)) != cudaSuccess) {
         int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(integrator)");
         dv_integrator_destroy(g);
         return rc;
@@ -1988,6 +2000,7 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
     for (double** v : vecs) debug_fill(*v, sizeof(double) * g->n, 4);
     debug_fill(g->d_g, sizeof(double) * 3 * DV_NACC, 4);
     debug_fill(g->h_g, sizeof(double) * 3 * DV_NACC, 8, true);
+    debug_fill(g->h_err, sizeof(int), 8, true);
     *out = g;
     return DV_OK;
 }
@@ -2163,6 +2176,11 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         }
         DV_TRY(precond_apply(m, g->ev, nullptr, g->ev, st));
         DV_LAUNCH(dv::K_VECTOR, st, k_err_scale<<<gr, VB, 0, st>>>(m->nc, n, g->y, g->z2, m->d_atol7, g->o.rtol, g->es));
+        // the accumulator rates of both stages and the device error word come back with the error
+        // norm (one synchronisation)
+        DV_CUDA(cudaMemcpyAsync(g->h_g + DV_NACC, g->d_g + DV_NACC, sizeof(double) * 2 * DV_NACC,
+                                cudaMemcpyDeviceToHost, st));
+        DV_CUDA(cudaMemcpyAsync(g->h_err, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
         double en;
         DV_TRY(rms_ratio(W, n, g->ev, g->es, &en, st));
         if (!std::isfinite(en)) en = 1e6;
@@ -2173,9 +2191,6 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
             continue;
         }
         // ---- accept
-        DV_CUDA(cudaMemcpyAsync(g->h_g + DV_NACC, g->d_g + DV_NACC, sizeof(double) * 2 * DV_NACC,
-                                cudaMemcpyDeviceToHost, st));
-        DV_CUDA(cudaStreamSynchronize(st));
         const double* g1 = g->h_g + DV_NACC;
         const double* g2 = g->h_g + 2 * DV_NACC;
         for (int q = 0; q < DV_NACC; ++q) {
@@ -2207,7 +2222,11 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         sync_nfev();
         DV_CUDA(cudaStreamSynchronize(st));
         *rep = R;
-        return check_device_error(m);
+        if (*g->h_err != 0) {                 // (read with the error norm; the rest of the step has no wait)
+            set_error(device_error_text(*g->h_err));
+            return DV_ERR_CUDA;
+        }
+        return DV_OK;
     }
     R.t = g->t;
     sync_nfev();
