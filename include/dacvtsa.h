@@ -180,7 +180,7 @@ int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, dou
  * ring's theta coupling, as the reference's theta_block keeps its innermost rings'; falls back to
  * mode 0 below 2 rings or 2 sectors).  Stored in the model. */
 int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, void* stream);
-/* Mixed-precision Krylov (no reference counterpart; the BASELINE mixed mode): with on != 0 the
+/* Mixed-precision Krylov (no reference counterpart; an opt-in FP32 preconditioner): with on != 0 the
  * factorisation also stores an FP32 copy of its blocks and dv_precond_solve, GMRES and the Newton
  * step read that copy (products and accumulation stay FP64; the residual, Jacobian, Newton update
  * and balances stay FP64).  Takes effect at the next dv_precond_factor. */
