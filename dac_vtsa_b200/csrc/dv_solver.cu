@@ -1164,7 +1164,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     }
     const bool fused = precond_apply_fusable(m);
     // the cooperative CGS2 kernel takes at most one block per SM (all of them must be resident)
-    static bool coop_ok = true;               // cleared if the driver refuses a cooperative node
+    static bool coop_ok = true;               // cleared if the CUDA driver refuses a cooperative node
     int nsm = 0, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
