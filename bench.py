@@ -332,6 +332,21 @@ def gpu_arm(a, rank, world, local_rank):
     clocks = sampler.stop()
     total_ms = max_over_ranks(total_ms, dist, dev)
     value = replica_throughput(world, a.steps, total_ms / 1e3)
+    # ---- e2e: public step-runner API, host states, outlet recording per accepted step
+    counters.reset()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, a.e2e_steps)):
+        st_in = st.copy()
+        run_cycle(st_in, cfg, grid, props, record_outlet=True)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    nE = max(1, a.e2e_steps)
+    e2e_s = max_over_ranks(e2e_s, dist, dev)
+    e2e = {"value": replica_throughput(world, nE, e2e_s), "unit": "bed-s/wall-s",
+           "h2d_bytes_per_step": counters.TRAFFIC["h2d"] // nE, "d2h_bytes_per_step": counters.TRAFFIC["d2h"] // nE,
+           "path": "runner.run_cycle (steps/_runner.py-compatible run_step per cycle step, outlet recorded at "
+                   "every accepted step)"}
     # ---- mixed precision (gpu.krylov_precision = fp32: FP32 factor storage in the preconditioner
     # sweep), the same cycle, one warm-up and one timed cycle; state difference to the FP64 cycle
     mixed = None
@@ -358,21 +373,6 @@ def gpu_arm(a, rank, world, local_rank):
                  "state_diff_vs_fp64_scaled_max": float(np.abs(dev_scaled).max()),
                  "state_diff_vs_fp64_rel_max": float(np.max(np.abs(y32h - y64h) / (np.abs(y64h) + m0.atol))),
                  "solver": st32}
-    # ---- e2e: public step-runner API, host states, outlet recording per accepted step
-    counters.reset()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(max(1, a.e2e_steps)):
-        st_in = st.copy()
-        run_cycle(st_in, cfg, grid, props, record_outlet=True)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    nE = max(1, a.e2e_steps)
-    e2e_s = max_over_ranks(e2e_s, dist, dev)
-    e2e = {"value": replica_throughput(world, nE, e2e_s), "unit": "bed-s/wall-s",
-           "h2d_bytes_per_step": counters.TRAFFIC["h2d"] // nE, "d2h_bytes_per_step": counters.TRAFFIC["d2h"] // nE,
-           "path": "runner.run_cycle (steps/_runner.py-compatible run_step per cycle step, outlet recorded at "
-                   "every accepted step)"}
     # ---- one profiled cycle: per-kernel device time from CUDA events around every launch
     _lib.profile_enable(True)
     _, _ = one_cycle()
@@ -438,7 +438,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cycle_8x8x32")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2, help="cycles of the e2e measurement (their mean)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision cycle")
     a = ap.parse_args()
