@@ -85,6 +85,26 @@ def _end_summary(model, d, end, c_feed_co2):
     return out
 
 
+def outlet_row(model, d, y, acc, c_feed_co2, V):
+    """The measured part of an outlet record (steps/_runner.py:104-121): both ends' summaries from
+    the diagnostics d, volume means of T, P and the loadings (y), cumulative CO2 out of each
+    valve and jacket heat from the accumulators acc; V = cell volumes."""
+    Vt = float(V.sum())
+    row = {}
+    for end in ("top", "bottom"):
+        row.update(_end_summary(model, d, end, c_feed_co2))
+    row["bed_T_mean_K"] = float(np.sum(d["T"] * V) / Vt)
+    row["bed_P_mean_Pa"] = float(np.sum(d["P"] * V) / Vt)
+    c, q, e, Tw = model.unpack(y)
+    for n, s in enumerate(model.adsorbed):
+        row[f"bed_q_{s}_mean"] = float(np.sum(q[n] * V) / Vt)
+    ai = model.acc_index
+    for v in ("V1", "V2", "V3"):
+        row[f"cum_CO2_out_{v}_mol"] = acc[ai[f"n_out_{v}_CO2"]]
+    row["cum_Q_jacket_J"] = acc[ai["Q_jac_pos"]] + acc[ai["Q_jac_neg"]]
+    return row
+
+
 def run_step(state_in, cfg, grid, props, step: Dict, cycle_idx: int = 1, t_cycle0: float = 0.0,
              T_jacket_prev: Optional[float] = None, logger=None, snapshots: Optional[int] = None,
              record_outlet: bool = True):
@@ -102,23 +122,11 @@ def run_step(state_in, cfg, grid, props, step: Dict, cycle_idx: int = 1, t_cycle
     every = cfg.solver.outlet_record_every
     counter = [0]
     V = grid.volume_full()
-    Vt = float(V.sum())
 
     def record(t, y, acc):
-        d = model.rhs(t, y, diag=True)
         row = {"cycle": cycle_idx, "step": step["name"], "t_step_s": t, "t_cycle_s": t_cycle0 + t,
                "t_total_s": state_in.t + t}
-        for end in ("top", "bottom"):
-            row.update(_end_summary(model, d, end, c_feed_co2))
-        row["bed_T_mean_K"] = float(np.sum(d["T"] * V) / Vt)
-        row["bed_P_mean_Pa"] = float(np.sum(d["P"] * V) / Vt)
-        c, q, e, Tw = model.unpack(y)
-        for n, s in enumerate(model.adsorbed):
-            row[f"bed_q_{s}_mean"] = float(np.sum(q[n] * V) / Vt)
-        ai = model.acc_index
-        for v in ("V1", "V2", "V3"):
-            row[f"cum_CO2_out_{v}_mol"] = acc[ai[f"n_out_{v}_CO2"]]
-        row["cum_Q_jacket_J"] = acc[ai["Q_jac_pos"]] + acc[ai["Q_jac_neg"]]
+        row.update(outlet_row(model, model.rhs(t, y, diag=True), y, acc, c_feed_co2, V))
         outlet.append(row)
 
     def on_step(t, y, acc):

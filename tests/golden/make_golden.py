@@ -11,6 +11,9 @@ Writes (all small, committed):
   colouring.npz          greedy colouring (numerics/sparsity.py:88-107): full arrays for small
                          grids, sha256 + colour count for the benchmark and ensemble grids
   jacobian_3x4x6.npz     coloured FD Jacobian values (core/jacobian.py:71-86)
+  outlet_cases.npz       (--outlet) the reference's diagnostics at seeded states of every cycle
+                         step and the outlet record its runner builds from them
+                         (steps/_runner.py:50-84,104-121)
   trajectory_c0.npz      TR-BDF2 integration of a 4x4x16 bed: 200 s adsorption from the seeded
                          constant-pressure state, then 10 s blowdown and 100 s heating; accepted
                          step sequence, end states, accumulators and solver counters
@@ -248,9 +251,77 @@ def make_bench_state_heating(ref_root, t_heat=4000.0):
     print("heating bench state written")
 
 
+def make_outlet_cases(ref_root):
+    """Outlet records of the reference's runner at seeded states of each cycle step (3x4x6 bed,
+    one seeded state per step), with the diagnostics they are built from."""
+    sys.path.insert(0, ref_root)
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.residual import TVSAModel
+    from core.state import initial_state
+    from properties import R_GAS, get_backend
+    from steps._runner import _end_summary
+    from valves.valve_logic import humid_air_composition
+
+    base = {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6, "jacket.theta_coverage_deg": [0.0, 180.0],
+            "feed.profile": "cosine_theta", "feed.profile_amplitude": 0.3}
+    out, meta = {}, []
+    for step_i in range(4):
+        name = f"step{step_i}"
+        cfg = rp.load_config(override_dict=base)
+        g = Grid.from_config(cfg)
+        props = get_backend(cfg)
+        st = initial_state(cfg, g, props)
+        rng = np.random.default_rng(500 + step_i)
+        st.T = st.T + 5.0 * rng.random(st.T.shape)
+        st.q = st.q + 0.5 * rng.random(st.q.shape)
+        st.c = st.c * (1.0 + 0.05 * rng.random(st.c.shape))
+        st.Tw = st.Tw + 3.0 * rng.random(st.Tw.shape)
+        step = cfg.cycle[step_i]
+        m = TVSAModel(cfg, g, props, step, st)
+        y = m.pack(st)
+        t = 3.0
+        _, acc = m.rhs(t, y)
+        d = m.rhs(t, y, diag=True)
+        yf = humid_air_composition(m.species, cfg.feed.P, cfg.feed.T, cfg.feed.RH if m.water else 0.0,
+                                   cfg.feed.y_co2_dry, float(props.p_sat(cfg.feed.T)))
+        c_feed = yf[m.i_co2] * cfg.feed.P / (R_GAS * cfg.feed.T)
+        row = {}
+        for end in ("top", "bottom"):
+            row.update(_end_summary(m, d, end, c_feed))
+        V = g.volume_full()
+        Vt = float(V.sum())
+        row["bed_T_mean_K"] = float(np.sum(d["T"] * V) / Vt)
+        row["bed_P_mean_Pa"] = float(np.sum(d["P"] * V) / Vt)
+        c, q, e, Tw = m.unpack(y)
+        for n, sp in enumerate(m.adsorbed):
+            row[f"bed_q_{sp}_mean"] = float(np.sum(q[n] * V) / Vt)
+        ai = m.acc_index
+        for v in ("V1", "V2", "V3"):
+            row[f"cum_CO2_out_{v}_mol"] = float(acc[ai[f"n_out_{v}_CO2"]])
+        row["cum_Q_jacket_J"] = float(acc[ai["Q_jac_pos"]] + acc[ai["Q_jac_neg"]])
+        out[f"{name}__y"] = y
+        out[f"{name}__P0"] = st.P
+        out[f"{name}__acc"] = acc
+        out[f"{name}__T"] = d["T"]
+        out[f"{name}__P"] = d["P"]
+        out[f"{name}__yk"] = d["y"]
+        for end in ("top", "bottom"):
+            for key, val in d["bnd"][end].items():
+                out[f"{name}__{end}__{key}"] = np.asarray(val, dtype=float)
+        meta.append({"name": name, "over": base, "step": step_i, "t": t, "c_feed_co2": c_feed,
+                     "bnd_keys": {end: sorted(d["bnd"][end].keys()) for end in ("top", "bottom")},
+                     "row": {k: (v.value if hasattr(v, "value") else v) for k, v in row.items()}})
+        print(name, step["name"], {k: row[k] for k in ("top_flow_out_mol_s", "bottom_flow_out_mol_s")}, flush=True)
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "outlet_cases.npz"), **out)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if "--bench-state" in sys.argv:
+    if "--outlet" in sys.argv:
+        make_outlet_cases(root)
+    elif "--bench-state" in sys.argv:
         make_bench_state(root)
     elif "--bench-state-heating" in sys.argv:
         make_bench_state_heating(root)

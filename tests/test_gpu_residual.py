@@ -92,3 +92,27 @@ def test_axisymmetric_state_stays_axisymmetric():
     for arr in (c, q, e[None]):
         spread = np.abs(arr - arr.mean(axis=-2, keepdims=True)).max()
         assert spread <= 1e-9 * max(np.abs(arr).max(), 1e-30)
+
+
+def test_outlet_records_match_reference():
+    """GPU diagnostics of every cycle step at a seeded state: the boundary records the outlet is
+    built from match the reference's, and so does the outlet row (steps/_runner.py:50-121)."""
+    import json
+    from cases import golden
+    from test_outlet_golden import _same_row
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.runner import outlet_row
+    d = golden("outlet_cases.npz")
+    for meta in json.loads(str(d["meta"])):
+        n = meta["name"]
+        m, _ = build(TVSAModel, meta["over"], meta["step"], d[f"{n}__P0"])
+        y = d[f"{n}__y"]
+        dg = m.rhs(meta["t"], y, diag=True)
+        for end in ("top", "bottom"):
+            assert sorted(dg["bnd"][end]) == meta["bnd_keys"][end], (n, end)
+            for k in meta["bnd_keys"][end]:
+                ref = d[f"{n}__{end}__{k}"]
+                scale = max(np.abs(ref).max(), 1e-300)
+                assert np.abs(dg["bnd"][end][k] - ref).max() <= 1e-12 * scale, (n, end, k)
+        row = outlet_row(m, dg, y, d[f"{n}__acc"], meta["c_feed_co2"], m.grid.volume_full())
+        _same_row(row, meta["row"], rtol=1e-10, atol=1e-18)
