@@ -113,6 +113,6 @@ def test_outlet_records_match_reference():
             for k in meta["bnd_keys"][end]:
                 ref = d[f"{n}__{end}__{k}"]
                 scale = max(np.abs(ref).max(), 1e-300)
-                assert np.abs(dg["bnd"][end][k] - ref).max() <= 1e-12 * scale, (n, end, k)
+                assert np.abs(dg["bnd"][end][k] - ref).max() <= TOL * scale, (n, end, k)
         row = outlet_row(m, dg, y, d[f"{n}__acc"], meta["c_feed_co2"], m.grid.volume_full())
         _same_row(row, meta["row"], rtol=1e-10, atol=1e-18)
