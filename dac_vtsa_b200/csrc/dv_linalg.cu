@@ -561,11 +561,11 @@ static __device__ __forceinline__ int ld_peer_cta(const int* p, uint32_t rank) {
 // slot sl of local plane t being global slot 4 - sl of plane Nz-1-t for rank 1.  TW: after its n
 // planes each rank also forms the multipliers of the separator planes n, n+1 and their Schur contributions Q = -(couplings through
 // the eliminated planes); rank 0 adds both ranks' Q to the separator blocks (read through
-// distributed shared memory) and factorises the 2 nb x 2 nb separator matrix S = [S11 S12; S21 S22]
-// as two more planes of the same block elimination (the inverse is not multiplied out, which loses
-// accuracy when S11 is poorly conditioned):
-//   plane zs:   slot 2 Dm^-1 = S11^-1,  slot 3 -Dm^-1 S12
-//   plane zs+1: slot 1 S21 Dm^-1,       slot 2 Dn^-1 = (S22 - S21 Dm^-1 S12)^-1
+// distributed shared memory) and stores the inverse of the 2 nb x 2 nb separator matrix
+// S = [S11 S12; S21 S22] by blocks (Dm = S11^-1, Dn = (S22 - S21 Dm S12)^-1):
+//   plane zs:   slot 2 Sinv11 = Dm + Dm S12 Dn S21 Dm,  slot 3 Sinv12 = -Dm S12 Dn
+//   plane zs+1: slot 1 Sinv21 = -Dn S21 Dm,             slot 2 Sinv22 = Dn
+// so that the sweep solves the separator in two independent stages.
 template <bool TW>
 __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __restrict__ A, int* __restrict__ info, int lds) {
     const int rank = TW ? (int)(blockIdx.x & 1u) : 0;
@@ -693,14 +693,17 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
             double *S11 = Sb[0], *S12 = Sb[1], *S21 = Sb[2], *S22 = Sb[3];
             double* Xn = S0;                                                   // free: S0, S1, Ui1, U11 (+ T)
             double* Y = S1;
-            bad |= sm_inverse(nb, lds, S11, T, perm, idx, pv, pi);             // Dm^-1
-            sm_gemm(nb, lds, -1.0, S11, S12, 0.0, Xn);                          // -Dm^-1 S12
-            sm_gemm(nb, lds, 1.0, S21, S11, 0.0, Y);                            // S21 Dm^-1
-            sm_gemm(nb, lds, 1.0, S21, Xn, 1.0, S22);                           // S22 - S21 Dm^-1 S12
-            bad |= sm_inverse(nb, lds, S22, T, perm, idx, pv, pi);             // Dn^-1
+            bad |= sm_inverse(nb, lds, S11, T, perm, idx, pv, pi);             // Dm = S11^-1
+            sm_gemm(nb, lds, -1.0, S11, S12, 0.0, Xn);                          // Xn = -Dm S12
+            sm_gemm(nb, lds, 1.0, S21, S11, 0.0, Y);                            // Y = S21 Dm
+            sm_gemm(nb, lds, 1.0, S21, Xn, 1.0, S22);                           // S22 - S21 Dm S12
+            bad |= sm_inverse(nb, lds, S22, T, perm, idx, pv, pi);             // Dn = Sinv22
+            sm_gemm(nb, lds, 1.0, Xn, S22, 0.0, S12);                           // Sinv12 = Xn Dn
+            sm_gemm(nb, lds, -1.0, S22, Y, 0.0, S21);                           // Sinv21 = -Dn Y
+            sm_gemm(nb, lds, -1.0, S12, Y, 1.0, S11);                           // Sinv11 = Dm - Sinv12 Y
             cp_out(nb, ld, lds, S11, B(n, 2));
-            cp_out(nb, ld, lds, Xn, B(n, 3));
-            cp_out(nb, ld, lds, Y, B(n + 1, 1));
+            cp_out(nb, ld, lds, S12, B(n, 3));
+            cp_out(nb, ld, lds, S21, B(n + 1, 1));
             cp_out(nb, ld, lds, S22, B(n + 1, 2));
             if (threadIdx.x == 0) info[part] = bad;
         }
@@ -942,9 +945,8 @@ struct PcFrame {
 //   X:                  p_n = b_n - L1_n z_{n-1} - L2_n z_{n-2},  p_{n+1} = b_{n+1} - L2_{n+1} z_{n-1}
 //                       (b of the separator read by rank 0 only); the two ranks' p are summed
 //                       through distributed shared memory into r
-//   C0, C1, C2:         the separator's block LU (both ranks; r_m, r_m1: global planes zs, zs+1)
-//                       C0: r_m1 -= (S21 Dm^-1) r_m;  C1: x_m1 = Dn^-1 r_m1;
-//                       C2: x_m = Dm^-1 r_m + (-Dm^-1 S12) x_m1
+//   C0, C1:             the separator (both ranks; r_m, r_m1: global planes zs, zs+1)
+//                       x of local plane n + i = [Sinv blocks of that plane] [r_m; r_m1]
 //   B(t), t = n-1..0:   x_t = Uinv_t z_t + (-Uinv_t U1_t) x_{t+1} + (-Uinv_t U2_t) x_{t+2}  (slots 2..4)
 // Without TW the backward stages run t = Nz-1..0 (couplings beyond the last plane are absent).
 #define PA_THREADS 256
@@ -974,7 +976,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
     double* xch = xb + (int64_t)Nz * LD;       // [2][LD]: this rank's partial right-hand sides of the separator (TW)
     TS* buf0 = reinterpret_cast<TS*>(xch + 2 * LD);   // NBUF ring buffers of [3 bs]
     const TS* base = A + (int64_t)part * Nz * 5 * bs;
-    const int S = TW ? 2 * n + 3 : 2 * Nz - 1;
+    const int S = TW ? 2 * n + 2 : 2 * Nz - 1;
     // local planes whose b this CTA reads and whose x it writes
     const int nio = TW ? (rank == 0 ? n + 2 : n) : Nz;
     auto blk = [&](int t, int sl) -> const TS* { return base + ((int64_t)fr.gp(t) * 5 + fr.gs(sl)) * bs; };
@@ -991,12 +993,12 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             src = (fr.rank == 0) ? blk(n, 0) : blk(n, 1);
             nblk = 2;
             src2 = blk(n + 1, 0);
-        } else if (TW && s <= n + 2) {                     // C0, C1: plane zs+1 slot 1, 2; C2: plane zs slots 2, 3
-            const int i = s - n;
-            src = (i < 2) ? base + ((int64_t)(g.zs + 1) * 5 + 1 + i) * bs : base + ((int64_t)g.zs * 5 + 2) * bs;
-            nblk = (i < 2) ? 1 : 2;
+        } else if (TW && s <= n + 1) {                     // C(i): the separator plane's two Sinv blocks
+            const int P = fr.gp(n + (s - n));
+            src = base + ((int64_t)P * 5 + (P == g.zs ? 2 : 1)) * bs;
+            nblk = 2;
         } else {                                           // B(t): slots 2..4
-            const int t = TW ? n - 1 - (s - (n + 3)) : Nz - 1 - (s - (Nz - 1));
+            const int t = TW ? n - 1 - (s - (n + 2)) : Nz - 1 - (s - (Nz - 1));
             src = (fr.rank == 0) ? blk(t, 2) : blk(t, 4);
             nblk = 3;
         }
@@ -1132,28 +1134,17 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
                 xch[LD + r0] = xs[(int64_t)(n + 1) * LD + r0] - a0;
                 if (act1) xch[LD + r1] = xs[(int64_t)(n + 1) * LD + r1] - a1;
             }
-        } else if (TW && s <= n + 2) {                         // C0..C2: both ranks solve the separator
-            const int i = s - n;
-            const int lz0 = (fr.rank == 0) ? n : n + 1;        // local planes of global zs, zs+1
-            const int lz1 = 2 * n + 1 - lz0;
-            if (i == 0) {
-                if (act0) dot2(buf, xs + (int64_t)lz0 * LD, a0, a1);
-                reduce(a0, a1);
-                put(xs + (int64_t)lz1 * LD, a0, a1, true);
-            } else if (i == 1) {
-                if (act0) dot2(buf, xs + (int64_t)lz1 * LD, a0, a1);
-                reduce(a0, a1);
-                put(xb + (int64_t)lz1 * LD, a0, a1, false);
-            } else {
-                if (act0) {
-                    dot2(buf, xs + (int64_t)lz0 * LD, a0, a1);
-                    dot2(buf + bs, xb + (int64_t)lz1 * LD, a0, a1);
-                }
-                reduce(a0, a1);
-                put(xb + (int64_t)lz0 * LD, a0, a1, false);
+        } else if (TW && s <= n + 1) {                         // C(i): both ranks solve the separator
+            const int t = n + (s - n);
+            const int lz0 = (fr.rank == 0) ? n : n + 1;        // local plane of global zs
+            if (act0) {
+                dot2(buf, xs + (int64_t)lz0 * LD, a0, a1);
+                dot2(buf + bs, xs + (int64_t)(2 * n + 1 - lz0) * LD, a0, a1);
             }
+            reduce(a0, a1);
+            put(xb + (int64_t)t * LD, a0, a1, false);
         } else {                                               // B(t)
-            const int t = TW ? n - 1 - (s - (n + 3)) : Nz - 1 - (s - (Nz - 1));
+            const int t = TW ? n - 1 - (s - (n + 2)) : Nz - 1 - (s - (Nz - 1));
             const int lim = TW ? n + 2 : Nz;
             const int64_t oU = (fr.rank == 0) ? 0 : 2 * bs, oW2 = (fr.rank == 0) ? 2 * bs : 0;
             if (act0) {
