@@ -22,8 +22,8 @@
 // Twisted form (Nz >= 8, both kernels in shared memory): the same recurrences run top-down over
 // planes 0..zs-1 and, mirrored, bottom-up over planes Nz-1..zs+2 at the same time (a cluster of
 // two CTAs per partition); the separator planes zs, zs+1 (zs = (Nz-2)/2) take the Schur
-// contributions of both sides and are factorised as two more planes.  Half the sequential plane
-// chain of the one-directional form, for the same matrix.
+// contributions of both sides, and their 2 nb x 2 nb system is inverted by blocks.  Half the
+// sequential plane chain of the one-directional form, for the same matrix.
 #include <algorithm>
 #include <type_traits>
 #include "dv_internal.h"
@@ -922,7 +922,7 @@ int selftest_mbar_timeout(int polls, int* err, cudaStream_t s) {
 // Plane frame of one elimination direction.  TW = false: planes 0..Nz-1 top-down (the whole
 // partition).  TW = true (twisted factorisation, a cluster of two CTAs per partition): rank 0
 // eliminates planes 0..zs-1 top-down, rank 1 planes Nz-1..zs+2 bottom-up, and the separator
-// planes zs, zs+1 take both ranks' contributions and a two-plane block LU of their own.  In its
+// planes zs, zs+1 take both ranks' contributions and an explicit inverse of their own.  In its
 // local frame each rank sees planes
 // t = 0, 1, .. (global gp(t)) with slot sl holding the coupling to local plane t + sl - 2, which is
 // global slot gs(sl): bottom-up, A(t, t-1) local is A(p, p+1) global, and so on.  The local
