@@ -98,7 +98,8 @@ class DvStepReport(C.Structure):
                 ("n_steps", I64), ("n_reject", I64), ("n_newton_fail", I64), ("n_krylov", I64), ("n_jac", I64),
                 ("n_lu", I64), ("nfev", I64), ("gmres_iters", I64), ("gmres_polish", I64),
                 ("balance_unclosed", I64), ("jac_refresh_in_newton", I64), ("krylov_ok", I64),
-                ("krylov_fail", I64), ("acc", D * DV_NACC)]
+                ("krylov_fail", I64), ("acc", D * DV_NACC), ("newton_iters", I64), ("pred_net", I64),
+                ("pred_extrap", I64), ("pred_retry", I64)]
 
 
 P = C.c_void_p
@@ -132,6 +133,17 @@ SIGNATURES = [
     ("dv_integrator_copy_y", C.c_int, [P, P, P]),
     ("dv_rhs_acc_noalloc", C.c_int, [C.POINTER(DvStepParams), P, P, P, D, P, P, P, P]),
     ("dv_selftest_wait_timeout", C.c_int, [I32, C.POINTER(I32)]),
+    ("dv_mlp_create", C.c_int, [I64, C.c_uint64, C.POINTER(P)]),
+    ("dv_mlp_destroy", C.c_int, [P]),
+    ("dv_mlp_reserve", C.c_int, [P, I64]),
+    ("dv_mlp_set_params", C.c_int, [P, P, I64, P, I32]),
+    ("dv_mlp_get_params", C.c_int, [P, P, P]),
+    ("dv_mlp_sample_count", I64, [P]),
+    ("dv_mlp_clear_samples", C.c_int, [P]),
+    ("dv_mlp_forward_host", C.c_int, [P, P, I64, P]),
+    ("dv_mlp_gradient_host", C.c_int, [P, P, P, I64, P, C.POINTER(D)]),
+    ("dv_mlp_train", C.c_int, [P, I32, C.c_float, C.c_uint64, I32, P, P]),
+    ("dv_integrator_set_predictor", C.c_int, [P, P, I32, I32, I32]),
 ]
 
 _lib = None
@@ -172,7 +184,8 @@ def check(rc: int, what: str = ""):
     raise LibraryError(f"{what} failed ({rc}): {msg}")
 
 
-KERNEL_KINDS = ("residual", "matvec", "fd_jacobian", "precond_factor", "precond_apply", "vector")
+KERNEL_KINDS = ("residual", "matvec", "fd_jacobian", "precond_factor", "precond_apply", "vector", "mlp",
+                "spmv")
 
 
 def profile_enable(on: bool = True):

@@ -26,6 +26,7 @@ SOURCES = {                      # file -> extra flags
     "dv_solver.cu": ["-fmad=false"],
     "dv_colour.cu": [],
     "dv_linalg.cu": [],
+    "dv_mlp.cu": [],
 }
 
 
@@ -47,7 +48,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "dacvtsa.h"))
-    objs = []
+    objs, cmds = [], []
     for src, extra in SOURCES.items():
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
@@ -56,9 +57,16 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
             cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", s, "-o", o]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(run, c) for c in cmds]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs]
         if verbose:

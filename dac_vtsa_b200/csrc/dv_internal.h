@@ -13,7 +13,7 @@ int cuda_fail(cudaError_t e, const char* what);
 // Launch accounting: every kernel launch of the library goes through DV_LAUNCH, which counts it per
 // kind and, when profiling is on (dv_profile_enable), brackets it with CUDA events on its stream.
 enum KernelKind { K_RESIDUAL = 0, K_MATVEC = 1, K_FDJAC = 2, K_PC_FACTOR = 3, K_PC_APPLY = 4, K_VECTOR = 5,
-                  K_NKIND = 6 };
+                  K_MLP = 6, K_SPMV = 7, K_NKIND = 8 };
 void prof_begin(int kind, cudaStream_t s);
 void prof_end(int kind, cudaStream_t s);
 void prof_flush();
@@ -26,6 +26,14 @@ void count_launches(int kind, int64_t n);
         __VA_ARGS__;                      \
         dv::prof_end(kind, stream);       \
     } while (0)
+
+#ifndef DV_TRY
+#define DV_TRY(x)                     \
+    do {                              \
+        int rc_ = (x);                \
+        if (rc_ != DV_OK) return rc_; \
+    } while (0)
+#endif
 
 #define DV_CUDA(call)                                      \
     do {                                                   \

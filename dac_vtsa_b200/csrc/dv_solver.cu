@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 #include "dv_internal.h"
+#include "dv_mlp.h"
 
 #include <utility>
 #include "dv_physics.cuh"
@@ -474,11 +475,6 @@ static int rms_ratio(Work& W, int64_t n, const double* a, const double* b, doubl
     return fetch(W, W.scal + 8, 1, out, s);
 }
 
-#define DV_TRY(x)                 \
-    do {                          \
-        int rc_ = (x);            \
-        if (rc_ != DV_OK) return rc_; \
-    } while (0)
 
 
 
@@ -1696,6 +1692,17 @@ __global__ void k_slope(int64_t n, const double* __restrict__ y, const double* _
         out[i] = (z2[i] - y[i]) / h;
 }
 
+// Start of a stage solve: keep cand (the network's guess) when its scaled residual is no larger than
+// that of alt (the extrapolation), else overwrite it with alt; count which one was taken.
+__global__ void k_pick(int64_t n, const double* __restrict__ r, const double* __restrict__ alt, double* __restrict__ cand,
+                       int64_t* __restrict__ cnt) {
+    const bool keep = r[0] <= r[1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[keep ? 0 : 1] += 1;
+    if (keep) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        cand[i] = alt[i];
+}
+
 }  // namespace dv
 
 struct dv_integrator {
@@ -1711,9 +1718,69 @@ struct dv_integrator {
     int jac_age;
     int64_t gm;                   // GMRES iterations (non-polish) since start
     dv_step_report rep;
+    // learned Newton predictor (dv_integrator_set_predictor)
+    dv_mlp* mlp;
+    int pred_on, rec_stride, step_code;
+    double *yprev, *zext;         // state before the last accepted step; the extrapolated guess
+    double h_prev;                // size of the last accepted step
+    bool have_prev;               // yprev and h_prev hold the step before the current state
+    int64_t *d_pick, *h_pick;     // [0] network guess chosen, [1] extrapolation chosen (device; pinned copy)
 };
 
 namespace dv {
+// The predictor's inputs for one stage: latest level A (at the stage's start), the one before it B,
+// f(A), and the stage's time offsets.
+static mlp::StageInputs stage_inputs(const dv_integrator* g, const double* A, const double* B, const double* fA,
+                                     double dt_tgt, double dt_ab, double h, int stage) {
+    mlp::StageInputs in;
+    const dv_model* m = g->m;
+    in.Nr = m->p.Nr;
+    in.Nth = m->p.Nth;
+    in.Nz = m->p.Nz;
+    in.nc = m->nc;
+    in.A = A;
+    in.B = B;
+    in.fA = fA;
+    in.atol7 = m->d_atol7;
+    in.rtol = g->o.rtol;
+    in.dt_tgt = dt_tgt;
+    in.dt_ab = dt_ab;
+    in.h = h;
+    in.stage = stage;
+    in.step_code = g->step_code;
+    return in;
+}
+
+// Predicted start of a stage: g->pred holds the extrapolation on entry.  With recording on, the
+// features of every rec_stride-th cell are stored (targets follow once the stage converged); with the
+// network on, g->pred becomes the network's guess or stays the extrapolation, whichever has the smaller
+// scaled stage residual (two residual evaluations, no host synchronisation).  Returns whether the
+// extrapolation was saved in g->zext (a fallback exists).
+static int predict_stage(dv_integrator* g, const mlp::StageInputs& in, double t, const double* rhs_known, double dh,
+                         int64_t first, int64_t cnt, bool* saved, cudaStream_t st) {
+    *saved = false;
+    if (!g->mlp || (!g->pred_on && g->rec_stride <= 0)) return DV_OK;
+    dv_model* m = g->m;
+    Work& W = *m->W;
+    const int64_t n = g->n;
+    const unsigned gr = vgrid(n);
+    DV_CUDA(cudaMemcpyAsync(g->zext, g->pred, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    *saved = true;
+    if (g->rec_stride > 0) DV_TRY(mlp::record_features(g->mlp, in, first, g->rec_stride, cnt, st));
+    if (!g->pred_on) return DV_OK;
+    DV_TRY(mlp::predict(g->mlp, in, in.stage == 0 ? in.A : in.B, g->pred, st));
+    const double* cands[2] = {g->pred, g->zext};
+    for (int q = 0; q < 2; ++q) {
+        DV_TRY(launch_stage_residual(m, t, cands[q], dh, rhs_known, W.Rt, st));
+        DV_LAUNCH(dv::K_VECTOR, st, k_scale<<<gr, VB, 0, st>>>(m->nc, n, cands[q], m->d_atol7, g->o.rtol, W.w));
+        DV_TRY(rms_ratio_dev(W, n, W.Rt, W.w, 0, W.scal + 26 + q, st));
+    }
+    m->nfev += 2;
+    DV_LAUNCH(dv::K_VECTOR, st, k_pick<<<gr, VB, 0, st>>>(n, W.scal + 26, g->zext, g->pred, g->d_pick));
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
 // A bounded device wait that gave up leaves a flag in the model; surface it as an error.
 static int check_device_error(dv_model* m) {
     int e = 0;
@@ -1960,9 +2027,12 @@ int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_k
 // ------------------------------------------------------------------ integrator
 int dv_integrator_destroy(dv_integrator* g) {
     if (!g) return DV_OK;
-    double* ptrs[] = {g->y, g->fn, g->slope, g->z1, g->z2, g->f1, g->f2, g->rhs1, g->rhs2, g->pred, g->ev, g->es, g->d_g};
+    double* ptrs[] = {g->y, g->fn, g->slope, g->z1, g->z2, g->f1, g->f2, g->rhs1, g->rhs2, g->pred, g->ev, g->es, g->d_g,
+                      g->yprev, g->zext};
     for (double* q : ptrs)
         if (q) cudaFree(q);
+    if (g->d_pick) cudaFree(g->d_pick);
+    if (g->h_pick) cudaFreeHost(g->h_pick);
     if (g->h_g) cudaFreeHost(g->h_g);
     if (g->h_err) cudaFreeHost(g->h_err);
     delete g;
@@ -2018,6 +2088,8 @@ int dv_integrator_start(dv_integrator* g, const double* y0, double t_end, void* 
     memset(g->acc, 0, sizeof(g->acc));
     g->h = std::min(std::min(g->o.h_init, g->o.h_max), t_end);
     g->have_J = g->have_lu = g->fresh = g->have_slope = false;
+    g->have_prev = false;
+    if (g->d_pick) DV_CUDA(cudaMemsetAsync(g->d_pick, 0, 2 * sizeof(int64_t), st));
     g->jac_age = 0;
     g->h_cap = INFINITY;
     g->h_lu = 0.0;
@@ -2034,6 +2106,36 @@ int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream) {
     if (!g || !dst) { set_error("null argument"); return DV_ERR_ARG; }
     DV_CUDA(cudaMemcpyAsync(dst, g->y, sizeof(double) * g->n, cudaMemcpyDefault, (cudaStream_t)stream));
     DV_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return DV_OK;
+}
+
+int dv_integrator_set_predictor(dv_integrator* g, dv_mlp* net, int32_t predict, int32_t record_stride,
+                                int32_t step_code) {
+    if (!g || record_stride < 0 || step_code < 0 || step_code > 3) {
+        set_error("dv_integrator_set_predictor: bad argument");
+        return DV_ERR_ARG;
+    }
+    if (!net) {
+        g->mlp = nullptr;
+        g->pred_on = 0;
+        g->rec_stride = 0;
+        return DV_OK;
+    }
+    DV_TRY(dv_mlp_reserve(net, g->m->nc));
+    if (!g->yprev) {
+        if (cudaMalloc((void**)&g->yprev, sizeof(double) * g->n) != cudaSuccess ||
+            cudaMalloc((void**)&g->zext, sizeof(double) * g->n) != cudaSuccess ||
+            cudaMalloc((void**)&g->d_pick, 2 * sizeof(int64_t)) != cudaSuccess ||
+            cudaMallocHost((void**)&g->h_pick, 2 * sizeof(int64_t)) != cudaSuccess)
+            return cuda_fail(cudaGetLastError(), "cudaMalloc(predictor)");
+        DV_CUDA(cudaMemset(g->d_pick, 0, 2 * sizeof(int64_t)));
+        g->h_pick[0] = g->h_pick[1] = 0;
+        g->have_prev = false;
+    }
+    g->mlp = net;
+    g->pred_on = predict ? 1 : 0;
+    g->rec_stride = record_stride;
+    g->step_code = step_code;
     return DV_OK;
 }
 
@@ -2110,17 +2212,51 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         } else {
             DV_CUDA(cudaMemcpyAsync(g->pred, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         }
+        // learned predictor (off unless dv_integrator_set_predictor attached a network)
+        const bool use_net = g->mlp && g->have_prev;
+        const int64_t stride = g->rec_stride > 0 ? g->rec_stride : 1;
+        mlp::StageInputs in1{};
+        bool saved1 = false;
+        const int64_t first1 = (R.n_steps * 2 + R.n_reject * 5 + R.n_newton_fail * 3) % stride;
+        const int64_t cnt1 = (m->nc - first1 + stride - 1) / stride;
+        if (use_net) {
+            in1 = stage_inputs(g, g->y, g->yprev, g->fn, c_mid * h, g->h_prev, h, 0);
+            DV_TRY(predict_stage(g, in1, g->t + c_mid * h, g->rhs1, dh, first1, cnt1, &saved1, st));
+        }
         no.allow_refresh = g->fresh ? 0 : 1;          // self._fresh = fresh (set before stage 1)
         dv_newton_result r1;
         memset(&r1, 0, sizeof r1);
         NewtonCtx C1{m, &W, m->d_atol7, n, npos, no, &r1, &g->gm};
         DV_TRY(newton_krylov(C1, g->t + c_mid * h, g->pred, g->rhs1, dh, g->z1, st));
         R.n_krylov += 1;
+        R.newton_iters += r1.iters;
         R.gmres_iters += r1.gmres_iters;
         R.gmres_polish += r1.gmres_polish;
         R.balance_unclosed += r1.balance_unclosed;
         R.jac_refresh_in_newton += r1.jac_refresh_in_newton;
         if (r1.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+        if (!r1.ok && saved1 && g->pred_on) {         // the network's start failed: again from the extrapolation
+            R.pred_retry += 1;
+            no.allow_refresh = (g->fresh || r1.refreshed) ? 0 : 1;
+            if (r1.refreshed) {
+                R.n_jac += 1;
+                R.n_lu += 1;
+                g->h_lu = dh / D_;
+                g->jac_age = 0;
+                g->fresh = true;
+            }
+            memset(&r1, 0, sizeof r1);
+            DV_TRY(newton_krylov(C1, g->t + c_mid * h, g->zext, g->rhs1, dh, g->z1, st));
+            R.n_krylov += 1;
+            R.newton_iters += r1.iters;
+            R.gmres_iters += r1.gmres_iters;
+            R.gmres_polish += r1.gmres_polish;
+            R.balance_unclosed += r1.balance_unclosed;
+            R.jac_refresh_in_newton += r1.jac_refresh_in_newton;
+            if (r1.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+        }
+        if (r1.ok && saved1 && g->rec_stride > 0)
+            DV_TRY(mlp::record_targets(g->mlp, in1, g->z1, g->zext, first1, g->rec_stride, cnt1, st));
         if (r1.refreshed) {
             R.n_jac += 1;
             R.n_lu += 1;
@@ -2136,16 +2272,48 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
                 DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<gr, VB, 0, st>>>(n, C1_, g->z1, -C2_, g->y, g->rhs2));
             }
             DV_LAUNCH(dv::K_VECTOR, st, k_pred2<<<gr, VB, 0, st>>>(n, npos, g->y, g->z1, c_mid, g->pred));
+            mlp::StageInputs in2{};
+            bool saved2 = false;
+            const int64_t first2 = (first1 + 1) % stride;
+            const int64_t cnt2 = (m->nc - first2 + stride - 1) / stride;
+            if (g->mlp) {      // levels z1 (with f(z1) from stage 1's last Newton iterate) and y
+                in2 = stage_inputs(g, g->z1, g->y, W.f, (1.0 - c_mid) * h, c_mid * h, h, 1);
+                DV_TRY(predict_stage(g, in2, g->t + h, g->rhs2, dh, first2, cnt2, &saved2, st));
+            }
             dv_newton_result r2;
             memset(&r2, 0, sizeof r2);
             NewtonCtx C2{m, &W, m->d_atol7, n, npos, no, &r2, &g->gm};
             DV_TRY(newton_krylov(C2, g->t + h, g->pred, g->rhs2, dh, g->z2, st));
             R.n_krylov += 1;
+            R.newton_iters += r2.iters;
             R.gmres_iters += r2.gmres_iters;
             R.gmres_polish += r2.gmres_polish;
             R.balance_unclosed += r2.balance_unclosed;
             R.jac_refresh_in_newton += r2.jac_refresh_in_newton;
             if (r2.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+            if (!r2.ok && saved2 && g->pred_on) {
+                R.pred_retry += 1;
+                if (r2.refreshed) {
+                    R.n_jac += 1;
+                    R.n_lu += 1;
+                    g->h_lu = dh / D_;
+                    g->jac_age = 0;
+                    g->fresh = true;
+                }
+                no.allow_refresh = g->fresh ? 0 : 1;
+                memset(&r2, 0, sizeof r2);
+                NewtonCtx C2b{m, &W, m->d_atol7, n, npos, no, &r2, &g->gm};
+                DV_TRY(newton_krylov(C2b, g->t + h, g->zext, g->rhs2, dh, g->z2, st));
+                R.n_krylov += 1;
+                R.newton_iters += r2.iters;
+                R.gmres_iters += r2.gmres_iters;
+                R.gmres_polish += r2.gmres_polish;
+                R.balance_unclosed += r2.balance_unclosed;
+                R.jac_refresh_in_newton += r2.jac_refresh_in_newton;
+                if (r2.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+            }
+            if (r2.ok && saved2 && g->rec_stride > 0)
+                DV_TRY(mlp::record_targets(g->mlp, in2, g->z2, g->zext, first2, g->rec_stride, cnt2, st));
             if (r2.refreshed) {
                 R.n_jac += 1;
                 R.n_lu += 1;
@@ -2203,7 +2371,16 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         }
         DV_LAUNCH(dv::K_VECTOR, st, k_slope<<<gr, VB, 0, st>>>(n, g->y, g->z2, h, g->slope));
         g->have_slope = true;
-        std::swap(g->y, g->z2);
+        if (g->yprev) {            // keep the state before this step for the predictor's second level
+            double* old_prev = g->yprev;
+            g->yprev = g->y;
+            g->y = g->z2;
+            g->z2 = old_prev;
+            g->have_prev = true;
+            g->h_prev = h;
+        } else {
+            std::swap(g->y, g->z2);
+        }
         std::swap(g->fn, g->f2);
         memcpy(g->gn, g2, sizeof(double) * DV_NACC);
         g->t = g->t + h;
@@ -2220,7 +2397,12 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         R.h_used = h;
         memcpy(R.acc, g->acc, sizeof(g->acc));
         sync_nfev();
+        if (g->d_pick) DV_CUDA(cudaMemcpyAsync(g->h_pick, g->d_pick, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         DV_CUDA(cudaStreamSynchronize(st));
+        if (g->d_pick) {
+            R.pred_net = g->h_pick[0];
+            R.pred_extrap = g->h_pick[1];
+        }
         *rep = R;
         if (*g->h_err != 0) {                 // (read with the error norm; the rest of the step has no wait)
             set_error(device_error_text(*g->h_err));

@@ -129,7 +129,8 @@ int dv_device_count(int* n);
 /* Launch accounting (no reference counterpart; instrumentation of this library).  Every kernel launch
  * is counted per kind: 0 residual (rhs / stage residual / diagnostics / accumulators), 1 finite-
  * difference matvec residual, 2 FD Jacobian, 3 preconditioner assembly + factorisation,
- * 4 preconditioner sweep, 5 vector / reduction kernels.  With profiling enabled each launch is also
+ * 4 preconditioner sweep, 5 vector / reduction kernels, 6 learned-predictor network kernels,
+ * 7 assembled-Jacobian (mixed-precision) operator kernels.  With profiling enabled each launch is also
  * bracketed by CUDA events on its own stream; dv_profile_read synchronises the device and returns the
  * launches, the timed launches and their summed device time [ms].  dv_profile_enable resets. */
 int dv_profile_enable(int32_t on);
@@ -222,6 +223,9 @@ typedef struct dv_step_report {
     int64_t n_steps, n_reject, n_newton_fail, n_krylov, n_jac, n_lu, nfev;
     int64_t gmres_iters, gmres_polish, balance_unclosed, jac_refresh_in_newton, krylov_ok, krylov_fail;
     double acc[DV_NACC];       /* accumulator integrals since start (host copy) */
+    int64_t newton_iters;      /* Newton iterations of all stage solves */
+    int64_t pred_net, pred_extrap;   /* stage starts taken from the network / from the extrapolation */
+    int64_t pred_retry;        /* stage solves repeated from the extrapolation after the network's start failed */
 } dv_step_report;
 
 /* TRBDF2(model, cfg, h_max, h_init) (core/solver.py:298-329) */
@@ -238,6 +242,52 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
 const double* dv_integrator_y(const dv_integrator* g);
 /* Copy the current state into dst (device or host memory); synchronises `stream`. */
 int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream);
+
+/* ------------------------------------------------------------------ learned Newton predictor
+ * No counterpart in the reference, which starts each implicit stage from a linear extrapolation
+ * (core/solver.py:420 stage 1, :432/:435 stage 2).  A per-cell network (DV_MLP_NIN inputs -> three tanh
+ * layers of DV_MLP_NH -> DV_MLP_NOUT outputs, BF16 weights and activations, FP32 accumulation on the
+ * tcgen05 tensor cores) predicts a correction to that extrapolation for the six cell unknowns, from the
+ * cell's and its six face neighbours' states at the two latest levels, f at the latest level, the step-
+ * size ratio, the stage and the cycle step.  Parameters (fp32, DV_MLP_NPARAM): W1 [NH x NIN], b1 [NH],
+ * W2 [NH x NH], b2, W3 [NH x NH], b3, W4 [NOUT x NH], b4 [NOUT]; normalisation constants (double,
+ * DV_MLP_NNORM): [0,6) level scales, [6,12) neighbour-difference scales, [12] scale of the solver-unit
+ * features, [13,19) output scale per unknown, [19] target clip. */
+#define DV_MLP_NIN 112
+#define DV_MLP_NH 128
+#define DV_MLP_NOUT 16
+#define DV_MLP_NPARAM 49552
+#define DV_MLP_NNORM 32
+#define DV_MLP_BATCH 4096
+typedef struct dv_mlp dv_mlp;
+/* Network with random hidden weights (seeded) and a zero output layer (predicts no correction), and
+ * room for `sample_capacity` recorded training samples. */
+int dv_mlp_create(int64_t sample_capacity, uint64_t seed, dv_mlp** out);
+int dv_mlp_destroy(dv_mlp* net);
+/* Inference buffers for models of up to ncell cells (dv_integrator_set_predictor calls it). */
+int dv_mlp_reserve(dv_mlp* net, int64_t ncell);
+/* Host parameters in / out (resets the optimiser state); norm may be NULL (unchanged). */
+int dv_mlp_set_params(dv_mlp* net, const float* params, int64_t nparams, const double* norm, int32_t nnorm);
+int dv_mlp_get_params(const dv_mlp* net, float* params, double* norm);
+int64_t dv_mlp_sample_count(const dv_mlp* net);
+int dv_mlp_clear_samples(dv_mlp* net);
+/* Forward pass of host feature rows X [rows][DV_MLP_NIN] (rounded to BF16) -> out [rows][DV_MLP_NOUT]. */
+int dv_mlp_forward_host(dv_mlp* net, const float* X, int64_t rows, float* out);
+/* Gradient of the mean squared error of the first 6 outputs against T [rows][8] (rows <= DV_MLP_BATCH)
+ * by the backward kernels, into grad [DV_MLP_NPARAM]; *loss = the mean squared error. */
+int dv_mlp_gradient_host(dv_mlp* net, const float* X, const float* T, int64_t rows, float* grad, double* loss);
+/* `steps` Adam steps (learning rate lr) on batches of DV_MLP_BATCH recorded samples drawn by a hash of
+ * seed; output scales set from the recorded targets first unless keep_scales; per-step mean loss into
+ * loss_hist (host, optional).  Synchronises `stream`. */
+int dv_mlp_train(dv_mlp* net, int32_t steps, float lr, uint64_t seed, int32_t keep_scales, float* loss_hist,
+                 void* stream);
+/* Attach a network to an integrator (net NULL detaches).  predict != 0: each stage starts from the
+ * network's guess or the extrapolation, whichever has the smaller scaled stage residual, and a Newton
+ * failure from the network's guess is retried from the extrapolation.  record_stride > 0: every
+ * record_stride-th cell of every converged stage is appended to the network's training samples.
+ * step_code: 0 adsorption, 1 blowdown, 2 heating, 3 cooling (a network input). */
+int dv_integrator_set_predictor(dv_integrator* g, dv_mlp* net, int32_t predict, int32_t record_stride,
+                                int32_t step_code);
 
 /* ------------------------------------------------------------------ allocation-free residual
  * No counterpart in the reference: an addition of this library.  Same results as dv_rhs with

@@ -2,7 +2,7 @@
 
 Run once in a container where the reference is importable:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout> [--outlet | --cycle ...]
 
 Writes (all small, committed):
   rhs_cases.npz          f(t, y) and the 36 accumulator rates of TVSAModel.rhs for seeded,
@@ -18,6 +18,12 @@ Writes (all small, committed):
                          constant-pressure state, then 10 s blowdown and 100 s heating; accepted
                          step sequence, end states, accumulators and solver counters
                          (core/solver.py:370-511)
+  cycle_8x8x32[_rtolX].npz  (--cycle [--rtol X]) one full adsorption -> blowdown -> heating ->
+                         cooling cycle of the 8x8x32 bed through the reference's own step runner
+                         (steps/_runner.py:87-188, states handed over in memory as vtsa_cycle.py:
+                         72-90 does with the bit-exact CSV hand-off): per step the end state, the
+                         accepted step times, accumulators, inventories and solver counters, and
+                         the balance rows of validation/conservation_checks.py:29-67
 """
 from __future__ import annotations
 
@@ -317,9 +323,79 @@ def make_outlet_cases(ref_root):
     np.savez_compressed(os.path.join(HERE, "outlet_cases.npz"), **out)
 
 
+CYCLE_POINT = {"solver.scheme": "trbdf2", "operation.T_adsorption_jacket": 288.0, "operation.T_cool": 288.0,
+               "operation.T_heat": 373.0, "operation.P_vacuum": 1e4, "feed.T": 288.0, "feed.RH": 0.5,
+               "ambient.T": 288.0}
+
+
+def make_cycle_golden(ref_root, grid=(8, 8, 32), rtol=None):
+    """The reference's full first cycle of a bed from the seeded constant-pressure state, step by
+    step through its runner, with the balance check of its cycle driver (vtsa_cycle.py:107-110)."""
+    sys.path.insert(0, ref_root)
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.state import initial_state
+    from properties import R_GAS, get_backend
+    from steps import RUNNERS
+    from validation.conservation_checks import check_cycle
+    import time
+    over = dict(CYCLE_POINT, **{"grid.Nr": grid[0], "grid.Ntheta": grid[1], "grid.Nz": grid[2]})
+    if rtol is not None:
+        over["solver.rtol"] = rtol
+    cfg = rp.load_config(override_dict=over)
+    g = Grid.from_config(cfg)
+    props = get_backend(cfg)
+    st = initial_state(cfg, g, props)
+    rng = np.random.default_rng(0)
+    T = 288.0 * (1.0 + 0.01 * (2.0 * rng.random(g.shape) - 1.0))
+    yfrac = st.c / st.c.sum(axis=0)
+    st.c = yfrac * (101325.0 / (R_GAS * T))[None]
+    st.T = T
+    st.Tw = np.full(g.wall_shape, 288.0)
+    out = {"over": np.array(json.dumps(over))}
+    steps, T_prev, t_cycle = [], None, 0.0
+    from core.residual import TVSAModel
+    out["y0"] = TVSAModel(cfg, g, props, cfg.cycle[0], st).pack(st)
+    wall0 = time.time()
+    for k, step in enumerate(cfg.cycle):
+        m = TVSAModel(cfg, g, props, step, st, T_prev)
+        out[f"s{k}_P0"] = st.P
+        out[f"s{k}_T_jacket_prev"] = np.array(np.nan if T_prev is None else T_prev)
+        st, sr = RUNNERS[step["type"]](st, cfg, g, props, step=step, cycle_idx=1, t_cycle0=t_cycle,
+                                       T_jacket_prev=T_prev)
+        out[f"s{k}_y"] = m.pack(st)
+        out[f"s{k}_t_accepted"] = np.array([r["t_step_s"] for r in sr.outlet])
+        out[f"s{k}_acc"] = np.array([sr.acc[nm] for nm in m.acc_names])
+        out[f"s{k}_inv"] = np.array(json.dumps({"start": sr.inv_start, "end": sr.inv_end}))
+        out[f"s{k}_solver"] = np.array(json.dumps({kk: (vv if not isinstance(vv, np.generic) else vv.item())
+                                                    for kk, vv in sr.solver.items()}))
+        out[f"s{k}_meta"] = np.array(json.dumps({"name": sr.name, "duration": sr.duration, "T_jacket": sr.T_jacket,
+                                                 "jacket_on": sr.jacket_on, "wall_time": sr.wall_time}))
+        print(sr.name, sr.duration, sr.solver, f"{sr.wall_time:.1f} s", flush=True)
+        t_cycle += sr.duration
+        T_prev = sr.T_jacket if sr.jacket_on else T_prev
+        steps.append(sr)
+    mb, eb, ok = check_cycle(steps, list(props.species))
+    out["mass_rel_err"] = np.array([r["relative_error"] for r in mb])
+    out["energy_rel_err"] = np.array([r["relative_error"] for r in eb])
+    out["balance_rows"] = np.array(json.dumps({"mass": mb, "energy": eb}, default=float))
+    out["wall_s"] = np.array(time.time() - wall0)
+    tag = "" if rtol is None else f"_rtol{rtol:g}"
+    name = f"cycle_{grid[0]}x{grid[1]}x{grid[2]}{tag}.npz"
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, "max |mass err|", np.abs(out["mass_rel_err"]).max(), "max |energy err|",
+          np.abs(out["energy_rel_err"]).max(), "wall", float(out["wall_s"]), flush=True)
+
+
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if "--outlet" in sys.argv:
+    if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
+        raise SystemExit("usage: make_golden.py <reference checkout> [--outlet | --bench-state | "
+                         "--bench-state-heating | --cycle [--rtol X]]")
+    root = sys.argv[1]
+    if "--cycle" in sys.argv:
+        rt = float(sys.argv[sys.argv.index("--rtol") + 1]) if "--rtol" in sys.argv else None
+        make_cycle_golden(root, rtol=rt)
+    elif "--outlet" in sys.argv:
         make_outlet_cases(root)
     elif "--bench-state" in sys.argv:
         make_bench_state(root)
