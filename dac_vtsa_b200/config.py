@@ -96,7 +96,7 @@ _DEFAULTS: Dict[str, Any] = {
                "jacobian_max_age": 40, "limiter": "van_albada", "max_steps_per_step": 200000,
                "outlet_record_every": 1},
     # GPU-only knobs live in their own namespace so reference configs stay valid.
-    "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation"},
+    "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation", "predictor_weights": ""},
 }
 
 # Choices checked by validate(); everything else is type-checked against the default.
@@ -116,7 +116,7 @@ _CHOICES = {
     "solver.newton_mode": ("krylov", "hybrid", "modified"),
     "solver.preconditioner": ("theta_block", "full"),
     "solver.limiter": ("van_albada", "van_albada_tvd", "van_leer", "minmod", "upwind"),
-    "gpu.krylov_precision": ("fp64", "fp32"),
+    "gpu.krylov_precision": ("fp64", "fp32", "fp32_factors"),
     "gpu.predictor": ("extrapolation", "learned"),
 }
 _POSITIVE = ("geometry.bed_length", "geometry.bed_radius", "grid.Nr", "grid.Ntheta", "grid.Nz",

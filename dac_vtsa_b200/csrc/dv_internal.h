@@ -60,7 +60,7 @@ struct Work {
     cudaGraph_t gm_graph = nullptr;
     cudaGraphExec_t gm_exec = nullptr;
     cudaStream_t gm_cs = nullptr;             // capture stream
-    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1;
+    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1, gm_op32 = -1;
     int gm_prefix = 0;                        // Arnoldi steps captured ahead of the WHILE node
     int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
@@ -109,6 +109,8 @@ struct dv_model {
     int pc_zs;                      // twisted factorisation: first separator plane (0: top-down only)
     int pc_fp32;                    // sweep reads an FP32 copy of the factors (mixed-precision Krylov)
     float* d_pc32;                  // that copy, same layout as d_pc
+    int op32;                       // GMRES operator = FP32 assembled Jacobian d_J32 (mixed-precision Krylov)
+    float* d_J32;                   // [DV_NSLOT][DV_NB][DV_NB][ncell] (allocated on first use)
     int pc_cap_nb, pc_cap_parts;
     double* d_pc;                   // [parts][Nz][5][nb*nb]
     double* d_pc_work;              // [parts][2][nb*nb] factorisation scratch
@@ -130,6 +132,13 @@ int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream
 int launch_matvec(dv_model* m, double t, const double* z, const double* u, const double* sc, const double* f0,
                   double dh, const double* scal, double* out, cudaStream_t s);
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s);
+// The same difference quotients rounded to FP32 (the mixed-precision Krylov operator's Jacobian).
+int launch_fd_jacobian32(dv_model* m, double t, const double* y, const double* f0, float* J, cudaStream_t s);
+// Assembled-Jacobian operator of the Newton system in scaled variables, FP32 products and sums:
+// out = (v - dh J v)/s with v = u s and J the FP32 block Jacobian m->d_J32; dh read from dh_dev when
+// non-null (graph capture), else dh.
+int launch_spmv32(dv_model* m, const double* u, const double* sc, double dh, const double* dh_dev, double* out,
+                  cudaStream_t s, bool count = true);
 // linear algebra (dv_linalg.cu)
 int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s);
 int64_t precond_doubles(int nb, int nparts, int Nz);

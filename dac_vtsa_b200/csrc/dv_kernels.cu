@@ -215,8 +215,9 @@ __global__ void __launch_bounds__(256) k_accumulators(dv_step_params p, const do
 // of the row cell.  With a distance-2 colouring every row sees exactly one perturbed column of
 // each colour, so evaluating the row cell with that single column perturbed reproduces the
 // coloured evaluation of core/jacobian.py:78-84 (colour = colour[column]).
+template <class TJ>
 __global__ void __launch_bounds__(128) k_fd_jacobian(dv_step_params p, Aux aux, double t, const double* __restrict__ y,
-                                                     const double* __restrict__ f0, double* __restrict__ J) {
+                                                     const double* __restrict__ f0, TJ* __restrict__ J) {
     const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz;
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -237,10 +238,10 @@ __global__ void __launch_bounds__(128) k_fd_jacobian(dv_step_params p, Aux aux, 
         default: ok = p.Nth > 1; nj = (j == p.Nth - 1) ? 0 : j + 1; break;
     }
     if (cv == DV_NV) ok = ok && p.wall_on && (ni == p.Nr - 1);
-    double* Jb = J + ((int64_t)slot * DV_NB * DV_NB + cv) * nc + c;     // row stride DV_NB*nc
+    TJ* Jb = J + ((int64_t)slot * DV_NB * DV_NB + cv) * nc + c;         // row stride DV_NB*nc
     if (!ok) {
 #pragma unroll
-        for (int rv = 0; rv < DV_NB; ++rv) Jb[(int64_t)rv * DV_NB * nc] = 0.0;
+        for (int rv = 0; rv < DV_NB; ++rv) Jb[(int64_t)rv * DV_NB * nc] = (TJ)0.0;
         return;
     }
     const int64_t ncell_n = ((int64_t)ni * p.Nth + nj) * p.Nz + nk;
@@ -253,9 +254,9 @@ __global__ void __launch_bounds__(128) k_fd_jacobian(dv_step_params p, Aux aux, 
     const bool outer_wall = (i == p.Nr - 1) && p.wall_on;
     cell_eval(p, aux, ld, t, i, j, k, f, outer_wall ? &fw : nullptr, (const Rec*)nullptr);
 #pragma unroll
-    for (int rv = 0; rv < DV_NV; ++rv) Jb[(int64_t)rv * DV_NB * nc] = (f[rv] - f0[rv * nc + c]) / h;
+    for (int rv = 0; rv < DV_NV; ++rv) Jb[(int64_t)rv * DV_NB * nc] = (TJ)((f[rv] - f0[rv * nc + c]) / h);
     Jb[(int64_t)DV_NV * DV_NB * nc] =
-        outer_wall ? (fw - f0[(int64_t)DV_NV * nc + (int64_t)j * p.Nz + k]) / h : 0.0;
+        (TJ)(outer_wall ? (fw - f0[(int64_t)DV_NV * nc + (int64_t)j * p.Nz + k]) / h : 0.0);
 }
 
 // ---------------------------------------------------------------- split residual
@@ -635,7 +636,14 @@ int matvec_capture(dv_model* m, const double* dargs, const double* z, const doub
 
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s) {
     dim3 grid(nblk(m->nc, 128), DV_NSLOT * DV_NB);
-    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
+    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<double><<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
+int launch_fd_jacobian32(dv_model* m, double t, const double* y, const double* f0, float* J, cudaStream_t s) {
+    dim3 grid(nblk(m->nc, 128), DV_NSLOT * DV_NB);
+    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<float><<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }

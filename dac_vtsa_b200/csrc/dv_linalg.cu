@@ -1523,4 +1523,93 @@ int precond_apply_capture(dv_model* m, const double* b, const double* sc, double
     return DV_OK;
 }
 
+// ---------------------------------------------------------------- FP32 assembled-Jacobian operator
+// Mixed-precision Krylov: the GMRES operator u -> (v - dh J v)/s, v = u s, with J the FP32 block
+// Jacobian (the same difference quotients as the FD Jacobian, rounded), products and sums in FP32;
+// replaces the FP64 finite-difference matvec (core/solver.py:196-203) inside GMRES.  One thread per
+// cell computes its six rows and, for an outer-ring cell, its wall node's row.  Blocks known to be
+// structurally zero (loading rows of neighbour slots, the wall row of inner cells) are not read.
+__global__ void __launch_bounds__(128) k_spmv32(int Nr, int Nth, int Nz, int wall, const float* __restrict__ J,
+                                                const double* __restrict__ u, const double* __restrict__ sc,
+                                                double dh, const double* __restrict__ dh_dev, double* __restrict__ out) {
+    const int64_t nc = (int64_t)Nr * Nth * Nz;
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const double dhv = dh_dev ? dh_dev[1] : dh;
+    const int k = (int)(c % Nz);
+    const int64_t rr = c / Nz;
+    const int j = (int)(rr % Nth);
+    const int i = (int)(rr / Nth);
+    const bool outer_wall = wall && i == Nr - 1;
+    const int64_t offw = (int64_t)DV_NV * nc;
+    float acc[DV_NB];
+#pragma unroll
+    for (int r = 0; r < DV_NB; ++r) acc[r] = 0.0f;
+#pragma unroll
+    for (int slot = 0; slot < DV_NSLOT; ++slot) {
+        int ni = i, nj = j, nk = k;
+        bool ok = true;
+        switch (slot) {
+            case 0: break;
+            case 1: nk = k - 1; ok = nk >= 0; break;
+            case 2: nk = k + 1; ok = nk < Nz; break;
+            case 3: nk = k - 2; ok = nk >= 0; break;
+            case 4: nk = k + 2; ok = nk < Nz; break;
+            case 5: ni = i - 1; ok = ni >= 0; break;
+            case 6: ni = i + 1; ok = ni < Nr; break;
+            case 7: ok = Nth > 1; nj = (j == 0) ? Nth - 1 : j - 1; break;
+            default: ok = Nth > 1; nj = (j == Nth - 1) ? 0 : j + 1; break;
+        }
+        if (!ok) continue;
+        const int64_t cn = ((int64_t)ni * Nth + nj) * Nz + nk;
+        const float* Js = J + (int64_t)slot * DV_NB * DV_NB * nc + c;
+#pragma unroll
+        for (int cv = 0; cv < DV_NV; ++cv) {
+            const int64_t q = (int64_t)cv * nc + cn;
+            const float x = (float)(u[q] * sc[q]);
+#pragma unroll
+            for (int rv = 0; rv < DV_NV; ++rv) {
+                if ((rv == 3 || rv == 4) && slot != 0) continue;
+                acc[rv] = fmaf(Js[(int64_t)(rv * DV_NB + cv) * nc], x, acc[rv]);
+            }
+            if (outer_wall && slot == 0) acc[DV_NV] = fmaf(Js[(int64_t)(DV_NV * DV_NB + cv) * nc], x, acc[DV_NV]);
+        }
+        if (wall && ni == Nr - 1) {      // the neighbour's wall node (column 6)
+            const int64_t q = offw + (int64_t)nj * Nz + nk;
+            const float x = (float)(u[q] * sc[q]);
+            if (slot == 0) {
+#pragma unroll
+                for (int rv = 0; rv < DV_NV; ++rv) {
+                    if (rv == 3 || rv == 4) continue;
+                    acc[rv] = fmaf(Js[(int64_t)(rv * DV_NB + DV_NV) * nc], x, acc[rv]);
+                }
+            }
+            if (outer_wall && (slot == 0 || slot == 1 || slot == 2 || slot == 7 || slot == 8))
+                acc[DV_NV] = fmaf(Js[(int64_t)(DV_NV * DV_NB + DV_NV) * nc], x, acc[DV_NV]);
+        }
+    }
+#pragma unroll
+    for (int rv = 0; rv < DV_NV; ++rv) {
+        const int64_t q = (int64_t)rv * nc + c;
+        out[q] = (u[q] * sc[q] - dhv * (double)acc[rv]) / sc[q];
+    }
+    if (outer_wall) {
+        const int64_t q = offw + (int64_t)j * Nz + k;
+        out[q] = (u[q] * sc[q] - dhv * (double)acc[DV_NV]) / sc[q];
+    }
+}
+
+int launch_spmv32(dv_model* m, const double* u, const double* sc, double dh, const double* dh_dev, double* out,
+                  cudaStream_t s, bool count) {
+    const dv_step_params& p = m->p;
+    const unsigned grid = (unsigned)((m->nc + 127) / 128);
+    if (count) {
+        DV_LAUNCH(dv::K_SPMV, s, k_spmv32<<<grid, 128, 0, s>>>(p.Nr, p.Nth, p.Nz, p.wall_on, m->d_J32, u, sc, dh, dh_dev, out));
+    } else {
+        k_spmv32<<<grid, 128, 0, s>>>(p.Nr, p.Nth, p.Nz, p.wall_on, m->d_J32, u, sc, dh, dh_dev, out);
+    }
+    DV_CUDA(cudaGetLastError());
+    return DV_OK;
+}
+
 }  // namespace dv

@@ -518,6 +518,7 @@ struct Op {
 static int apply_AP(Work& W, const Op& op, const double* w, double* out, cudaStream_t st) {
     DV_TRY(precond_apply(op.m, w, op.s, W.u, st));                      // u = prec(w)
     DV_TRY(rms_ratio_dev(W, op.n, W.u, nullptr, 0, W.scal + 0, st));   // scal[0] = rms(u)
+    if (op.m->op32) return launch_spmv32(op.m, W.u, op.s, op.dh, nullptr, out, st);
     DV_TRY(launch_matvec(op.m, op.t, op.z, W.u, op.s, op.f, op.dh, W.scal, out, st));
     return DV_OK;
 }
@@ -1132,6 +1133,17 @@ static bool gmres_coop_enabled() {
     return v == 1;
 }
 
+// The GMRES operator's launches inside the graph: the FP64 finite-difference matvec (three residual
+// kernels) or, with the mixed-precision operator, one FP32 assembled-Jacobian product.
+static int op_capture(dv_model* m, Work& W, const double* dargs, double* out, cudaStream_t c) {
+    if (m->op32) return launch_spmv32(m, W.u, W.s, 0.0, dargs, out, c, false);
+    return matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, out, c);
+}
+static void op_count(const dv_model* m, int64_t* cnt) {
+    if (m->op32) cnt[K_SPMV] += 1;
+    else cnt[K_MATVEC] += 3;
+}
+
 static int gm_build(dv_model* m, Work& W, int kdim) {
     if (W.gm_exec) { cudaGraphExecDestroy(W.gm_exec); W.gm_exec = nullptr; }
     if (W.gm_graph) { cudaGraphDestroy(W.gm_graph); W.gm_graph = nullptr; }
@@ -1183,7 +1195,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         F.n = n;
         F.stop = &st->done;
         int rc = precond_apply_capture(m, W.vin, W.s, W.u, c, F);
-        if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, c);
+        if (rc == DV_OK) rc = op_capture(m, W, dargs, W.wout, c);
         if (coop) {                          // CGS2 as one cooperative launch (co-resident blocks)
             cudaLaunchConfig_t cfg = {};
             cfg.gridDim = dim3(gc);
@@ -1214,7 +1226,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         for (int q = 0; q < prefix && e == cudaSuccess; ++q) {
             if (arnoldi_step(cs) != DV_OK) e = cudaErrorUnknown;
             fixed[K_PC_APPLY] += 1;
-            fixed[K_MATVEC] += 3;
+            op_count(m, fixed);
             fixed[K_VECTOR] += ncgs;
         }
         if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &ndeps);
@@ -1237,7 +1249,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         if (fused) {
             rc = arnoldi_step(body_cs);
             iter[K_PC_APPLY] += 1;
-            iter[K_MATVEC] += 3;
+            op_count(m, iter);
             iter[K_VECTOR] += ncgs;
         } else {
             k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
@@ -1247,8 +1259,8 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
             k_sumsq<<<g, VB, 0, body_cs>>>(n, W.u, nullptr, W.part);
             k_finish<<<1, VB, 0, body_cs>>>((int)g, W.part, (double)n, 0, W.scal + 0);
             iter[K_VECTOR] += 2;
-            if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.wout, body_cs);
-            iter[K_MATVEC] += 3;
+            if (rc == DV_OK) rc = op_capture(m, W, dargs, W.wout, body_cs);
+            op_count(m, iter);
             for (int pass = 0; pass < 2; ++pass) {
                 double* hb = W.hbuf + pass * (kdim + 2);
                 k_dots_gm<<<g, VB, 0, body_cs>>>(n, st, W.V, ldv, W.wout, W.part);
@@ -1285,8 +1297,8 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
             fixed[K_VECTOR] += 2;
         }
         fixed[K_PC_APPLY] += 1;
-        if (rc == DV_OK) rc = matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, W.r, cs);
-        fixed[K_MATVEC] += 3;
+        if (rc == DV_OK) rc = op_capture(m, W, dargs, W.r, cs);
+        op_count(m, fixed);
         k_axpby<<<g, VB, 0, cs>>>(n, 1.0, W.b, -1.0, W.r, W.r);
         k_sumsq_finish<<<g, VB, 0, cs>>>(n, W.r, nullptr, W.part, W.tickets + 6, 2, W.scal + 10);
         k_gm_info<<<1, 32, 0, cs>>>(st, W.scal);
@@ -1317,6 +1329,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     W.gm_zs = m->pc_zs;
     W.gm_prefix = prefix;
     W.gm_fp32 = m->pc_fp32;
+    W.gm_op32 = m->op32;
     for (int k = 0; k < K_NKIND; ++k) {
         W.gm_fixed[k] = fixed[k];
         W.gm_iter[k] = iter[k];
@@ -1330,7 +1343,8 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
                        int64_t* inner, cudaStream_t st) {
     dv_model* m = op.m;
     if (!W.gm_exec || W.gm_kdim != kdim || W.gm_mode != m->pc_mode || W.gm_nb != m->pc_nb ||
-        W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32 || W.gm_zs != m->pc_zs)
+        W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32 || W.gm_zs != m->pc_zs ||
+        W.gm_op32 != m->op32)
         DV_TRY(gm_build(m, W, kdim));
     GmHost* hst = (GmHost*)W.gm_host;
     hst->args[0] = op.t;
@@ -1416,6 +1430,10 @@ static int refresh_J(NewtonCtx& C, double t, const double* z, double dh, cudaStr
     DV_TRY(launch_rhs(C.m, t, z, W.tmp, nullptr, st));
     DV_TRY(launch_fd_jacobian(C.m, t, z, W.tmp, W.J, st));
     C.m->nfev += C.m->ncolours;
+    if (C.m->op32) {
+        DV_TRY(launch_fd_jacobian32(C.m, t, z, W.tmp, C.m->d_J32, st));
+        C.m->nfev += C.m->ncolours;
+    }
     const double D = (2.0 - std::sqrt(2.0)) / 2.0;
     const double h = dh / D;
     DV_TRY(precond_factor(C.m, W.J, D * h, C.o.precond_mode, st));
@@ -1715,6 +1733,7 @@ struct dv_integrator {
     double acc[DV_NACC], gn[DV_NACC];
     double t, t_end, h, h_cap, h_lu, log_refactor;
     bool have_J, have_lu, fresh, have_slope, started;
+    bool j32_fresh;               // the FP32 operator Jacobian was taken at the current state
     int jac_age;
     int64_t gm;                   // GMRES iterations (non-polish) since start
     dv_step_report rep;
@@ -1857,18 +1876,20 @@ int dv_device_count(int* n) {
     return DV_OK;
 }
 
-int dv_model_set_krylov_fp32(dv_model* m, int32_t on) {
-    if (!m) { set_error("null argument"); return DV_ERR_ARG; }
-    if (m->pc_fp32 != (on ? 1 : 0)) {
-        m->pc_fp32 = on ? 1 : 0;
+int dv_model_set_krylov_fp32(dv_model* m, int32_t mask) {
+    if (!m || mask < 0 || mask > 3) { set_error("dv_model_set_krylov_fp32: mask must be 0..3"); return DV_ERR_ARG; }
+    const int f = (mask & DV_KRYLOV_FP32_FACTORS) ? 1 : 0;
+    if (m->pc_fp32 != f) {
+        m->pc_fp32 = f;
         m->pc_ready = 0;                // the next dv_precond_factor builds the copy the sweep reads
     }
+    m->op32 = (mask & DV_KRYLOV_FP32_OPERATOR) ? 1 : 0;
     return DV_OK;
 }
 
 int dv_model_destroy(dv_model* m) {
     if (!m) return DV_OK;
-    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_acc, m->d_pc, m->d_pc32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
+    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_acc, m->d_pc, m->d_pc32, m->d_J32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
                     m->d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -1915,6 +1936,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
                 cudaMalloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc32, sizeof(float) * pc_need) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_J32, sizeof(float) * m->jac_doubles) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts) != cudaSuccess ||
@@ -1930,6 +1952,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     debug_fill(m->d_acc, sizeof(double) * DV_NACC, 1);
     debug_fill(m->d_pc, sizeof(double) * pc_need, 1);
     debug_fill(m->d_pc32, sizeof(float) * pc_need, 1);
+    debug_fill(m->d_J32, sizeof(float) * m->jac_doubles, 1);
     debug_fill(m->d_pc_work, sizeof(double) * work_need, 1);
     debug_fill(m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb, 1);
     debug_fill(m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts, 1);
@@ -2018,6 +2041,12 @@ int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_k
     cudaStream_t st = (cudaStream_t)stream;
     memset(r, 0, sizeof(*r));
     NewtonCtx C{m, m->W, m->d_atol7, m->n, DV_NG * m->nc + DV_NA * m->nc, *o, r, nullptr};
+    if (m->op32) {                     // FP32 operator Jacobian at z0
+        Work& W = *m->W;
+        DV_TRY(launch_rhs(m, t, z0, W.tmp, nullptr, st));
+        DV_TRY(launch_fd_jacobian32(m, t, z0, W.tmp, m->d_J32, st));
+        m->nfev += 1 + m->ncolours;
+    }
     int rc = newton_krylov(C, t, z0, rhs_known, dh, z_out, st);
     cudaStreamSynchronize(st);
     if (rc == DV_OK) rc = check_device_error(m);
@@ -2048,8 +2077,9 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
     g->o = *o;
     g->n = m->n;
     g->log_refactor = std::log(o->refactor_ratio);
-    if (m->pc_fp32 != (o->krylov_fp32 ? 1 : 0)) {   // factors must be rebuilt in the requested storage
-        m->pc_fp32 = o->krylov_fp32 ? 1 : 0;
+    m->op32 = (o->krylov_fp32 & DV_KRYLOV_FP32_OPERATOR) ? 1 : 0;
+    if (m->pc_fp32 != ((o->krylov_fp32 & DV_KRYLOV_FP32_FACTORS) ? 1 : 0)) {   // factors rebuilt in the requested storage
+        m->pc_fp32 = (o->krylov_fp32 & DV_KRYLOV_FP32_FACTORS) ? 1 : 0;
         m->pc_ready = 0;
     }
     double** vecs[] = {&g->y, &g->fn, &g->slope, &g->z1, &g->z2, &g->f1, &g->f2, &g->rhs1, &g->rhs2, &g->pred, &g->ev, &g->es};
@@ -2089,6 +2119,7 @@ int dv_integrator_start(dv_integrator* g, const double* y0, double t_end, void* 
     g->h = std::min(std::min(g->o.h_init, g->o.h_max), t_end);
     g->have_J = g->have_lu = g->fresh = g->have_slope = false;
     g->have_prev = false;
+    g->j32_fresh = false;
     if (g->d_pick) DV_CUDA(cudaMemsetAsync(g->d_pick, 0, 2 * sizeof(int64_t), st));
     g->jac_age = 0;
     g->h_cap = INFINITY;
@@ -2200,6 +2231,11 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
             g->have_lu = true;
         }
         const double dh = D_ * h;
+        if (m->op32 && !g->j32_fresh) {    // FP32 operator Jacobian at the step's start state
+            DV_TRY(launch_fd_jacobian32(m, g->t, g->y, g->fn, m->d_J32, st));
+            m->nfev += m->ncolours;
+            g->j32_fresh = true;
+        }
         // ---- stage 1
         if (sd) {
             DV_CUDA(cudaMemcpyAsync(g->rhs1, g->y, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
@@ -2385,6 +2421,7 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         memcpy(g->gn, g2, sizeof(double) * DV_NACC);
         g->t = g->t + h;
         R.n_steps += 1;
+        g->j32_fresh = false;
         g->jac_age += 1;
         g->fresh = false;
         if (g->gm - gm0 > g->o.gmres_refresh) g->jac_age = g->o.jacobian_max_age;

@@ -296,12 +296,13 @@ class TVSAModel:
 
     # ------------------------------------------------------------------ linear algebra entry points
     def set_krylov_precision(self, precision: str):
-        """"fp64" (default) or "fp32": storage of the preconditioner factors the sweep streams
-        (products stay FP64); takes effect at the next factorisation."""
-        if precision not in ("fp64", "fp32"):
-            raise ValueError(f"krylov precision must be fp64 or fp32, not {precision!r}")
-        check(self.lib.dv_model_set_krylov_fp32(self.handle, 1 if precision == "fp32" else 0),
-              "dv_model_set_krylov_fp32")
+        """"fp64" (default), "fp32_factors" (the preconditioner factors the sweep streams are FP32;
+        takes effect at the next factorisation) or "fp32" (those factors and GMRES on the FP32
+        assembled Jacobian, refreshed by newton_stage at its start)."""
+        masks = {"fp64": 0, "fp32_factors": 1, "fp32": 3}
+        if precision not in masks:
+            raise ValueError(f"krylov precision must be one of {sorted(masks)}, not {precision!r}")
+        check(self.lib.dv_model_set_krylov_fp32(self.handle, masks[precision]), "dv_model_set_krylov_fp32")
 
     def precond_factor(self, J_block: torch.Tensor, dh: float, mode: str = "theta_block"):
         """Factorise I - dh J (block layout J) along z per partition: "theta_block" (the innermost ring

@@ -104,10 +104,27 @@ class NewtonPredictor:
     def attach(self, integ, step_type: str, predict: bool = True, record_stride: int = 0):
         """Attach to a dac_vtsa_b200.solver.TRBDF2 for its next integrate()."""
         check(self.lib.dv_integrator_set_predictor(integ.handle, self.handle, int(bool(predict)), int(record_stride),
-                                                   STEP_CODES[step_type]), "dv_integrator_set_predictor")
+                                                   STEP_CODES.get(step_type, 0)), "dv_integrator_set_predictor")
         integ.predictor = self
 
 
 def detach(integ):
     check(load().dv_integrator_set_predictor(integ.handle, None, 0, 0, 0), "dv_integrator_set_predictor")
     integ.predictor = None
+
+
+PACKAGED = {"default": "predictor_weights.npz"}
+_CACHE = {}
+
+
+def default_network(path: str = ""):
+    """The network of `path` (or the packaged trained weights), loaded once per process."""
+    import os
+    if not path:
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), PACKAGED["default"])
+    if path not in _CACHE:
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"gpu.predictor = learned needs trained weights: {path} is missing "
+                                    f"(train them with python -m dac_vtsa_b200.train_predictor)")
+        _CACHE[path] = NewtonPredictor.load(path)
+    return _CACHE[path]

@@ -195,12 +195,14 @@ class _PState:
         self.P = P
 
 
-def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None):
+def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predictor=None, predict=True,
+                     record_stride=0):
     """Device-resident cycle: y stays on the GPU from step to step; returns (y_end, per-step stats).
 
     Per step only the start pressure field (for the valve ramps) is evaluated, through the model's
     diagnostics kernel on the device state; the hand-off keeps e (internal energy) as the unknown,
-    which is what the reference's T round trip (pack(to_state(y))) reproduces to round-off."""
+    which is what the reference's T round trip (pack(to_state(y))) reproduces to round-off.
+    predictor: a NewtonPredictor attached to every step's integrator (predict and/or record samples)."""
     y = y0
     stats = []
     last_model = None
@@ -209,6 +211,8 @@ def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None):
         model = TVSAModel(cfg, grid, props, step, _PState(P), T_jac_prev)
         dur = float(step["duration"])
         integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * dur)
+        if predictor is not None:
+            predictor.attach(integ, step["type"], predict=predict, record_stride=record_stride)
         res = integ.integrate(y, dur, np.array([dur]), keep_on_device=True)
         y = res.y
         stats.append({"step": step["name"], "steps": res.n_steps, "rejected": res.n_reject, "nfev": res.nfev,

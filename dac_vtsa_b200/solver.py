@@ -26,6 +26,7 @@ from .config import gpu_option
 from .jacobian import FDJacobian
 from .model import PRECOND_MODES
 
+KRYLOV_FP32_FACTORS, KRYLOV_FP32_OPERATOR = 1, 2
 GAMMA = 2.0 - np.sqrt(2.0)
 D = GAMMA / 2.0
 G_SD = 1.0 - 1.0 / np.sqrt(2.0)
@@ -91,15 +92,25 @@ class TRBDF2:
         o.conservation_tol = float(s.conservation_tol or 0.0)
         o.h_max = h_max
         o.h_init = self.h_init
-        # gpu.krylov_precision: fp64 (default, the parity path) or fp32 (factors streamed in FP32)
+        # gpu.krylov_precision: fp64 (default, the parity path); fp32 (GMRES on the FP32 assembled
+        # Jacobian with FP32 preconditioner factors, FP64 residual / Newton update as refinement);
+        # fp32_factors (only the factors in FP32)
         self.krylov_precision = gpu_option(cfg, "krylov_precision", "fp64")
-        o.krylov_fp32 = 1 if self.krylov_precision == "fp32" else 0
+        o.krylov_fp32 = {"fp64": 0, "fp32_factors": KRYLOV_FP32_FACTORS,
+                         "fp32": KRYLOV_FP32_FACTORS | KRYLOV_FP32_OPERATOR}[self.krylov_precision]
         self.opts = o
 
         h = C.c_void_p()
         check(self.lib.dv_integrator_create(model.handle, C.byref(o), C.byref(h)), "dv_integrator_create")
         self.handle = h
         self._y_host = None
+        # gpu.predictor: extrapolation (default, the reference's predictor) or learned (the trained
+        # network of gpu.predictor_weights, or the packaged one, corrects each stage's start)
+        self.predictor = None
+        if gpu_option(cfg, "predictor", "extrapolation") == "learned":
+            from .predictor import default_network
+            default_network(gpu_option(cfg, "predictor_weights", "")).attach(
+                self, model.step.get("type", "adsorption"), predict=True)
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -196,6 +207,8 @@ class TRBDF2:
             self.stats.update({"krylov_ok": rep.krylov_ok, "krylov_fail": rep.krylov_fail,
                                "gmres_iters": rep.gmres_iters, "gmres_polish": rep.gmres_polish,
                                "balance_unclosed": rep.balance_unclosed,
-                               "jac_refresh_in_newton": rep.jac_refresh_in_newton})
+                               "jac_refresh_in_newton": rep.jac_refresh_in_newton,
+                               "newton_iters": rep.newton_iters, "pred_net": rep.pred_net,
+                               "pred_extrap": rep.pred_extrap, "pred_retry": rep.pred_retry})
             res.wall_time = time.time() - wall0
             return res

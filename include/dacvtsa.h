@@ -181,11 +181,20 @@ int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, dou
  * ring's theta coupling, as the reference's theta_block keeps its innermost rings'; falls back to
  * mode 0 below 2 rings or 2 sectors).  Stored in the model. */
 int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, void* stream);
-/* Mixed-precision Krylov (no reference counterpart; an opt-in FP32 preconditioner): with on != 0 the
- * factorisation also stores an FP32 copy of its blocks and dv_precond_solve, GMRES and the Newton
- * step read that copy (products and accumulation stay FP64; the residual, Jacobian, Newton update
- * and balances stay FP64).  Takes effect at the next dv_precond_factor. */
-int dv_model_set_krylov_fp32(dv_model* m, int32_t on);
+/* Mixed-precision Krylov (no reference counterpart), a mask:
+ *  DV_KRYLOV_FP32_FACTORS   the factorisation also stores an FP32 copy of its blocks, which
+ *                           dv_precond_solve, GMRES and the Newton step stream (sums stay FP64);
+ *                           takes effect at the next dv_precond_factor;
+ *  DV_KRYLOV_FP32_OPERATOR  GMRES's operator is the assembled Jacobian in FP32 (products and sums in
+ *                           FP32) instead of the FP64 finite-difference matvec (core/solver.py:196-
+ *                           203); the integrator refreshes that Jacobian at the start of every step
+ *                           (and with every in-stage refresh), dv_newton_stage at its z0.
+ * The residual, the Jacobian's differencing, the Newton update, the line search and the balances stay
+ * FP64: each Newton iteration is an FP64 refinement of the FP32 Krylov solution, and the unchanged
+ * FP64 convergence test decides. */
+#define DV_KRYLOV_FP32_FACTORS 1
+#define DV_KRYLOV_FP32_OPERATOR 2
+int dv_model_set_krylov_fp32(dv_model* m, int32_t mask);
 /* x = M^-1 b with the stored factors (lu.solve). b and x may alias. */
 int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream);
 
@@ -213,7 +222,7 @@ int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_k
 typedef struct dv_solver_opts {
     int32_t scheme;            /* 0 = sdirk2, 1 = trbdf2 (solver.scheme) */
     int32_t max_newton_iter, jacobian_max_age, gmres_refresh, precond_mode;
-    int32_t krylov_fp32;       /* 1: the preconditioner sweep reads FP32 factors (see dv_model_set_krylov_fp32) */
+    int32_t krylov_fp32;       /* DV_KRYLOV_FP32_* mask (see dv_model_set_krylov_fp32) */
     int64_t max_steps;
     double rtol, newton_kappa, refactor_ratio, conservation_tol, h_max, h_init;
 } dv_solver_opts;

@@ -191,6 +191,26 @@ def test_replay_step_end_states_within_1e8():
     assert np.allclose(acc_gpu, acc_cpu, rtol=1e-8, atol=1e-20)
 
 
+def test_mixed_precision_replay_matches_fp64_within_1e6():
+    """Mixed-precision Krylov (GMRES on the FP32 assembled Jacobian with FP32 factors; FP64 residual and
+    Newton update) replaying the reference's first accepted steps of the 4x4x16 adsorption with every
+    stage solved tightly: the step-end states agree with the FP64 path's to <= 1e-6 relative per
+    entry (the stated mixed-mode tolerance; FP64 refinement makes the agreement far closer)."""
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.replay import fixed_step_run as gpu_run
+    d, m64, cfg, meta = _c0_model(TVSAModel)
+    _, m32, _, _ = _c0_model(TVSAModel)
+    m32.set_krylov_precision("fp32")
+    ts = np.concatenate([[0.0], d["s0_t_accepted"]])
+    hs = np.diff(ts)[:12]
+    y0 = d["s0_y0"]
+    ys64, acc64 = gpu_run(m64, y0, hs, scheme="trbdf2")
+    ys32, acc32 = gpu_run(m32, y0, hs, scheme="trbdf2")
+    worst = max(float((np.abs(a - b) / (np.abs(b) + m64.atol)).max()) for a, b in zip(ys32, ys64))
+    assert worst <= 1e-6, worst
+    assert np.allclose(acc32, acc64, rtol=1e-6, atol=1e-20)
+
+
 def test_free_running_adsorption_matches_reference_to_tolerance():
     """Adaptive 200 s adsorption of the 4x4x16 bed (TR-BDF2, reference defaults): the end state agrees
     with the reference's within its own tolerance scale, and mass/energy balances close as tightly."""
@@ -264,7 +284,7 @@ def test_fp32_factors_solve_to_single_precision(Nz):
     b = np.random.default_rng(11).standard_normal(m.n_core)
     m.precond_factor(J, 1.0)
     x64 = m.precond_solve(b)
-    m.set_krylov_precision("fp32")
+    m.set_krylov_precision("fp32_factors")
     m.precond_factor(J, 1.0)
     x32 = m.precond_solve(b)
     rel = np.abs(x32 - x64).max() / np.abs(x64).max()
