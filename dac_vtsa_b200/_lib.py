@@ -119,6 +119,7 @@ SIGNATURES = [
     ("dv_rhs", C.c_int, [P, D, P, P, P, P]),
     ("dv_stage_residual", C.c_int, [P, D, P, D, P, P, P]),
     ("dv_rhs_diag", C.c_int, [P, D, P, P, P]),
+    ("dv_outlet_row", C.c_int, [P, D, P, D, P, P]),
     ("dv_colour_columns", C.c_int, [I32, I32, I32, I32, P, C.POINTER(I32)]),
     ("dv_fd_jacobian", C.c_int, [P, D, P, P, P, P]),
     ("dv_precond_factor", C.c_int, [P, P, D, I32, P]),

@@ -101,6 +101,7 @@ struct dv_model {
     dv::RecLayout rl;
     double* d_rec;                  // internal record scratch (accumulators)
     double* d_split;                // per-cell properties and per-face fluxes of the split residual
+    double* d_diag;                 // diagnostics record of the outlet summary (dv_outlet_row)
     double* d_acc;                  // DV_NACC
     int64_t nfev;
     int64_t jac_doubles;
@@ -128,6 +129,8 @@ int launch_rhs(dv_model* m, double t, const double* y, double* f, double* acc, c
 int launch_stage_residual(dv_model* m, double t, const double* y, double gamma_h, const double* rhs_known,
                           double* R, cudaStream_t s);
 int launch_diag(dv_model* m, double t, const double* y, double* diag, cudaStream_t s);
+// Outlet summary of state y into row (DV_OUTLET_N doubles, device), via the diagnostics in m->d_diag.
+int launch_outlet(dv_model* m, double t, const double* y, double c_feed, double* row, cudaStream_t s);
 // out = (v - dh (f(z + sig v) - f0)/sig)/s with v = u*s, sig = SQRT_EPS*scal[1]/scal[0] (scal on device)
 int launch_matvec(dv_model* m, double t, const double* z, const double* u, const double* sc, const double* f0,
                   double dh, const double* scal, double* out, cudaStream_t s);

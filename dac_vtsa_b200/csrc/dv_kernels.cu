@@ -648,6 +648,115 @@ int launch_fd_jacobian32(dv_model* m, double t, const double* y, const double* f
     return DV_OK;
 }
 
+// ---------------------------------------------------------------- outlet record
+// The summary of one accepted step that the step runner records (the columns of the outlet time
+// series, steps/_runner.py:50-84,104-121), reduced on the device from the diagnostics record so that
+// only DV_OUTLET_N doubles leave the GPU per step.  Per end: the net outflow (minus the summed inflow
+// records), the area-weighted face pressure, and the composition and temperature of the gas leaving
+// (weighted by each face's outflow, over the faces with outflow; valve ends use their outflow part)
+// or, with no outflow, the area-weighted layer averages.  Fixed-order block reductions.
+constexpr int OUTLET_THREADS = 256;
+
+__device__ double outlet_sum(double v, double* red) {
+    const int tid = threadIdx.x;
+    red[tid] = v;
+    __syncthreads();
+    for (int st = OUTLET_THREADS / 2; st > 0; st >>= 1) {
+        if (tid < st) red[tid] += red[tid + st];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(OUTLET_THREADS) k_outlet(dv_step_params p, Rec rec, const double* __restrict__ y,
+                                                           double c_feed, double* __restrict__ out) {
+    __shared__ double red[OUTLET_THREADS];
+    const int tid = threadIdx.x;
+    const int64_t nc = (int64_t)p.Nr * p.Nth * p.Nz;
+    const int nf = p.Nr * p.Nth;
+    double a[5] = {0.0, 0.0, 0.0, 0.0, 0.0};          // V T, V P, V q_CO2, V q_H2O, V
+    for (int64_t c = tid; c < nc; c += OUTLET_THREADS) {
+        const double V = p.V[c / ((int64_t)p.Nth * p.Nz)];
+        a[0] += rec.T[c] * V;
+        a[1] += rec.P[c] * V;
+        a[2] += y[3 * nc + c] * V;
+        a[3] += y[4 * nc + c] * V;
+        a[4] += V;
+    }
+    double bed[5];
+    for (int q = 0; q < 5; ++q) bed[q] = outlet_sum(a[q], red);
+    if (tid == 0) {
+        out[24] = bed[0] / bed[4];
+        out[25] = bed[1] / bed[4];
+        out[26] = bed[2] / bed[4];
+        out[27] = bed[3] / bed[4];
+    }
+    for (int e = 0; e < 2; ++e) {
+        const int klay = e == 0 ? 0 : p.Nz - 1;
+        const double* b = rec.bnd + (int64_t)e * BR_N * nf;
+        const bool part = p.ends[e].kind == DV_END_VALVE;
+        // A, P A, net outflow, leaving flow, leaving species (3), T leaving flow, y A (3), T A
+        double sm[12];
+        for (int q = 0; q < 12; ++q) sm[q] = 0.0;
+        for (int f = tid; f < nf; f += OUTLET_THREADS) {
+            const double A = p.Az[f / p.Nth];
+            const int64_t cell = (int64_t)f * p.Nz + klay;
+            double Fo[DV_NG], tot = 0.0, tot2 = 0.0;
+            for (int k = 0; k < DV_NG; ++k) tot += -b[(BR_FIN + k) * nf + f];
+            for (int k = 0; k < DV_NG; ++k) {
+                Fo[k] = part ? b[(BR_FOUTP + k) * nf + f] : -b[(BR_FIN + k) * nf + f];
+                tot2 += Fo[k];
+            }
+            const bool leaving = tot2 > 0.0;
+            const double Tl = rec.T[cell];
+            sm[0] += A;
+            sm[1] += b[BR_PFACE * nf + f] * A;
+            sm[2] += tot;
+            if (leaving) {
+                sm[3] += tot2;
+                for (int k = 0; k < DV_NG; ++k) sm[4 + k] += Fo[k];
+                sm[7] += Tl * tot2;
+            }
+            for (int k = 0; k < DV_NG; ++k) sm[8 + k] += rec.y[(int64_t)k * nc + cell] * A;
+            sm[11] += Tl * A;
+        }
+        double r[12];
+        for (int q = 0; q < 12; ++q) r[q] = outlet_sum(sm[q], red);
+        if (tid == 0) {
+            double* o = out + 12 * e;
+            const double Pf = r[1] / r[0];
+            double ys[DV_NG], Tg;
+            if (r[3] > 1e-14) {
+                for (int k = 0; k < DV_NG; ++k) ys[k] = r[4 + k] / r[3];
+                Tg = r[7] / r[3];
+            } else {
+                for (int k = 0; k < DV_NG; ++k) ys[k] = r[8 + k] / r[0];
+                Tg = r[11] / r[0];
+            }
+            o[0] = r[2];
+            o[1] = Pf;
+            o[2] = Tg;
+            for (int k = 0; k < DV_NG; ++k) o[3 + k] = ys[k];
+            const double cco2 = ys[0] * Pf / (DV_R * Tg);
+            o[6] = cco2;
+            o[7] = c_feed > 0.0 ? cco2 / c_feed : __longlong_as_double(0x7ff8000000000000LL);
+            o[8] = r[3];
+            o[9] = o[10] = o[11] = 0.0;
+        }
+    }
+    if (tid == 0)
+        for (int q = 28; q < DV_OUTLET_N; ++q) out[q] = 0.0;
+}
+
+int launch_outlet(dv_model* m, double t, const double* y, double c_feed, double* row, cudaStream_t s) {
+    DV_TRY(launch_diag(m, t, y, m->d_diag, s));
+    Rec rec = make_rec(m->rl, m->d_diag);
+    DV_LAUNCH(dv::K_RESIDUAL, s, k_outlet<<<1, OUTLET_THREADS, 0, s>>>(m->p, rec, y, c_feed, row));
+    return cuda_fail(cudaGetLastError(), "k_outlet");
+}
+
 }  // namespace dv
 
 // ---------------------------------------------------------------- allocation-free residual + accumulators

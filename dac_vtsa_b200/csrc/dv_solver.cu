@@ -1889,7 +1889,7 @@ int dv_model_set_krylov_fp32(dv_model* m, int32_t mask) {
 
 int dv_model_destroy(dv_model* m) {
     if (!m) return DV_OK;
-    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_acc, m->d_pc, m->d_pc32, m->d_J32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
+    void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_diag, m->d_acc, m->d_pc, m->d_pc32, m->d_J32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
                     m->d_err};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -1933,6 +1933,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_split, sizeof(double) * split_doubles(*p)) != cudaSuccess ||
+                cudaMalloc((void**)&m->d_diag, sizeof(double) * m->rl.total) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_pc32, sizeof(float) * pc_need) != cudaSuccess ||
@@ -1949,6 +1950,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     }
     debug_fill(m->d_rec, sizeof(double) * rec_n, 1);
     debug_fill(m->d_split, sizeof(double) * split_doubles(*p), 1);
+    debug_fill(m->d_diag, sizeof(double) * m->rl.total, 1);
     debug_fill(m->d_acc, sizeof(double) * DV_NACC, 1);
     debug_fill(m->d_pc, sizeof(double) * pc_need, 1);
     debug_fill(m->d_pc32, sizeof(float) * pc_need, 1);
@@ -2015,6 +2017,11 @@ int dv_stage_residual(dv_model* m, double t, const double* y, double gamma_h, co
 int dv_rhs_diag(dv_model* m, double t, const double* y, double* diag, void* stream) {
     if (!m || !y || !diag) { set_error("null argument"); return DV_ERR_ARG; }
     return launch_diag(m, t, y, diag, (cudaStream_t)stream);
+}
+
+int dv_outlet_row(dv_model* m, double t, const double* y, double c_feed_co2, double* row, void* stream) {
+    if (!m || !y || !row) { set_error("null argument"); return DV_ERR_ARG; }
+    return launch_outlet(m, t, y, c_feed_co2, row, (cudaStream_t)stream);
 }
 
 int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, void* stream) {

@@ -21,7 +21,10 @@ from typing import Dict, List, Optional
 import numpy as np
 import torch
 
-from . import host
+import ctypes as C
+
+from . import counters, host
+from ._lib import check
 from .model import TVSAModel
 from .solver import TRBDF2
 
@@ -52,127 +55,142 @@ class StepResult:
     ads_end: Dict[str, float] = field(default_factory=dict)
 
 
-def _end_summary(model, d, end, c_feed_co2):
-    """Outlet composition / flow of one end (steps/_runner.py:50-84)."""
-    b = d["bnd"][end]
-    Fout = -b["F_in"]
-    tot = Fout.sum(axis=0)
-    Ftot = float(tot.sum())
-    k_lay = 0 if end == "top" else -1
-    T_lay = d["T"][..., k_lay]
-    A = model.grid.Az * np.ones_like(T_lay)
-    P_face = float(np.sum(b["P_face"] * A) / np.sum(A))
-    out_faces = tot > 0.0
-    if "F_outpart" in b:
-        Fout = b["F_outpart"]
-        tot = Fout.sum(axis=0)
-        out_faces = tot > 0.0
-    F_leaving = float(tot[out_faces].sum()) if np.any(out_faces) else 0.0
-    if F_leaving > 1e-14:
-        ys = [float(Fout[k][out_faces].sum()) / F_leaving for k in range(model.ng)]
-        T_g = float(np.sum(T_lay[out_faces] * tot[out_faces]) / F_leaving)
-    else:
-        yl = d["y"][..., k_lay]
-        ys = [float(np.sum(yl[k] * A) / np.sum(A)) for k in range(model.ng)]
-        T_g = float(np.sum(T_lay * A) / np.sum(A))
-    out = {f"{end}_valve": model.conds[end].valve or "closed", f"{end}_valve_state": model.conds[end].state.value,
-           f"{end}_flow_out_mol_s": Ftot, f"{end}_P_Pa": P_face, f"{end}_T_K": T_g}
-    for k, s in enumerate(model.species):
-        out[f"{end}_y_{s}"] = ys[k]
-    c_co2 = ys[model.i_co2] * P_face / (R_GAS * T_g)
-    out[f"{end}_c_CO2_mol_m3"] = c_co2
-    out[f"{end}_C_over_Cfeed"] = c_co2 / c_feed_co2 if c_feed_co2 > 0 else np.nan
-    return out
+OUTLET_N = 32          # DV_OUTLET_N: doubles of one device outlet summary (include/dacvtsa.h)
+_END_FIELDS = ("flow_out_mol_s", "P_Pa", "T_K")
 
 
-def outlet_row(model, d, y, acc, c_feed_co2, V):
-    """The measured part of an outlet record (steps/_runner.py:104-121): both ends' summaries from
-    the diagnostics d, volume means of T, P and the loadings (y), cumulative CO2 out of each
-    valve and jacket heat from the accumulators acc; V = cell volumes."""
-    Vt = float(V.sum())
-    row = {}
-    for end in ("top", "bottom"):
-        row.update(_end_summary(model, d, end, c_feed_co2))
-    row["bed_T_mean_K"] = float(np.sum(d["T"] * V) / Vt)
-    row["bed_P_mean_Pa"] = float(np.sum(d["P"] * V) / Vt)
-    c, q, e, Tw = model.unpack(y)
-    for n, s in enumerate(model.adsorbed):
-        row[f"bed_q_{s}_mean"] = float(np.sum(q[n] * V) / Vt)
-    ai = model.acc_index
-    for v in ("V1", "V2", "V3"):
-        row[f"cum_CO2_out_{v}_mol"] = acc[ai[f"n_out_{v}_CO2"]]
-    row["cum_Q_jacket_J"] = acc[ai["Q_jac_pos"]] + acc[ai["Q_jac_neg"]]
-    return row
+def feed_co2_concentration(cfg, model) -> float:
+    """CO2 concentration of the humid feed [mol/m3] (the reference of the C/C_feed column)."""
+    yf = host.humid_air_composition(model.species, cfg.feed.P, cfg.feed.T, cfg.feed.RH if model.water else 0.0,
+                                    cfg.feed.y_co2_dry, float(host.arden_buck(cfg.feed.T)))
+    return float(yf[model.i_co2] * cfg.feed.P / (R_GAS * cfg.feed.T))
+
+
+class OutletRecorder:
+    """The outlet time series of one cycle step (the reference runner's per-step records).
+
+    Every record is reduced on the GPU from the model's diagnostics (dv_outlet_row) into one row of
+    a device ring; the ring is copied to the host once, when the step's rows are assembled.  Host
+    side per record: the time and the accumulator integrals (already on the host)."""
+
+    def __init__(self, model, c_feed_co2: float, capacity: int = 1024):
+        self.m = model
+        self.c_feed = float(c_feed_co2)
+        self.ring = torch.empty((capacity, OUTLET_N), dtype=torch.float64, device=model.device)
+        self.times: List[float] = []
+        self.accs: List[np.ndarray] = []
+
+    def record(self, t: float, y_ptr: int, acc):
+        k = len(self.times)
+        if k == self.ring.shape[0]:
+            self.ring = torch.cat([self.ring, torch.empty_like(self.ring)])
+        check(self.m.lib.dv_outlet_row(self.m.handle, float(t), C.c_void_p(y_ptr), self.c_feed,
+                                       C.c_void_p(self.ring[k].data_ptr()),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream)), "dv_outlet_row")
+        self.times.append(float(t))
+        self.accs.append(np.array(acc, dtype=float, copy=True))
+
+    @property
+    def last_t(self) -> float:
+        return self.times[-1] if self.times else -np.inf
+
+    def rows(self, head: Dict) -> List[Dict]:
+        """Row dicts with the reference runner's keys; head supplies cycle, step and time offsets."""
+        vals = self.ring[:len(self.times)].cpu().numpy()
+        counters.d2h(vals.nbytes)
+        m = self.m
+        ai = m.acc_index
+        valve = {e: (m.conds[e].valve or "closed", m.conds[e].state.value) for e in ("top", "bottom")}
+        out = []
+        for t, v, acc in zip(self.times, vals, self.accs):
+            row = {"cycle": head["cycle"], "step": head["step"], "t_step_s": t, "t_cycle_s": head["t_cycle0"] + t,
+                   "t_total_s": head["t_total0"] + t}
+            for e, end in enumerate(("top", "bottom")):
+                b = v[12 * e:12 * e + 12]
+                row[f"{end}_valve"], row[f"{end}_valve_state"] = valve[end]
+                for q, name in enumerate(_END_FIELDS):
+                    row[f"{end}_{name}"] = float(b[q])
+                for k, sp in enumerate(m.species):
+                    row[f"{end}_y_{sp}"] = float(b[3 + k])
+                row[f"{end}_c_CO2_mol_m3"] = float(b[6])
+                row[f"{end}_C_over_Cfeed"] = float(b[7])
+            row["bed_T_mean_K"], row["bed_P_mean_Pa"] = float(v[24]), float(v[25])
+            for n, sp in enumerate(m.adsorbed):
+                row[f"bed_q_{sp}_mean"] = float(v[26 + n])
+            for vv in ("V1", "V2", "V3"):
+                row[f"cum_CO2_out_{vv}_mol"] = float(acc[ai[f"n_out_{vv}_CO2"]])
+            row["cum_Q_jacket_J"] = float(acc[ai["Q_jac_pos"]] + acc[ai["Q_jac_neg"]])
+            out.append(row)
+        return out
+
+
+def _stop_rule(model, step):
+    """(stop_fn, value, direction) of a step's stop_on entry, or Nones (steps/_runner.py semantics)."""
+    stop = step.get("stop_on")
+    if not stop:
+        return None, None, 1
+    return model.stop_metric, stop["value"], (-1 if stop["criterion"] == "min_temperature" else 1)
 
 
 def run_step(state_in, cfg, grid, props, step: Dict, cycle_idx: int = 1, t_cycle0: float = 0.0,
              T_jacket_prev: Optional[float] = None, logger=None, snapshots: Optional[int] = None,
              record_outlet: bool = True):
-    """One cycle step on the GPU (steps/_runner.py:87-188)."""
+    """One cycle step on the GPU: same arguments and result as the reference's run_step
+    (steps/_runner.py:87-188): the end state and a StepResult with accumulators, inventories,
+    solver counters, snapshots and the outlet time series (recorded after every
+    outlet_record_every-th accepted step, on the device)."""
     log = logger or (lambda *a, **k: None)
     model = TVSAModel(cfg, grid, props, step, state_in, T_jacket_prev)
-    y0 = model.pack(state_in)
     dur = float(step["duration"])
+    y0 = model.pack(state_in)
+    y0_dev = torch.from_numpy(y0).to(model.device)
+    counters.h2d(y0.nbytes)
+    rec = OutletRecorder(model, feed_co2_concentration(cfg, model)) if record_outlet else None
+    every = max(1, int(cfg.solver.outlet_record_every))
+    accepted = [0]
+
+    def after_step(t, y_ptr, acc):
+        accepted[0] += 1
+        if accepted[0] % every == 0:
+            rec.record(t, y_ptr, acc)
+
+    if rec is not None:
+        rec.record(0.0, y0_dev.data_ptr(), np.zeros(model.n_acc))
+    stop_fn, stop_val, direction = _stop_rule(model, step)
     n_snap = snapshots if snapshots is not None else cfg.run.snapshots_per_step
-    t_out = np.linspace(0.0, dur, max(2, n_snap))
-    yf = host.humid_air_composition(model.species, cfg.feed.P, cfg.feed.T, cfg.feed.RH if model.water else 0.0,
-                                    cfg.feed.y_co2_dry, float(host.arden_buck(cfg.feed.T)))
-    c_feed_co2 = yf[model.i_co2] * cfg.feed.P / (R_GAS * cfg.feed.T)
-    outlet: List[Dict] = []
-    every = cfg.solver.outlet_record_every
-    counter = [0]
-    V = grid.volume_full()
-
-    def record(t, y, acc):
-        row = {"cycle": cycle_idx, "step": step["name"], "t_step_s": t, "t_cycle_s": t_cycle0 + t,
-               "t_total_s": state_in.t + t}
-        row.update(outlet_row(model, model.rhs(t, y, diag=True), y, acc, c_feed_co2, V))
-        outlet.append(row)
-
-    def on_step(t, y, acc):
-        counter[0] += 1
-        if record_outlet and counter[0] % every == 0:
-            record(t, y, acc)
-
-    if record_outlet:
-        record(0.0, y0, np.zeros(model.n_acc))
-    stop = step.get("stop_on")
-    stop_fn = stop_val = None
-    direction = 1
-    if stop:
-        stop_fn = model.stop_metric
-        stop_val = stop["value"]
-        direction = -1 if stop["criterion"] == "min_temperature" else 1
     wall0 = time.time()
     integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * dur)
-    res = integ.integrate(y0, dur, t_out, on_step=on_step if record_outlet else None, stop_fn=stop_fn,
+    res = integ.integrate(y0_dev, dur, np.linspace(0.0, dur, max(2, n_snap)),
+                          on_step_device=after_step if rec is not None else None, stop_fn=stop_fn,
                           stop_value=stop_val, stop_direction=direction)
-    solver_stats = {"method": "trbdf2", "steps": res.n_steps, "rejected": res.n_reject,
-                    "newton_fail": res.n_newton_fail, "krylov": res.n_krylov, "jacobians": res.n_jac,
-                    "lu": res.n_lu, "nfev": res.nfev, "groups": integ.jac.ngroups, **integ.stats}
-    if record_outlet and outlet[-1]["t_step_s"] < res.t:
-        record(res.t, res.y, res.acc)
+    if rec is not None and rec.last_t < res.t:
+        rec.record(res.t, integ.y_ptr(), res.acc)
     wall = time.time() - wall0
-    state_out = model.to_state(res.y, state_in, state_in.t + res.t, step["name"])
-    state_out.cycle = cycle_idx
+    st_out = model.to_state(res.y, state_in, state_in.t + res.t, step["name"])
+    st_out.cycle = cycle_idx
     snaps = []
-    for (ts, ys, _a) in res.snapshots:
-        st = model.to_state(ys, state_in, state_in.t + ts, step["name"])
-        st.cycle = cycle_idx
+    for ts, ys, _ in res.snapshots:
+        s = model.to_state(ys, state_in, state_in.t + ts, step["name"])
+        s.cycle = cycle_idx
         snaps.append({"cycle": cycle_idx, "step": step["name"], "t_step": ts, "t_cycle": t_cycle0 + ts,
-                      "t_total": state_in.t + ts, "state": st})
-    inv0, inv1 = model.inventories(y0), model.inventories(res.y)
-    acc_d = {nm: float(res.acc[i]) for i, nm in enumerate(model.acc_names)}
-    T_jac = model.T_jacket(res.t) if model.jacket_on else cfg.ambient.T
+                      "t_total": state_in.t + ts, "state": s})
+    inv_start, inv_end = model.inventories(y0), model.inventories(res.y)
+    solver_stats = dict({"method": "trbdf2", "steps": res.n_steps, "rejected": res.n_reject,
+                         "newton_fail": res.n_newton_fail, "krylov": res.n_krylov, "jacobians": res.n_jac,
+                         "lu": res.n_lu, "nfev": res.nfev, "groups": integ.jac.ngroups}, **integ.stats)
+    outlet = rec.rows({"cycle": cycle_idx, "step": step["name"], "t_cycle0": t_cycle0, "t_total0": state_in.t}) \
+        if rec is not None else []
     sr = StepResult(name=step["name"], type=step["type"], cycle=cycle_idx, t_start_cycle=t_cycle0,
-                    duration_planned=dur, duration=res.t, stopped_early=res.stopped_early, acc=acc_d,
-                    inv_start=inv0, inv_end=inv1, outlet=outlet, snapshots=snaps, solver=solver_stats,
-                    wall_time=wall, T_jacket=float(T_jac), jacket_on=model.jacket_on,
-                    product_port=step.get("product_port", "V3"), valves=dict(step["valves"]),
-                    ads_start={s: inv0[f"ads_{s}"] for s in model.adsorbed},
-                    ads_end={s: inv1[f"ads_{s}"] for s in model.adsorbed})
+                    duration_planned=dur, duration=res.t, stopped_early=res.stopped_early,
+                    acc=dict(zip(model.acc_names, (float(a) for a in res.acc))), inv_start=inv_start,
+                    inv_end=inv_end, outlet=outlet, snapshots=snaps, solver=solver_stats, wall_time=wall,
+                    T_jacket=float(model.T_jacket(res.t) if model.jacket_on else cfg.ambient.T),
+                    jacket_on=model.jacket_on, product_port=step.get("product_port", "V3"),
+                    valves=dict(step["valves"]),
+                    ads_start={sp: inv_start[f"ads_{sp}"] for sp in model.adsorbed},
+                    ads_end={sp: inv_end[f"ads_{sp}"] for sp in model.adsorbed})
     log(f"    {step['name']:<14s} {res.t:9.1f} s  steps={res.n_steps:>5}  wall={wall:6.2f}s")
-    return state_out, sr
+    return st_out, sr
 
 
 def run_cycle(state, cfg, grid, props, cycle_idx: int = 1, T_jac_prev=None, logger=None, record_outlet=True):

@@ -136,6 +136,10 @@ class TRBDF2:
               "dv_integrator_copy_y")
         return out
 
+    def y_ptr(self) -> int:
+        """Device address of the integrator's current state (it moves from step to step)."""
+        return int(self.lib.dv_integrator_y(self.handle) or 0)
+
     def _host_y(self) -> np.ndarray:
         if self._y_host is None:
             self._y_host = torch.empty(self.m.n_core, dtype=torch.float64).pin_memory()
@@ -146,11 +150,14 @@ class TRBDF2:
 
     def integrate(self, y0, t_end: float, t_out, on_step: Optional[Callable] = None,
                   stop_fn: Optional[Callable] = None, stop_value: Optional[float] = None,
-                  stop_direction: int = 1, keep_on_device: bool = False) -> IntegrationResult:
+                  stop_direction: int = 1, keep_on_device: bool = False,
+                  on_step_device: Optional[Callable] = None) -> IntegrationResult:
         """Adaptive integration over [0, t_end] (core/solver.py:370-511).
 
         y0: numpy array (host, copied) or float64 CUDA tensor.  With keep_on_device=True the result's
-        ``y`` is a device tensor and snapshots are skipped unless callbacks need host copies."""
+        ``y`` is a device tensor and snapshots are skipped unless callbacks need host copies.
+        on_step_device(t, y_ptr, acc): called where on_step is, with the device address of the
+        accepted state (valid until the next step) instead of a host copy."""
         m = self.m
         wall0 = time.time()
         with torch.cuda.device(m.device):
@@ -191,10 +198,14 @@ class TRBDF2:
                         res.stop_value = sv
                         if on_step:
                             on_step(t, yh, acc)
+                        if on_step_device:
+                            on_step_device(t, self.y_ptr(), acc)
                         res.snapshots.append((t, yh.copy(), acc.copy()))
                         break
                 if on_step:
                     on_step(t, yh, acc)
+                if on_step_device:
+                    on_step_device(t, self.y_ptr(), acc)
                 if k_out < len(t_out) and t >= t_out[k_out] * (1.0 - 1e-12):
                     if not keep_on_device:
                         res.snapshots.append((t, yh.copy(), acc.copy()))

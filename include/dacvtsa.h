@@ -162,6 +162,15 @@ int dv_stage_residual(dv_model* m, double t, const double* y, double gamma_h, co
  * H_inpart H_outpart T_layer 0; Q_jac, Q_amb, Q_wb, R_bed [Nth Nz]; Q_hx [ncell]. */
 int dv_rhs_diag(dv_model* m, double t, const double* y, double* diag, void* stream);
 
+/* Outlet summary of one state (the quantities the reference's runner records after every accepted
+ * step, steps/_runner.py:50-84,104-121), reduced on the device from the diagnostics of t, y into
+ * `row` (DEVICE, DV_OUTLET_N doubles): per end e (top 0, bottom 1) at row[12 e + ...]: 0 net outflow
+ * [mol/s], 1 area-weighted face pressure [Pa], 2 temperature of the leaving gas [K], 3..5 its mole
+ * fractions, 6 its CO2 concentration [mol/m3], 7 that over c_feed_co2 (NaN if c_feed_co2 <= 0),
+ * 8 the leaving flow; row[24..27] volume means of T, P, q_CO2, q_H2O.  Asynchronous on `stream`. */
+#define DV_OUTLET_N 32
+int dv_outlet_row(dv_model* m, double t, const double* y, double c_feed_co2, double* row, void* stream);
+
 /* ------------------------------------------------------------------ Jacobian
  * Greedy distance-2 column colouring of the stencil pattern, bit-identical to
  * color_columns(build_pattern(...)) (numerics/sparsity.py:29-107).  Host call; colour has

@@ -96,12 +96,14 @@ def test_axisymmetric_state_stays_axisymmetric():
 
 def test_outlet_records_match_reference():
     """GPU diagnostics of every cycle step at a seeded state: the boundary records the outlet is
-    built from match the reference's, and so does the outlet row (steps/_runner.py:50-121)."""
+    built from match the reference's, and so does the outlet row reduced on the device (the
+    reference's runner record, steps/_runner.py:50-121)."""
     import json
     from cases import golden
-    from test_outlet_golden import _same_row
+    from outlet_rows import same_row as _same_row
     from dac_vtsa_b200.model import TVSAModel
-    from dac_vtsa_b200.runner import outlet_row
+    import torch
+    from dac_vtsa_b200.runner import OutletRecorder
     d = golden("outlet_cases.npz")
     for meta in json.loads(str(d["meta"])):
         n = meta["name"]
@@ -114,5 +116,10 @@ def test_outlet_records_match_reference():
                 ref = d[f"{n}__{end}__{k}"]
                 scale = max(np.abs(ref).max(), 1e-300)
                 assert np.abs(dg["bnd"][end][k] - ref).max() <= TOL * scale, (n, end, k)
-        row = outlet_row(m, dg, y, d[f"{n}__acc"], meta["c_feed_co2"], m.grid.volume_full())
+        rec = OutletRecorder(m, meta["c_feed_co2"], capacity=2)
+        yd = torch.from_numpy(np.ascontiguousarray(y)).to(m.device)
+        rec.record(meta["t"], yd.data_ptr(), d[f"{n}__acc"])
+        row = rec.rows({"cycle": 1, "step": "x", "t_cycle0": 0.0, "t_total0": 0.0})[0]
+        for k in ("cycle", "step", "t_step_s", "t_cycle_s", "t_total_s"):
+            row.pop(k)
         _same_row(row, meta["row"], rtol=1e-10, atol=1e-18)
