@@ -697,9 +697,10 @@ __global__ void __launch_bounds__(OUTLET_THREADS) k_outlet(dv_step_params p, Rec
         const int klay = e == 0 ? 0 : p.Nz - 1;
         const double* b = rec.bnd + (int64_t)e * BR_N * nf;
         const bool part = p.ends[e].kind == DV_END_VALVE;
-        // A, P A, net outflow, leaving flow, leaving species (3), T leaving flow, y A (3), T A
-        double sm[12];
-        for (int q = 0; q < 12; ++q) sm[q] = 0.0;
+        // A, P A, net outflow, leaving flow, leaving species (3), T leaving flow, y A (3), T A,
+        // net outflow and its CO2 over the faces with net outflow, loading q_CO2 of the layer
+        double sm[15];
+        for (int q = 0; q < 15; ++q) sm[q] = 0.0;
         for (int f = tid; f < nf; f += OUTLET_THREADS) {
             const double A = p.Az[f / p.Nth];
             const int64_t cell = (int64_t)f * p.Nz + klay;
@@ -721,9 +722,14 @@ __global__ void __launch_bounds__(OUTLET_THREADS) k_outlet(dv_step_params p, Rec
             }
             for (int k = 0; k < DV_NG; ++k) sm[8 + k] += rec.y[(int64_t)k * nc + cell] * A;
             sm[11] += Tl * A;
+            if (tot > 0.0) {
+                sm[12] += tot;
+                sm[13] += -b[BR_FIN * nf + f];
+            }
+            sm[14] += y[(int64_t)DV_NG * nc + cell];
         }
-        double r[12];
-        for (int q = 0; q < 12; ++q) r[q] = outlet_sum(sm[q], red);
+        double r[15];
+        for (int q = 0; q < 15; ++q) r[q] = outlet_sum(sm[q], red);
         if (tid == 0) {
             double* o = out + 12 * e;
             const double Pf = r[1] / r[0];
@@ -743,7 +749,9 @@ __global__ void __launch_bounds__(OUTLET_THREADS) k_outlet(dv_step_params p, Rec
             o[6] = cco2;
             o[7] = c_feed > 0.0 ? cco2 / c_feed : __longlong_as_double(0x7ff8000000000000LL);
             o[8] = r[3];
-            o[9] = o[10] = o[11] = 0.0;
+            o[9] = r[12] > 0.0 ? r[13] / r[12] : 0.0;
+            o[10] = r[14] / nf;
+            o[11] = 0.0;
         }
     }
     if (tid == 0)

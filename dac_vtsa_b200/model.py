@@ -155,57 +155,78 @@ class TVSAModel:
     def nfev(self) -> int:
         return int(self.lib.dv_model_nfev(self.handle))
 
+    # ------------------------------------------------------------------ state layout
+    def _blocks(self):
+        """(name, slice, shape) of every variable block of y in order: the gas species, the adsorbed
+        species, e and (with a wall) Tw -- the variable-major layout of core/residual.py:110-118."""
+        g, n = self.grid, self.grid.ncell
+        out = [(f"c_{sp}", slice(k * n, (k + 1) * n), g.shape) for k, sp in enumerate(self.species)]
+        out += [(f"q_{sp}", slice(self.off_q + j * n, self.off_q + (j + 1) * n), g.shape)
+                for j, sp in enumerate(self.adsorbed)]
+        out.append(("e", slice(self.off_e, self.off_w), g.shape))
+        if self.n_w:
+            out.append(("Tw", slice(self.off_w, self.n_core), g.wall_shape))
+        return out
+
+    def _weights(self):
+        """Per-unknown weights of the four balances: moles of each gas species (gas + adsorbed,
+        rows 0..ng-1) and energy of bed and wall (row ng); W @ y are the inventories."""
+        if getattr(self, "_W", None) is None:
+            Vc = np.broadcast_to(self.grid.V, self.grid.shape).ravel()
+            W = np.zeros((self.ng + 1, self.n_core))
+            for name, sl, _ in self._blocks():
+                kind, sp = name.split("_", 1) if "_" in name else (name, None)
+                if kind == "c":
+                    W[self.species.index(sp), sl] = self.eps_t * Vc
+                elif kind == "q":
+                    W[self.species.index(sp), sl] = self.rho_b * Vc
+                elif name == "e":
+                    W[self.ng, sl] = Vc
+                else:
+                    W[self.ng, sl] = self.wall.C
+            self._W = W
+        return self._W
+
     def conservation_matrix(self):
         """Sparse W (ng+1, n_core) with W @ y = inventories (core/residual.py:146-168)."""
         import scipy.sparse as sp
-        g = self.grid
-        n = g.ncell
-        Vc = np.broadcast_to(g.V, g.shape).ravel()
-        rows, cols, vals = [], [], []
-        for k, s in enumerate(self.species):
-            rows.append(np.full(n, k)); cols.append(np.arange(k * n, (k + 1) * n)); vals.append(self.eps_t * Vc)
-            if s in self.adsorbed:
-                j = self.adsorbed.index(s)
-                rows.append(np.full(n, k)); cols.append(self.off_q + np.arange(j * n, (j + 1) * n))
-                vals.append(self.rho_b * Vc)
-        rows.append(np.full(n, self.ng)); cols.append(self.off_e + np.arange(n)); vals.append(Vc)
-        if self.n_w:
-            rows.append(np.full(self.n_w, self.ng)); cols.append(self.off_w + np.arange(self.n_w))
-            vals.append(np.full(self.n_w, self.wall.C))
-        return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
-                             shape=(self.ng + 1, self.n_core))
+        return sp.csr_matrix(self._weights())
 
     def pack(self, st) -> np.ndarray:
-        e = self.thermo.energy(st.T, st.c, st.q)
-        parts = [st.c.ravel(), st.q.ravel(), e.ravel()]
+        """CycleState -> y (core/residual.py:170-183); e from T by the host thermo algebra."""
+        y = np.empty(self.n_core)
+        src = {f"c_{sp}": st.c[k] for k, sp in enumerate(self.species)}
+        src.update({f"q_{sp}": st.q[j] for j, sp in enumerate(self.adsorbed)})
+        src["e"] = self.thermo.energy(st.T, st.c, st.q)
         if self.n_w:
-            parts.append(st.Tw.ravel())
-        return np.concatenate(parts)
+            src["Tw"] = st.Tw
+        for name, sl, _ in self._blocks():
+            y[sl] = np.asarray(src[name]).ravel()
+        return y
 
     def unpack(self, y):
-        g = self.grid
+        """y -> (c, q, e, Tw) views (core/residual.py:185-190); Tw is None without a wall."""
         if isinstance(y, torch.Tensor):
             y = y.detach().cpu().numpy()
-        c = y[:self.n_c].reshape((self.ng,) + g.shape)
-        q = y[self.off_q:self.off_e].reshape((self.na,) + g.shape)
-        e = y[self.off_e:self.off_w].reshape(g.shape)
-        Tw = y[self.off_w:self.n_core].reshape(g.wall_shape) if self.n_w else None
-        return c, q, e, Tw
+        parts = {name: y[sl].reshape(shape) for name, sl, shape in self._blocks()}
+        c = np.stack([parts[f"c_{sp}"] for sp in self.species])
+        q = np.stack([parts[f"q_{sp}"] for sp in self.adsorbed])
+        return c, q, parts["e"], parts.get("Tw")
 
     def to_state(self, y, template, t_abs: float, step_name: str):
+        """y -> CycleState at absolute time t_abs (core/residual.py:192-202)."""
         c, q, e, Tw = self.unpack(y)
-        T = self.thermo.temperature(e, c, q)
         st = template.copy()
-        st.c, st.q, st.T = c.copy(), q.copy(), T.copy()
-        st.Tw = Tw.copy() if Tw is not None else T[-1].copy()
-        st.t = t_abs
-        st.step = step_name
+        st.c, st.q = c.copy(), q.copy()
+        st.T = self.thermo.temperature(e, c, q)
+        st.Tw = st.T[-1].copy() if Tw is None else Tw.copy()
+        st.t, st.step = t_abs, step_name
         return st
 
     def T_jacket(self, t):
-        if self.jac_tau <= 0:
-            return self.T_jac_set
-        return self.T_jac_set + (self.T_jac_prev - self.T_jac_set) * np.exp(-t / self.jac_tau)
+        """Jacket temperature: first-order approach from the previous step's to the set point."""
+        lag = np.exp(-t / self.jac_tau) if self.jac_tau > 0 else 0.0
+        return self.T_jac_set + (self.T_jac_prev - self.T_jac_set) * lag
 
     # ------------------------------------------------------------------ device plumbing
     def _to_dev(self, y, buf):
@@ -346,16 +367,17 @@ class TVSAModel:
     # ------------------------------------------------------------------ inventories / diagnostics
     def inventories(self, y) -> Dict[str, float]:
         """Moles of each species (gas + adsorbed) and bed + wall energy (core/residual.py:426-443)."""
-        g = self.grid
-        c, q, e, Tw = self.unpack(y)
+        if isinstance(y, torch.Tensor):
+            y = y.detach().cpu().numpy()
+        W = self._weights()
         out = {}
-        V = g.V
-        for k, s in enumerate(self.species):
-            gas = float(np.sum(self.eps_t * c[k] * V))
-            ads = float(np.sum(self.rho_b * q[self.adsorbed.index(s)] * V)) if s in self.adsorbed else 0.0
-            out[f"gas_{s}"], out[f"ads_{s}"], out[f"tot_{s}"] = gas, ads, gas + ads
-        out["E_bed"] = float(np.sum(e * V))
-        out["E_wall"] = float(np.sum(self.wall.C * (Tw - self.wall.T_ref))) if Tw is not None else 0.0
+        for k, sp in enumerate(self.species):
+            gas = sum(float(W[k, sl] @ y[sl]) for name, sl, _ in self._blocks() if name == f"c_{sp}")
+            ads = sum(float(W[k, sl] @ y[sl]) for name, sl, _ in self._blocks() if name == f"q_{sp}")
+            out[f"gas_{sp}"], out[f"ads_{sp}"], out[f"tot_{sp}"] = gas, ads, gas + ads
+        blocks = {name: sl for name, sl, _ in self._blocks()}
+        out["E_bed"] = float(W[self.ng, blocks["e"]] @ y[blocks["e"]])
+        out["E_wall"] = (float(self.wall.C * np.sum(y[blocks["Tw"]] - self.wall.T_ref)) if "Tw" in blocks else 0.0)
         out["E_total"] = out["E_bed"] + out["E_wall"]
         return out
 
@@ -369,32 +391,37 @@ class TVSAModel:
         p = yv * cfg.feed.P
         return float(_q_co2_host(cfg, p[self.i_co2], T, _q_h2o_host(cfg, p[self.i_h2o], T, psat)))
 
+    def _summary(self, t, y) -> np.ndarray:
+        """The device outlet summary (dv_outlet_row, DV_OUTLET_N doubles) of state y."""
+        with torch.cuda.device(self.device):
+            yd, _ = self._to_dev(y, self._y)
+            if getattr(self, "_row", None) is None:
+                self._row = torch.empty(32, dtype=torch.float64, device=self.device)
+            check(self.lib.dv_outlet_row(self.handle, float(t), _ptr(yd), 0.0, _ptr(self._row), _stream()),
+                  "dv_outlet_row")
+            v = self._row.cpu().numpy()
+            counters.d2h(v.nbytes)
+            return v
+
     def stop_metric(self, t, y) -> Optional[float]:
-        """Step stop criterion value (core/residual.py:445-469)."""
+        """Value of the step's stop criterion at (t, y) (core/residual.py:445-469), from the device
+        summary: bed mean temperature, CO2 loading of the last layer over the feed equilibrium, or the
+        CO2 fraction leaving the product end over the feed's."""
         stop = self.step.get("stop_on")
         if not stop:
             return None
         crit = stop["criterion"]
-        g = self.grid
-        c, q, e, Tw = self.unpack(y)
+        if crit not in ("min_temperature", "max_temperature", "end_saturation", "outlet_ratio"):
+            return None
+        v = self._summary(t, y)
         if crit in ("min_temperature", "max_temperature"):
-            T = self.thermo.temperature(e, c, q)
-            return float(np.sum(T * g.V) / np.sum(g.V * np.ones_like(T)))
+            return float(v[24])
         if crit == "end_saturation":
-            return float(np.mean(q[0][..., -1]) / self.q_feed_eq())
-        if crit == "outlet_ratio":
-            d = self.rhs(t, y, diag=True)
-            b = d["bnd"]["bottom"] if self.conds["top"].kind == "feed" else d["bnd"]["top"]
-            Fout = -b["F_in"]
-            tot = Fout.sum(axis=0)
-            m = tot > 0
-            if not np.any(m):
-                return 0.0
-            y_out = Fout[self.i_co2][m].sum() / tot[m].sum()
-            yf = self.conds["top"].y_ext[self.i_co2] if self.conds["top"].y_ext is not None else 4e-4
-            return float(y_out / yf)
-        return None
-
+            return float(v[12 + 10] / self.q_feed_eq())
+        end = 1 if self.conds["top"].kind == "feed" else 0
+        y_ext = self.conds["top"].y_ext
+        yf = y_ext[self.i_co2] if y_ext is not None else 4e-4
+        return float(v[12 * end + 9] / yf)
 
 def _toth_host(p, T, q_inf0, chi, b0, dH0, tau0, alpha, T0):
     p = max(p, 0.0)

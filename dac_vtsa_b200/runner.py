@@ -214,13 +214,15 @@ class _PState:
 
 
 def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predictor=None, predict=True,
-                     record_stride=0):
+                     record_stride=0, writer=None, handoff=None):
     """Device-resident cycle: y stays on the GPU from step to step; returns (y_end, per-step stats).
 
     Per step only the start pressure field (for the valve ramps) is evaluated, through the model's
     diagnostics kernel on the device state; the hand-off keeps e (internal energy) as the unknown,
     which is what the reference's T round trip (pack(to_state(y))) reproduces to round-off.
-    predictor: a NewtonPredictor attached to every step's integrator (predict and/or record samples)."""
+    predictor: a NewtonPredictor attached to every step's integrator (predict and/or record samples).
+    writer + handoff (template state, cycle index, directory): each step's end state is also written
+    as the reference's hand-off CSV by the AsyncStateWriter while the next step runs."""
     y = y0
     stats = []
     last_model = None
@@ -234,7 +236,12 @@ def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predic
         res = integ.integrate(y, dur, np.array([dur]), keep_on_device=True)
         y = res.y
         stats.append({"step": step["name"], "steps": res.n_steps, "rejected": res.n_reject, "nfev": res.nfev,
-                      "jac": res.n_jac, "lu": res.n_lu, **integ.stats})
+                      "jac": res.n_jac, "lu": res.n_lu, **integ.stats, "t": res.t,
+                      "acc": dict(zip(model.acc_names, (float(a) for a in res.acc)))})
+        if writer is not None:
+            template, cyc, folder = handoff
+            writer.submit(y, model, template, template.t + res.t, step["name"], cyc, grid,
+                          os.path.join(folder, f"state_after_{step['name']}.csv"))
         T_jac_prev = model.T_jacket(res.t) if model.jacket_on else T_jac_prev
         last_model = model
     return y, stats, T_jac_prev

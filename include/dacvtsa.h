@@ -167,7 +167,9 @@ int dv_rhs_diag(dv_model* m, double t, const double* y, double* diag, void* stre
  * `row` (DEVICE, DV_OUTLET_N doubles): per end e (top 0, bottom 1) at row[12 e + ...]: 0 net outflow
  * [mol/s], 1 area-weighted face pressure [Pa], 2 temperature of the leaving gas [K], 3..5 its mole
  * fractions, 6 its CO2 concentration [mol/m3], 7 that over c_feed_co2 (NaN if c_feed_co2 <= 0),
- * 8 the leaving flow; row[24..27] volume means of T, P, q_CO2, q_H2O.  Asynchronous on `stream`. */
+ * 8 the leaving flow, 9 the CO2 fraction of the net outflow over the faces with net outflow (0 when
+ * none), 10 the mean q_CO2 of the end layer; row[24..27] volume means of T, P, q_CO2, q_H2O.  These
+ * also give the stop criteria of core/residual.py:445-469.  Asynchronous on `stream`. */
 #define DV_OUTLET_N 32
 int dv_outlet_row(dv_model* m, double t, const double* y, double c_feed_co2, double* row, void* stream);
 

@@ -18,6 +18,11 @@ Writes (all small, committed):
                          constant-pressure state, then 10 s blowdown and 100 s heating; accepted
                          step sequence, end states, accumulators and solver counters
                          (core/solver.py:370-511)
+  state_csv/seeded_3x4x6*  (--csv) a seeded state written by the reference's save_state_csv
+                         (the 17-digit hand-off format, simio/checkpoint.py:27-53)
+  stop_young2021.npz     (--stop) the young2021 1-D case's adsorption step, stopped by its
+                         end_saturation criterion (core/residual.py:445-482, core/solver.py:
+                         476-494): stop time, stop value, end state
   cycle_8x8x32[_rtolX].npz  (--cycle [--rtol X]) one full adsorption -> blowdown -> heating ->
                          cooling cycle of the 8x8x32 bed through the reference's own step runner
                          (steps/_runner.py:87-188, states handed over in memory as vtsa_cycle.py:
@@ -387,12 +392,77 @@ def make_cycle_golden(ref_root, grid=(8, 8, 32), rtol=None):
           np.abs(out["energy_rel_err"]).max(), "wall", float(out["wall_s"]), flush=True)
 
 
+def make_csv_golden(ref_root):
+    """A seeded non-trivial 3x4x6 state written by the reference's save_state_csv (simio/checkpoint.py:
+    27-53), with the arrays it came from."""
+    sys.path.insert(0, ref_root)
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.state import initial_state
+    from properties import get_backend
+    from simio.checkpoint import save_state_csv
+    cfg = rp.load_config(override_dict={"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6})
+    g = Grid.from_config(cfg)
+    st = initial_state(cfg, g, get_backend(cfg))
+    rng = np.random.default_rng(11)
+    st.T = st.T + 7.0 * rng.random(st.T.shape)
+    st.q = st.q + rng.random(st.q.shape)
+    st.c = st.c * (1.0 + 0.1 * rng.random(st.c.shape))
+    st.Tw = st.Tw + 3.0 * rng.random(st.Tw.shape)
+    st.t, st.cycle, st.step = 1234.5678901234567, 3, "heating"
+    d = os.path.join(HERE, "state_csv")
+    save_state_csv(st, g, os.path.join(d, "seeded_3x4x6.csv"))
+    np.savez_compressed(os.path.join(d, "seeded_3x4x6.npz"), c=st.c, q=st.q, T=st.T, Tw=st.Tw,
+                        meta=np.array(json.dumps({"t": st.t, "cycle": st.cycle, "step": st.step})))
+
+
+def make_stop_golden(ref_root):
+    """The adsorption step of the reference's young2021 1-D case (config/cases/
+    young2021_1d_equivalent.yaml: 1x1x30 bed, stop_on end_saturation 0.9895) from its initial state,
+    run by the reference's step runner until the stop criterion fires: stop time and value, the
+    stop metric at the start, the end state and the solver counters."""
+    sys.path.insert(0, ref_root)
+    import yaml
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.residual import TVSAModel
+    from core.state import initial_state
+    from properties import get_backend
+    from steps import RUNNERS
+    case = os.path.join(ref_root, "config", "cases", "young2021_1d_equivalent.yaml")
+    with open(case) as fh:
+        raw = yaml.safe_load(fh)
+    cfg = rp.load_config(user_yaml=case)
+    g = Grid.from_config(cfg)
+    props = get_backend(cfg)
+    st = initial_state(cfg, g, props)
+    k = [i for i, s_ in enumerate(cfg.cycle) if s_.get("stop_on")][0]
+    step = cfg.cycle[k]
+    m = TVSAModel(cfg, g, props, step, st)
+    y0 = m.pack(st)
+    metric0 = m.stop_metric(0.0, y0)
+    st1, sr = RUNNERS[step["type"]](st, cfg, g, props, step=step, cycle_idx=1, snapshots=2)
+    y1 = TVSAModel(cfg, g, props, step, st).pack(st1)
+    out = {"case_yaml": np.array(json.dumps(raw)), "step_index": np.array(k), "y0": y0, "P0": st.P,
+           "metric0": np.array(metric0), "q_feed_eq": np.array(m.q_feed_eq()), "y_end": y1,
+           "t_stop": np.array(sr.duration), "stopped_early": np.array(sr.stopped_early),
+           "stop_value": np.array(m.stop_metric(sr.duration, y1)),
+           "solver": np.array(json.dumps({kk: (vv.item() if isinstance(vv, np.generic) else vv)
+                                          for kk, vv in sr.solver.items()}))}
+    np.savez_compressed(os.path.join(HERE, "stop_young2021.npz"), **out)
+    print("stop golden:", sr.duration, sr.stopped_early, out["stop_value"], sr.solver, flush=True)
+
+
 if __name__ == "__main__":
     if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
         raise SystemExit("usage: make_golden.py <reference checkout> [--outlet | --bench-state | "
-                         "--bench-state-heating | --cycle [--rtol X]]")
+                         "--bench-state-heating | --cycle [--rtol X] | --stop | --csv]")
     root = sys.argv[1]
-    if "--cycle" in sys.argv:
+    if "--stop" in sys.argv:
+        make_stop_golden(root)
+    elif "--csv" in sys.argv:
+        make_csv_golden(root)
+    elif "--cycle" in sys.argv:
         rt = float(sys.argv[sys.argv.index("--rtol") + 1]) if "--rtol" in sys.argv else None
         make_cycle_golden(root, rtol=rt)
     elif "--outlet" in sys.argv:
