@@ -120,6 +120,7 @@ SIGNATURES = [
     ("dv_stage_residual", C.c_int, [P, D, P, D, P, P, P]),
     ("dv_rhs_diag", C.c_int, [P, D, P, P, P]),
     ("dv_outlet_row", C.c_int, [P, D, P, D, P, P]),
+    ("dv_precond_partitions", C.c_int, [P, C.POINTER(I32), C.POINTER(I32), P, I32, C.POINTER(I32)]),
     ("dv_colour_columns", C.c_int, [I32, I32, I32, I32, P, C.POINTER(I32)]),
     ("dv_fd_jacobian", C.c_int, [P, D, P, P, P, P]),
     ("dv_precond_factor", C.c_int, [P, P, D, I32, P]),
@@ -134,6 +135,7 @@ SIGNATURES = [
     ("dv_integrator_copy_y", C.c_int, [P, P, P]),
     ("dv_rhs_acc_noalloc", C.c_int, [C.POINTER(DvStepParams), P, P, P, D, P, P, P, P]),
     ("dv_selftest_wait_timeout", C.c_int, [I32, C.POINTER(I32)]),
+    ("dv_model_flag_wait_timeout", C.c_int, [P, I32]),
     ("dv_mlp_create", C.c_int, [I64, C.c_uint64, C.POINTER(P)]),
     ("dv_mlp_destroy", C.c_int, [P]),
     ("dv_mlp_reserve", C.c_int, [P, I64]),

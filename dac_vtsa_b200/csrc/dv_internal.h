@@ -9,6 +9,11 @@ namespace dv {
 
 void set_error(const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+// DV_OK after a successful launch, else the launch error as DV_ERR_CUDA.
+inline int launch_ok(const char* what) {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DV_OK : cuda_fail(e, what);
+}
 
 // Launch accounting: every kernel launch of the library goes through DV_LAUNCH, which counts it per
 // kind and, when profiling is on (dv_profile_enable), brackets it with CUDA events on its stream.
@@ -145,6 +150,11 @@ int launch_spmv32(dv_model* m, const double* u, const double* sc, double dh, con
 // linear algebra (dv_linalg.cu)
 int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s);
 int64_t precond_doubles(int nb, int nparts, int Nz);
+// Partition mode, twisted separator plane and block size of every partition of the current factors
+// (nb_out up to cap entries); returns the number of partitions (0 before the first factorisation).
+int precond_partitions(const dv_model* m, int* mode, int* zs, int* nb_out, int cap);
+// Largest block, partition count and storage over the partition modes a model of p can factorise.
+void precond_capacity(const dv_step_params& p, int* cap_nb, int* cap_parts, int64_t* pc_need, int64_t* work_need);
 int64_t precond_work_doubles(int nb, int nparts, int Nz);
 // x = diag(1/sc) M^-1 diag(sc) b  (sc may be NULL: plain solve)
 int precond_apply(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s);

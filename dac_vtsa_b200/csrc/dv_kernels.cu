@@ -762,7 +762,7 @@ int launch_outlet(dv_model* m, double t, const double* y, double c_feed, double*
     DV_TRY(launch_diag(m, t, y, m->d_diag, s));
     Rec rec = make_rec(m->rl, m->d_diag);
     DV_LAUNCH(dv::K_RESIDUAL, s, k_outlet<<<1, OUTLET_THREADS, 0, s>>>(m->p, rec, y, c_feed, row));
-    return cuda_fail(cudaGetLastError(), "k_outlet");
+    return launch_ok("k_outlet");
 }
 
 }  // namespace dv

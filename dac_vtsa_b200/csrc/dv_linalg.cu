@@ -33,18 +33,46 @@ namespace dv {
 
 struct PcGeom {
     int Nr, Nth, Nz, wall, mode, nb, nparts, ld;
+    int rg, tg;            // mode 3: ring groups per sector (rings 1..Nr-1), theta groups of the core ring
     int zs;                // twisted factorisation: separator planes zs, zs+1 (0: one direction, top-down)
     int ncv;               // cell unknowns (6 per cell) of the partition; nb - ncv wall nodes follow
     int64_t nc, bs;        // bs: block stride in doubles (nb*ld rounded up to even: 16-byte multiple)
 };
 
+// Mode 3 (mode 2 split for large cross-sections): contiguous groups of n items in G groups, the
+// first n % G groups one item larger.  Ring groups cover rings 1..Nr-1 of a sector (the wall node
+// goes with the outermost, smallest group); theta groups cover the sectors of the core ring.
+static __host__ __device__ __forceinline__ void pc_group(int n, int G, int gi, int& a0, int& a1) {
+    const int base = n / G, extra = n % G;
+    a0 = gi * base + (gi < extra ? gi : extra);
+    a1 = a0 + base + (gi < extra ? 1 : 0);
+}
+static __host__ __device__ __forceinline__ int pc_group_of(int n, int G, int t) {
+    const int base = n / G, extra = n % G;
+    return (t < extra * (base + 1)) ? t / (base + 1) : extra + (t - extra * (base + 1)) / base;
+}
+
 // Geometry as seen by one partition: nb and ncv of that partition (ld, bs and strides stay the
 // largest partition's).  Mode 2: parts 0..Nth-1 are sectors (rings 1..Nr-1 + wall), part Nth the core.
+// Mode 3: part j*rg + gi is ring group gi of sector j (+ the wall in the last group), part
+// Nth*rg + h theta group h of the core ring.
 static __host__ __device__ __forceinline__ PcGeom pc_part(const PcGeom& g, int part) {
     PcGeom q = g;
     if (g.mode == 2) {
         if (part == g.Nth) { q.ncv = DV_NV * g.Nth; q.nb = q.ncv; }
         else { q.ncv = DV_NV * (g.Nr - 1); q.nb = q.ncv + (g.wall ? 1 : 0); }
+    } else if (g.mode == 3) {
+        int a0, a1;
+        if (part >= g.Nth * g.rg) {
+            pc_group(g.Nth, g.tg, part - g.Nth * g.rg, a0, a1);
+            q.ncv = DV_NV * (a1 - a0);
+            q.nb = q.ncv;
+        } else {
+            const int gi = part % g.rg;
+            pc_group(g.Nr - 1, g.rg, gi, a0, a1);
+            q.ncv = DV_NV * (a1 - a0);
+            q.nb = q.ncv + ((g.wall && gi == g.rg - 1) ? 1 : 0);
+        }
     }
     return q;
 }
@@ -53,6 +81,8 @@ static __host__ __device__ __forceinline__ PcGeom pc_part(const PcGeom& g, int p
 static __device__ __forceinline__ int pc_part_of(const PcGeom& g, int i, int j) {
     if (g.mode == 0) return j;
     if (g.mode == 2) return (i == 0) ? g.Nth : j;
+    if (g.mode == 3)
+        return (i == 0) ? g.Nth * g.rg + pc_group_of(g.Nth, g.tg, j) : j * g.rg + pc_group_of(g.Nr - 1, g.rg, i - 1);
     return 0;
 }
 
@@ -73,6 +103,21 @@ static inline int pc_lds(int nb, size_t budget) {
 
 static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int k, int l) {
     const int64_t offw = (int64_t)DV_NV * g.nc;
+    if (g.mode == 3) {
+        int a0, a1;
+        if (part >= g.Nth * g.rg) {             // core theta group: (sector j, var v) of ring 0
+            pc_group(g.Nth, g.tg, part - g.Nth * g.rg, a0, a1);
+            const int j = a0 + l / DV_NV, v = l % DV_NV;
+            return (int64_t)v * g.nc + (int64_t)j * g.Nz + k;
+        }
+        const int j = part / g.rg, gi = part % g.rg;
+        pc_group(g.Nr - 1, g.rg, gi, a0, a1);
+        if (l < DV_NV * (a1 - a0)) {            // rings 1 + a0 .. 1 + a1 - 1 of sector j
+            const int i = 1 + a0 + l / DV_NV, v = l % DV_NV;
+            return (int64_t)v * g.nc + ((int64_t)i * g.Nth + j) * g.Nz + k;
+        }
+        return offw + (int64_t)j * g.Nz + k;
+    }
     if (g.mode == 2) {
         if (part == g.Nth) {                    // core: (sector j, var v) of ring 0
             const int j = l / DV_NV, v = l % DV_NV;
@@ -100,6 +145,19 @@ static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int
 
 // local index of (cell (i, j), var v) / wall (j) inside its partition
 static __device__ __forceinline__ int pc_local(const PcGeom& g, int i, int j, int v) {
+    if (g.mode == 3) {
+        int a0, a1;
+        if (v == DV_NV) {                       // the wall node follows the cells of the outer group
+            pc_group(g.Nr - 1, g.rg, g.rg - 1, a0, a1);
+            return DV_NV * (a1 - a0);
+        }
+        if (i == 0) {
+            pc_group(g.Nth, g.tg, pc_group_of(g.Nth, g.tg, j), a0, a1);
+            return (j - a0) * DV_NV + v;
+        }
+        pc_group(g.Nr - 1, g.rg, pc_group_of(g.Nr - 1, g.rg, i - 1), a0, a1);
+        return (i - 1 - a0) * DV_NV + v;
+    }
     if (g.mode == 2) {
         if (v == DV_NV) return DV_NV * (g.Nr - 1);
         return (i == 0) ? j * DV_NV + v : (i - 1) * DV_NV + v;
@@ -1289,16 +1347,49 @@ __global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const TS* __r
     }
 }
 
-static PcGeom geom_of(const dv_model* m, int mode) {
+// Largest partition of mode 3 the shared-memory kernels take at their tuned size.
+#define PC_SPLIT_NB 48
+
+static PcGeom geom_of_params(const dv_step_params& p, int mode) {
     PcGeom g;
-    g.Nr = m->p.Nr;
-    g.Nth = m->p.Nth;
-    g.Nz = m->p.Nz;
-    g.wall = m->p.wall_on;
+    g.Nr = p.Nr;
+    g.Nth = p.Nth;
+    g.Nz = p.Nz;
+    g.wall = p.wall_on;
+    g.rg = g.tg = 1;
     // mode 2 needs a second ring and a second sector; below that it is mode 0 (or 1 for one sector)
-    if (mode == 2 && (m->p.Nr < 2 || m->p.Nth < 2)) mode = 0;
-    g.mode = (m->p.Nth > 1 && (mode == 0 || mode == 2)) ? mode : 1;
-    g.nc = m->nc;
+    if (mode == 2 && (p.Nr < 2 || p.Nth < 2)) mode = 0;
+    g.mode = (p.Nth > 1 && (mode == 0 || mode == 2)) ? mode : 1;
+    g.nc = (int64_t)p.Nr * p.Nth * p.Nz;
+    static const bool split_ok = [] {
+        const char* e = getenv("DVTSA_PC_SPLIT");
+        return !(e && e[0] == '0');
+    }();
+    if (g.mode == 2 && split_ok && std::max(DV_NV * (g.Nr - 1) + (g.wall ? 1 : 0), DV_NV * g.Nth) > PC_SMEM_NB) {
+        // too large for the shared-memory kernels: split the sectors into ring groups and the core
+        // ring into theta groups of at most PC_SPLIT_NB unknowns (mode 3)
+        g.mode = 3;
+        auto nb_ring = [&](int G) {
+            int worst = 0;
+            for (int gi = 0; gi < G; ++gi) {
+                int a0, a1;
+                pc_group(g.Nr - 1, G, gi, a0, a1);
+                worst = std::max(worst, DV_NV * (a1 - a0) + ((g.wall && gi == G - 1) ? 1 : 0));
+            }
+            return worst;
+        };
+        g.rg = 1;
+        while (g.rg < g.Nr - 1 && nb_ring(g.rg) > PC_SPLIT_NB) ++g.rg;
+        g.tg = 1;
+        while (g.tg < g.Nth && DV_NV * ((g.Nth + g.tg - 1) / g.tg) > PC_SPLIT_NB) ++g.tg;
+        g.nb = std::max(nb_ring(g.rg), DV_NV * ((g.Nth + g.tg - 1) / g.tg));
+        g.ncv = g.nb;
+        g.nparts = g.Nth * g.rg + g.tg;
+        g.ld = pc_ld(g.nb);
+        g.bs = (((int64_t)g.nb * g.ld + 1) / 2) * 2;
+        g.zs = 0;
+        return g;
+    }
     if (g.mode == 0) {
         g.nb = DV_NV * g.Nr + (g.wall ? 1 : 0);
         g.ncv = DV_NV * g.Nr;
@@ -1317,6 +1408,33 @@ static PcGeom geom_of(const dv_model* m, int mode) {
     g.bs = (((int64_t)g.nb * g.ld + 1) / 2) * 2;
     g.zs = 0;
     return g;
+}
+
+static PcGeom geom_of(const dv_model* m, int mode) { return geom_of_params(m->p, mode); }
+
+void precond_capacity(const dv_step_params& p, int* cap_nb, int* cap_parts, int64_t* pc_need, int64_t* work_need) {
+    int nb = 0, parts = 0;
+    int64_t need = 0;
+    for (int mode : {0, 1, 2}) {
+        const PcGeom g = geom_of_params(p, mode);
+        if (g.mode == 1 && g.nb > 512) continue;       // whole cross-sections only up to 512 unknowns
+        nb = std::max(nb, g.nb);
+        parts = std::max(parts, g.nparts);
+        need = std::max(need, precond_doubles(g.nb, g.nparts, g.Nz));
+    }
+    *cap_nb = nb;
+    *cap_parts = parts;
+    *pc_need = need;
+    *work_need = precond_work_doubles(nb, parts, p.Nz);
+}
+
+int precond_partitions(const dv_model* m, int* mode, int* zs, int* nb_out, int cap) {
+    if (!m->pc_ready) return 0;
+    const PcGeom g = geom_of(m, m->pc_mode);
+    *mode = g.mode;
+    *zs = m->pc_zs;
+    for (int q = 0; q < g.nparts && q < cap; ++q) nb_out[q] = pc_part(g, q).nb;
+    return g.nparts;
 }
 
 // the geometry the current factors were computed with

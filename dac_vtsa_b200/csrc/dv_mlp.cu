@@ -236,7 +236,7 @@ static int gemm(const GemmP& g, int grid, cudaStream_t s) {
         attr = true;
     }
     DV_LAUNCH(dv::K_MLP, s, k_gemm<<<grid, 128, GEMM_SMEM_ALLOC, s>>>(g));
-    return cuda_fail(cudaGetLastError(), "k_gemm");
+    return launch_ok("k_gemm");
 }
 
 // ------------------------------------------------------------------------------------ features
@@ -441,7 +441,7 @@ static unsigned g1(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b);
 static int pack(dv_mlp* net, cudaStream_t s) {
     DV_LAUNCH(dv::K_MLP, s, k_pack_weights<<<g1((int64_t)NH * NIN), 256, 0, s>>>(net->P, net->W1, net->W2, net->W3,
                                                                                  net->W4, net->W2t, net->W3t, net->W4t));
-    return cuda_fail(cudaGetLastError(), "k_pack_weights");
+    return launch_ok("k_pack_weights");
 }
 
 static GemmP base(dv_mlp* net) {
@@ -496,7 +496,7 @@ static int grad_batch(dv_mlp* net, int64_t rows_valid, cudaStream_t s) {
     w.A = net->H3t; w.B = net->D4t; w.rb = NOUT; w.N = NOUT; w.of = net->part + 3 * PS;
     DV_TRY(gemm(w, NSPLIT, s));
     DV_LAUNCH(dv::K_MLP, s, k_collect_grad<<<g1(NPARAM), 256, 0, s>>>(net->part, net->bpart, net->G));
-    return cuda_fail(cudaGetLastError(), "k_collect_grad");
+    return launch_ok("k_collect_grad");
 }
 
 static int forward_rows(dv_mlp* net, const bf16* X, int64_t rows, int64_t rows_valid, float* out, cudaStream_t s) {
@@ -525,14 +525,14 @@ int predict(dv_mlp* net, const StageInputs& in, const double* ytr, double* pred,
     DV_CUDA(cudaGetLastError());
     DV_TRY(forward_rows(net, net->Xi, rows, in.nc, net->Oi, s));
     DV_LAUNCH(dv::K_MLP, s, k_apply<<<g1(in.nc), 256, 0, s>>>(in, net->norm, net->Oi, ytr, pred));
-    return cuda_fail(cudaGetLastError(), "k_apply");
+    return launch_ok("k_apply");
 }
 
 int record_features(dv_mlp* net, const StageInputs& in, int64_t first, int64_t stride, int64_t cnt, cudaStream_t s) {
     if (net->count + cnt > net->cap) return DV_OK;
     DV_LAUNCH(dv::K_MLP, s, k_features<<<g1(cnt, 128), 128, 0, s>>>(in, net->norm, first, stride, cnt, net->Xs, net->cap,
                                                                       net->count));
-    return cuda_fail(cudaGetLastError(), "k_features");
+    return launch_ok("k_features");
 }
 
 int record_targets(dv_mlp* net, const StageInputs& in, const double* zstar, const double* zext, int64_t first,

@@ -1801,11 +1801,21 @@ static int predict_stage(dv_integrator* g, const mlp::StageInputs& in, double t,
 }
 
 // A bounded device wait that gave up leaves a flag in the model; surface it as an error.
+// After a reported timeout nothing of the abandoned wait is in flight (the caller synchronised):
+// clear the error word and the ticket counters the abandoned reduction or barrier left behind, so
+// the model's next call starts clean.
+static void clear_device_error(dv_model* m) {
+    cudaMemset(m->d_err, 0, sizeof(int));
+    if (m->W && m->W->tickets) cudaMemset(m->W->tickets, 0, 16 * sizeof(unsigned));
+    cudaDeviceSynchronize();
+}
+
 static int check_device_error(dv_model* m) {
     int e = 0;
     DV_CUDA(cudaMemcpy(&e, m->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e != 0) {
         set_error(device_error_text(e));
+        clear_device_error(m);
         return DV_ERR_CUDA;
     }
     return DV_OK;
@@ -1841,6 +1851,12 @@ int dv_selftest_wait_timeout(int32_t polls, int32_t* bits) {
     if (rc != DV_OK) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "dv_selftest_wait_timeout");
     *bits = h;
+    return DV_OK;
+}
+
+int dv_model_flag_wait_timeout(dv_model* m, int32_t bits) {
+    if (!m || bits <= 0) { set_error("dv_model_flag_wait_timeout: bad argument"); return DV_ERR_ARG; }
+    DV_CUDA(cudaMemcpy(m->d_err, &bits, sizeof(int), cudaMemcpyHostToDevice));
     return DV_OK;
 }
 
@@ -1928,6 +1944,14 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     int64_t pc_need = std::max(precond_doubles(nb_sector, p->Nth, p->Nz),
                                full_ok ? precond_doubles(nb_full, 1, p->Nz) : (int64_t)0);
     if (nb_ring) pc_need = std::max(pc_need, precond_doubles(nb_ring, p->Nth + 1, p->Nz));
+    {   // the split partitions (mode 3) that large cross-sections use instead of mode 2
+        int cnb = 0, cparts = 0;
+        int64_t cneed = 0, cwork = 0;
+        precond_capacity(*p, &cnb, &cparts, &cneed, &cwork);
+        m->pc_cap_nb = std::max(m->pc_cap_nb, cnb);
+        m->pc_cap_parts = std::max(m->pc_cap_parts, cparts);
+        pc_need = std::max(pc_need, cneed);
+    }
     int64_t work_need = precond_work_doubles(m->pc_cap_nb, m->pc_cap_parts, p->Nz);
     const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
     bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
@@ -2033,6 +2057,17 @@ int dv_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, dou
 int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, void* stream) {
     if (!m || !J) { set_error("null argument"); return DV_ERR_ARG; }
     return precond_factor(m, J, dh, mode, (cudaStream_t)stream);
+}
+
+int dv_precond_partitions(const dv_model* m, int32_t* mode, int32_t* zs, int32_t* nb, int32_t cap, int32_t* nparts) {
+    if (!m || !mode || !zs || !nparts || (cap > 0 && !nb)) { set_error("null argument"); return DV_ERR_ARG; }
+    int md = -1, z = 0;
+    std::vector<int> tmp(std::max(cap, 0));
+    *nparts = precond_partitions(m, &md, &z, tmp.data(), cap);
+    *mode = md;
+    *zs = z;
+    for (int q = 0; q < cap && q < *nparts; ++q) nb[q] = tmp[q];
+    return DV_OK;
 }
 
 int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream) {
@@ -2450,6 +2485,8 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         *rep = R;
         if (*g->h_err != 0) {                 // (read with the error norm; the rest of the step has no wait)
             set_error(device_error_text(*g->h_err));
+            *g->h_err = 0;
+            clear_device_error(m);
             return DV_ERR_CUDA;
         }
         return DV_OK;

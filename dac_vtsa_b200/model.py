@@ -333,6 +333,14 @@ class TVSAModel:
             check(self.lib.dv_precond_factor(self.handle, _ptr(J_block), float(dh), PRECOND_MODES[mode],
                                              _stream()), "dv_precond_factor")
 
+    def precond_partitions(self):
+        """(mode, first twisted separator plane, block size of every partition) of the stored factors."""
+        mode, zs, npart = C.c_int32(), C.c_int32(), C.c_int32()
+        nb = np.zeros(4096, dtype=np.int32)
+        check(self.lib.dv_precond_partitions(self.handle, C.byref(mode), C.byref(zs), nb.ctypes.data, nb.size,
+                                             C.byref(npart)), "dv_precond_partitions")
+        return mode.value, zs.value, nb[:npart.value].tolist()
+
     def precond_solve(self, b):
         """x = M^-1 b with the stored factors (the reference's lu.solve)."""
         with torch.cuda.device(self.device):

@@ -7,7 +7,7 @@
  *   FDJacobian (core/jacobian.py:21-91), color_columns (numerics/sparsity.py:88-107)
  *                                        -> dv_colour_columns, dv_fd_jacobian
  *   TRBDF2._factor / splu (core/solver.py:334-337)
- *                                        -> dv_precond_factor, dv_precond_solve
+ *                                        -> dv_precond_factor, dv_precond_solve, dv_precond_partitions
  *   newton_krylov (core/solver.py:154-294) -> dv_newton_stage
  *   TRBDF2.integrate (core/solver.py:370-511) -> dv_integrator_*
  * Each entry point below names the reference interface it replaces.
@@ -206,6 +206,12 @@ int dv_precond_factor(dv_model* m, const double* J, double dh, int32_t mode, voi
 #define DV_KRYLOV_FP32_FACTORS 1
 #define DV_KRYLOV_FP32_OPERATOR 2
 int dv_model_set_krylov_fp32(dv_model* m, int32_t mask);
+/* Layout of the stored factors (no reference counterpart; for accounting): partition mode (3 = the
+ * split form mode 2 takes when a sector or the core ring exceeds the shared-memory kernels: rings
+ * 1.. of each sector in groups of at most 48 unknowns, the wall node with the outer group, and the
+ * core ring in theta groups), the first twisted separator plane (0: one direction), and each
+ * partition's block size (up to cap entries).  Host call. */
+int dv_precond_partitions(const dv_model* m, int32_t* mode, int32_t* zs, int32_t* nb, int32_t cap, int32_t* nparts);
 /* x = M^-1 b with the stored factors (lu.solve). b and x may alias. */
 int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream);
 
@@ -319,7 +325,9 @@ int dv_integrator_set_predictor(dv_integrator* g, dv_mlp* net, int32_t predict, 
  * f (n_core), acc (DV_NACC).  The face and wall records live in a static 2 MiB device array per
  * device (enough for 16x16x64); larger grids are rejected with DV_ERR_ARG.  The first call on a
  * device looks up that array's address with the device current; make that first call before any
- * stream capture.  Each call clears the part it uses on `stream` before its kernels run.  Every
+ * stream capture.  The address is kept for the life of the process: a device reset (cudaDeviceReset)
+ * after the first call on that device is not supported.  Each call clears the part it uses on
+ * `stream` before its kernels run.  Every
  * call on a device shares the array: calls that overlap on the GPU (other streams, other threads)
  * race and must be serialised by the caller.  Asynchronous on `stream`. */
 int dv_rhs_acc_noalloc(const dv_step_params* p, const double* feed_flux, const double* n_nom,
@@ -332,6 +340,11 @@ int dv_rhs_acc_noalloc(const dv_step_params* p, const double* feed_flux, const d
  * bulk-copy wait, 4: the grid barrier; 5 when both timed out as they must).  The waits return,
  * so the CUDA context stays usable.  Synchronous; allocates 16 bytes of device memory. */
 int dv_selftest_wait_timeout(int32_t polls, int32_t* bits);
+/* Failure-injection hook on the host (no reference counterpart): sets the model's device error word
+ * to `bits` as a bounded wait that gave up would.  The model's next synchronising call reports
+ * DV_ERR_CUDA with the wait named, then clears the word and the reduction tickets the abandoned wait
+ * left, so the call after that runs normally. */
+int dv_model_flag_wait_timeout(dv_model* m, int32_t bits);
 
 #ifdef __cplusplus
 }

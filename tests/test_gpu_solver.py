@@ -23,20 +23,55 @@ def _partition_of(m, mode):
     if mode == "sector":
         return sector
     if mode == "theta_block":
-        return np.where(ring == 0, g.Nth, sector)
+        split = _split_groups(g.Nr, g.Nth, m.n_w > 0)
+        if split is None:
+            return np.where(ring == 0, g.Nth, sector)
+        rg, tg = split
+        ring_group = np.array([_group_of(g.Nr - 1, rg, i - 1) if i > 0 else 0 for i in range(g.Nr)])
+        theta_group = np.array([_group_of(g.Nth, tg, j) for j in range(g.Nth)])
+        return np.where(ring == 0, g.Nth * rg + theta_group[sector], sector * rg + ring_group[ring])
     return np.zeros_like(idx)
 
 
-def _pc_model(Nz, Nr=3):
-    """Nr x 4 x Nz bed and a state: the golden Jacobian state for 3 x 4 x 6, else a seeded state."""
+def _group_of(n, G, t):
+    base, extra = n // G, n % G
+    return t // (base + 1) if t < extra * (base + 1) else extra + (t - extra * (base + 1)) // base
+
+
+def _split_groups(Nr, Nth, wall, limit=56, target=48):
+    """(ring groups, theta groups) of the split theta_block partitions, or None when the sectors
+    and the core ring fit the shared-memory kernels whole: rings 1..Nr-1 of a sector in the fewest
+    contiguous groups (larger groups inside, the wall node with the outermost) of at most `target`
+    unknowns, the core ring's sectors likewise."""
+    if Nr < 2 or Nth < 2 or max(6 * (Nr - 1) + (1 if wall else 0), 6 * Nth) <= limit:
+        return None
+
+    def ring_nb(G):
+        n, out = Nr - 1, 0
+        base, extra = n // G, n % G
+        for gi in range(G):
+            size = base + (1 if gi < extra else 0)
+            out = max(out, 6 * size + (1 if (wall and gi == G - 1) else 0))
+        return out
+    rg = 1
+    while rg < Nr - 1 and ring_nb(rg) > target:
+        rg += 1
+    tg = 1
+    while tg < Nth and 6 * -(-Nth // tg) > target:
+        tg += 1
+    return rg, tg
+
+
+def _pc_model(Nz, Nr=3, Nth=4):
+    """Nr x Nth x Nz bed and a state: the golden Jacobian state for 3 x 4 x 6, else a seeded state."""
     from dac_vtsa_b200.model import TVSAModel
-    if Nz == 6 and Nr == 3:
+    if Nz == 6 and Nr == 3 and Nth == 4:
         d = golden("jacobian_3x4x6.npz")
         m, _ = build(TVSAModel, {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6}, 0, d["P0"])
         return m, d["y"]
     from dac_vtsa_b200 import host
     from dac_vtsa_b200.config import load_config
-    cfg = load_config(override_dict={"grid.Nr": Nr, "grid.Ntheta": 4, "grid.Nz": Nz})
+    cfg = load_config(override_dict={"grid.Nr": Nr, "grid.Ntheta": Nth, "grid.Nz": Nz})
     g = host.Grid.from_config(cfg)
     props = host.get_backend(cfg)
     st = host.seeded_state(cfg, g, props, seed=3, amplitude=0.05)
@@ -84,8 +119,19 @@ def test_preconditioner_exact_on_dominant_system_8_rings(mode):
     _check_dominant(mode, 12, 8)
 
 
-def _check_dominant(mode, Nz, Nr):
-    m, _ = _pc_model(Nz, Nr)
+# beds whose theta_block partitions exceed the shared-memory kernels: 11 rings (sector rings split
+# 5 + 5, the wall with the outer group), 10 sectors (core ring split 5 + 5), and the 16 x 16 cross-
+# section (rings 8 + 7 + wall, core 8 + 8 sectors)
+@pytest.mark.parametrize("Nr,Nth,Nz", [(11, 4, 9), (3, 10, 12), (16, 16, 8)])
+def test_split_partitions_exact_on_dominant_system(Nr, Nth, Nz):
+    """Large cross-sections factorise split partitions (ring groups per sector, theta groups of the
+    core ring): the solve equals a sparse LU of I - J restricted to exactly those partitions."""
+    assert _split_groups(Nr, Nth, True) is not None
+    _check_dominant("theta_block", Nz, Nr, Nth)
+
+
+def _check_dominant(mode, Nz, Nr, Nth=4):
+    m, _ = _pc_model(Nz, Nr, Nth)
     Jd, Jc = _dominant_jacobian(m, 40 + Nz)
     m.precond_factor(Jd, 1.0, mode)
     M = _restricted(m, Jc, mode, 1.0)
