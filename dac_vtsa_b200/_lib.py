@@ -93,6 +93,10 @@ class DvSolverOpts(C.Structure):
                 ("h_max", D), ("h_init", D)]
 
 
+class DvTuning(C.Structure):
+    _fields_ = [("gmres_prefix", I32), ("sweep_nbuf", I32), ("spmv_block", I32), ("fdjac_block", I32)]
+
+
 class DvStepReport(C.Structure):
     _fields_ = [("t", D), ("h_used", D), ("err_norm", D),
                 ("n_steps", I64), ("n_reject", I64), ("n_newton_fail", I64), ("n_krylov", I64), ("n_jac", I64),
@@ -136,6 +140,9 @@ SIGNATURES = [
     ("dv_rhs_acc_noalloc", C.c_int, [C.POINTER(DvStepParams), P, P, P, D, P, P, P, P]),
     ("dv_selftest_wait_timeout", C.c_int, [I32, C.POINTER(I32)]),
     ("dv_model_flag_wait_timeout", C.c_int, [P, I32]),
+    ("dv_model_set_tuning", C.c_int, [P, C.POINTER(DvTuning)]),
+    ("dv_model_get_tuning", C.c_int, [P, C.POINTER(DvTuning)]),
+    ("dv_autotune", C.c_int, [P, D, P, D, I32, C.POINTER(DvTuning), P, I32, P]),
     ("dv_mlp_create", C.c_int, [I64, C.c_uint64, C.POINTER(P)]),
     ("dv_mlp_destroy", C.c_int, [P]),
     ("dv_mlp_reserve", C.c_int, [P, I64]),

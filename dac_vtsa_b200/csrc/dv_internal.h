@@ -65,7 +65,7 @@ struct Work {
     cudaGraph_t gm_graph = nullptr;
     cudaGraphExec_t gm_exec = nullptr;
     cudaStream_t gm_cs = nullptr;             // capture stream
-    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1, gm_op32 = -1;
+    int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1, gm_op32 = -1, gm_tuned = -2;
     int gm_prefix = 0;                        // Arnoldi steps captured ahead of the WHILE node
     int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
@@ -126,6 +126,7 @@ struct dv_model {
     dv::Work* W;                    // Krylov / Newton workspace (allocated at creation)
     double* d_atol7;                // per-block absolute tolerances (device)
     int ncolours;                   // colours of the Jacobian pattern (counts RHS-equivalents)
+    dv_tuning tune;                 // launch parameters (dv_model_set_tuning / dv_autotune)
 };
 
 namespace dv {

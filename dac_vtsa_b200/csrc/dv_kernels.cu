@@ -634,16 +634,20 @@ int matvec_capture(dv_model* m, const double* dargs, const double* z, const doub
     return DV_OK;
 }
 
+static int fdjac_block(const dv_model* m) { return m->tune.fdjac_block == 64 ? 64 : 128; }
+
 int launch_fd_jacobian(dv_model* m, double t, const double* y, const double* f0, double* J, cudaStream_t s) {
-    dim3 grid(nblk(m->nc, 128), DV_NSLOT * DV_NB);
-    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<double><<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
+    const int bl = fdjac_block(m);
+    dim3 grid(nblk(m->nc, bl), DV_NSLOT * DV_NB);
+    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<double><<<grid, bl, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }
 
 int launch_fd_jacobian32(dv_model* m, double t, const double* y, const double* f0, float* J, cudaStream_t s) {
-    dim3 grid(nblk(m->nc, 128), DV_NSLOT * DV_NB);
-    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<float><<<grid, 128, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
+    const int bl = fdjac_block(m);
+    dim3 grid(nblk(m->nc, bl), DV_NSLOT * DV_NB);
+    DV_LAUNCH(dv::K_FDJAC, s, k_fd_jacobian<float><<<grid, bl, 0, s>>>(m->p, aux_of(m), t, y, f0, J));
     DV_CUDA(cudaGetLastError());
     return DV_OK;
 }

@@ -1556,7 +1556,10 @@ static size_t apply_smem(const PcGeom& g, int nbuf, size_t tsize) {
 static size_t pc_tsize(const dv_model* m) { return m->pc_fp32 ? sizeof(float) : sizeof(double); }
 
 // ring depth: three stages in flight when they fit in shared memory, else two
-static int apply_nbuf(const PcGeom& g, size_t tsize) { return apply_smem(g, 3, tsize) <= (size_t)smem_optin() ? 3 : 2; }
+static int apply_nbuf(const PcGeom& g, size_t tsize, int want = 0) {
+    const bool three = apply_smem(g, 3, tsize) <= (size_t)smem_optin();
+    return (three && want != 2) ? 3 : 2;
+}
 
 template <int NJ, int NBUF, typename TS, bool TW>
 static void launch_apply_tw(const PcGeom& g, dv_model* m, const TS* A, const double* b, const double* sc, double* x,
@@ -1581,10 +1584,10 @@ template <int NJ>
 static void launch_apply_nj(const PcGeom& g, dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
                             const PaFuse& F, bool count) {
     if (m->pc_fp32) {               // factors stored in FP32 (mixed-precision Krylov), products in FP64
-        if (apply_nbuf(g, sizeof(float)) == 3) launch_apply_k<NJ, 3, float>(g, m, m->d_pc32, b, sc, x, s, F, count);
+        if (apply_nbuf(g, sizeof(float), m->tune.sweep_nbuf) == 3) launch_apply_k<NJ, 3, float>(g, m, m->d_pc32, b, sc, x, s, F, count);
         else launch_apply_k<NJ, 2, float>(g, m, m->d_pc32, b, sc, x, s, F, count);
     } else {
-        if (apply_nbuf(g, sizeof(double)) == 3) launch_apply_k<NJ, 3, double>(g, m, m->d_pc, b, sc, x, s, F, count);
+        if (apply_nbuf(g, sizeof(double), m->tune.sweep_nbuf) == 3) launch_apply_k<NJ, 3, double>(g, m, m->d_pc, b, sc, x, s, F, count);
         else launch_apply_k<NJ, 2, double>(g, m, m->d_pc, b, sc, x, s, F, count);
     }
 }
@@ -1647,7 +1650,7 @@ int precond_apply_capture(dv_model* m, const double* b, const double* sc, double
 // replaces the FP64 finite-difference matvec (core/solver.py:196-203) inside GMRES.  One thread per
 // cell computes its six rows and, for an outer-ring cell, its wall node's row.  Blocks known to be
 // structurally zero (loading rows of neighbour slots, the wall row of inner cells) are not read.
-__global__ void __launch_bounds__(128) k_spmv32(int Nr, int Nth, int Nz, int wall, const float* __restrict__ J,
+__global__ void __launch_bounds__(256) k_spmv32(int Nr, int Nth, int Nz, int wall, const float* __restrict__ J,
                                                 const double* __restrict__ u, const double* __restrict__ sc,
                                                 double dh, const double* __restrict__ dh_dev, double* __restrict__ out) {
     const int64_t nc = (int64_t)Nr * Nth * Nz;
@@ -1720,11 +1723,12 @@ __global__ void __launch_bounds__(128) k_spmv32(int Nr, int Nth, int Nz, int wal
 int launch_spmv32(dv_model* m, const double* u, const double* sc, double dh, const double* dh_dev, double* out,
                   cudaStream_t s, bool count) {
     const dv_step_params& p = m->p;
-    const unsigned grid = (unsigned)((m->nc + 127) / 128);
+    const int bl = (m->tune.spmv_block == 64 || m->tune.spmv_block == 256) ? m->tune.spmv_block : 128;
+    const unsigned grid = (unsigned)((m->nc + bl - 1) / bl);
     if (count) {
-        DV_LAUNCH(dv::K_SPMV, s, k_spmv32<<<grid, 128, 0, s>>>(p.Nr, p.Nth, p.Nz, p.wall_on, m->d_J32, u, sc, dh, dh_dev, out));
+        DV_LAUNCH(dv::K_SPMV, s, k_spmv32<<<grid, bl, 0, s>>>(p.Nr, p.Nth, p.Nz, p.wall_on, m->d_J32, u, sc, dh, dh_dev, out));
     } else {
-        k_spmv32<<<grid, 128, 0, s>>>(p.Nr, p.Nth, p.Nz, p.wall_on, m->d_J32, u, sc, dh, dh_dev, out);
+        k_spmv32<<<grid, bl, 0, s>>>(p.Nr, p.Nth, p.Nz, p.wall_on, m->d_J32, u, sc, dh, dh_dev, out);
     }
     DV_CUDA(cudaGetLastError());
     return DV_OK;

@@ -1221,7 +1221,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     // The first GM_PREFIX steps are plain nodes ahead of the WHILE node: every solve takes at least
     // two steps and most take five or more, and each pass through the WHILE body costs a device-side
     // relaunch (~20 us on B200) that a plain node does not; a step after the stop returns at once.
-    const int prefix = fused ? std::min(gmres_prefix(), kdim) : 0;
+    const int prefix = fused ? std::min(m->tune.gmres_prefix >= 0 ? m->tune.gmres_prefix : gmres_prefix(), kdim) : 0;
     if (e == cudaSuccess) {
         for (int q = 0; q < prefix && e == cudaSuccess; ++q) {
             if (arnoldi_step(cs) != DV_OK) e = cudaErrorUnknown;
@@ -1330,6 +1330,7 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
     W.gm_prefix = prefix;
     W.gm_fp32 = m->pc_fp32;
     W.gm_op32 = m->op32;
+    W.gm_tuned = m->tune.gmres_prefix;
     for (int k = 0; k < K_NKIND; ++k) {
         W.gm_fixed[k] = fixed[k];
         W.gm_iter[k] = iter[k];
@@ -1344,7 +1345,7 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
     dv_model* m = op.m;
     if (!W.gm_exec || W.gm_kdim != kdim || W.gm_mode != m->pc_mode || W.gm_nb != m->pc_nb ||
         W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32 || W.gm_zs != m->pc_zs ||
-        W.gm_op32 != m->op32)
+        W.gm_op32 != m->op32 || W.gm_tuned != m->tune.gmres_prefix)
         DV_TRY(gm_build(m, W, kdim));
     GmHost* hst = (GmHost*)W.gm_host;
     hst->args[0] = op.t;
@@ -1823,6 +1824,28 @@ static int check_device_error(dv_model* m) {
 }  // namespace dv
 using namespace dv;
 
+namespace {
+// time `reps` back-to-back runs of fn on stream s (CUDA events), microseconds per run
+template <class F>
+static int time_us(cudaStream_t s, int reps, F&& fn, double* out) {
+    cudaEvent_t a, b;
+    DV_CUDA(cudaEventCreate(&a));
+    DV_CUDA(cudaEventCreate(&b));
+    int rc = fn();                                   // warm-up (attributes, graph build)
+    if (rc == DV_OK) rc = cudaEventRecord(a, s) == cudaSuccess ? DV_OK : DV_ERR_CUDA;
+    for (int r = 0; r < reps && rc == DV_OK; ++r) rc = fn();
+    if (rc == DV_OK) rc = cudaEventRecord(b, s) == cudaSuccess ? DV_OK : DV_ERR_CUDA;
+    if (rc == DV_OK) rc = cudaEventSynchronize(b) == cudaSuccess ? DV_OK : DV_ERR_CUDA;
+    float ms = 0.0f;
+    if (rc == DV_OK) cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *out = 1e3 * ms / std::max(reps, 1);
+    return rc;
+}
+
+}  // namespace
+
 extern "C" {
 
 int dv_abi_version(void) { return DV_ABI_VERSION; }
@@ -1852,6 +1875,107 @@ int dv_selftest_wait_timeout(int32_t polls, int32_t* bits) {
     if (e != cudaSuccess) return cuda_fail(e, "dv_selftest_wait_timeout");
     *bits = h;
     return DV_OK;
+}
+
+int dv_model_set_tuning(dv_model* m, const dv_tuning* t) {
+    if (!m || !t || t->gmres_prefix < -1 || t->gmres_prefix > 8 || (t->sweep_nbuf != 0 && t->sweep_nbuf != 2 &&
+        t->sweep_nbuf != 3) || (t->spmv_block != 0 && t->spmv_block != 64 && t->spmv_block != 128 &&
+        t->spmv_block != 256) || (t->fdjac_block != 0 && t->fdjac_block != 64 && t->fdjac_block != 128)) {
+        set_error("dv_model_set_tuning: parameter outside its candidates");
+        return DV_ERR_ARG;
+    }
+    m->tune = *t;
+    return DV_OK;
+}
+
+int dv_model_get_tuning(const dv_model* m, dv_tuning* t) {
+    if (!m || !t) { set_error("null argument"); return DV_ERR_ARG; }
+    *t = m->tune;
+    return DV_OK;
+}
+
+int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps, dv_tuning* best, double* times_us,
+                int32_t ntimes, void* stream) {
+    if (!m || !y || !best || reps < 1 || dh <= 0.0) { set_error("dv_autotune: bad argument"); return DV_ERR_ARG; }
+    cudaStream_t st = (cudaStream_t)stream;
+    Work& W = *m->W;
+    const int64_t n = m->n;
+    double tm[DV_TUNE_NTIMES];
+    for (double& v : tm) v = 0.0;
+    const dv_tuning saved = m->tune;
+    dv_tuning tu = m->tune;
+    const int mode = m->pc_ready ? m->pc_mode : 2;
+    DV_TRY(launch_rhs(m, t, y, W.f, nullptr, st));
+    // FD Jacobian block size
+    const int fj[2] = {64, 128};
+    double bestv = INFINITY;
+    for (int q = 0; q < 2; ++q) {
+        m->tune.fdjac_block = fj[q];
+        DV_TRY(time_us(st, reps, [&] { return launch_fd_jacobian(m, t, y, W.f, W.J, st); }, &tm[q]));
+        if (tm[q] < bestv) { bestv = tm[q]; tu.fdjac_block = fj[q]; }
+    }
+    m->tune.fdjac_block = tu.fdjac_block;
+    DV_TRY(precond_factor(m, W.J, dh, mode, st));
+    // sweep ring depth (the shared-memory sweep only)
+    DV_CUDA(cudaMemcpyAsync(W.b, W.f, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    if (precond_apply_fusable(m)) {
+        bestv = INFINITY;
+        for (int q = 0; q < 2; ++q) {
+            m->tune.sweep_nbuf = 2 + q;
+            DV_TRY(time_us(st, reps, [&] { return precond_apply(m, W.b, nullptr, W.x, st); }, &tm[2 + q]));
+            if (tm[2 + q] < bestv) { bestv = tm[2 + q]; tu.sweep_nbuf = 2 + q; }
+        }
+        m->tune.sweep_nbuf = tu.sweep_nbuf;
+    }
+    // FP32 Jacobian product block size
+    DV_TRY(launch_fd_jacobian32(m, t, y, W.f, m->d_J32, st));
+    DV_LAUNCH(dv::K_VECTOR, st, k_scale<<<vgrid(n), VB, 0, st>>>(m->nc, n, y, m->d_atol7, 1e-4, W.s));
+    const int sb[3] = {64, 128, 256};
+    bestv = INFINITY;
+    for (int q = 0; q < 3; ++q) {
+        m->tune.spmv_block = sb[q];
+        DV_TRY(time_us(st, reps, [&] { return launch_spmv32(m, W.b, W.s, dh, nullptr, W.r, st); }, &tm[4 + q]));
+        if (tm[4 + q] < bestv) { bestv = tm[4 + q]; tu.spmv_block = sb[q]; }
+    }
+    m->tune.spmv_block = tu.spmv_block;
+    // GMRES prefix: whole stage solves z - dh f(t, z) = y from the explicit Euler guess
+    DV_LAUNCH(dv::K_VECTOR, st, k_xpay<<<vgrid(n), VB, 0, st>>>(n, y, dh, W.f, W.zt));
+    double* z0 = nullptr;
+    double* zo = nullptr;
+    DV_CUDA(cudaMalloc((void**)&z0, sizeof(double) * n));
+    DV_CUDA(cudaMalloc((void**)&zo, sizeof(double) * n));
+    DV_CUDA(cudaMemcpyAsync(z0, W.zt, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    dv_newton_opts no;
+    no.max_iter = 7;
+    no.krylov_dim = 30;
+    no.allow_refresh = 0;
+    no.precond_mode = mode;
+    no.kappa = 0.01;
+    no.eta = 1e-2;
+    no.rtol = 1e-4;
+    no.cons_tol = 0.0;
+    bestv = INFINITY;
+    int rc = DV_OK;
+    const int64_t nfev0 = m->nfev;
+    for (int q = 0; q < 5 && rc == DV_OK; ++q) {
+        m->tune.gmres_prefix = 2 * q;
+        rc = time_us(st, std::max(1, reps / 10), [&] {
+            dv_newton_result r;
+            memset(&r, 0, sizeof r);
+            NewtonCtx C{m, &W, m->d_atol7, n, (int64_t)(DV_NG + DV_NA) * m->nc, no, &r, nullptr};
+            return newton_krylov(C, t + dh, z0, y, dh, zo, st);
+        }, &tm[7 + q]);
+        if (rc == DV_OK && tm[7 + q] < bestv) { bestv = tm[7 + q]; tu.gmres_prefix = 2 * q; }
+    }
+    m->nfev = nfev0;
+    cudaFree(z0);
+    cudaFree(zo);
+    if (rc != DV_OK) { m->tune = saved; return rc; }
+    m->tune = tu;
+    *best = tu;
+    if (times_us)
+        for (int q = 0; q < ntimes && q < DV_TUNE_NTIMES; ++q) times_us[q] = tm[q];
+    return check_device_error(m);
 }
 
 int dv_model_flag_wait_timeout(dv_model* m, int32_t bits) {
@@ -2005,6 +2129,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
         return rc;
     }
     m->ncolours = ncol;
+    m->tune.gmres_prefix = -1;
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         dv_model_destroy(m);
