@@ -1,21 +1,26 @@
 #!/usr/bin/env python
 """Throughput of the implicit stepping path: simulated bed-seconds per wall-second.
 
-Workload (default ``cycle_8x8x32``): one full adsorption (8000 s) -> blowdown (60 s) -> heating
-(22400 s) -> cooling (400 s) cycle of an 8x8x32 bed (2048 cells, 12 544 unknowns, FP64), TR-BDF2
-scheme, reference solver defaults, from the seeded constant-pressure initial state (clean bed,
-T = 288 (1 +- 1 %), numpy default_rng(0)); feed 400 ppm CO2 at 50 % RH and 288 K, T_heat 373 K,
-P_vacuum 10 kPa.  A "step" of this benchmark is one such cycle.
+Workload of the line (default ``heat_window_8x8x32``, the same for ``--impl ours`` and ``--impl
+reference``): the heating step of the 8x8x32 cycle (2048 cells, 12 544 unknowns, FP64, TR-BDF2 at the
+reference defaults, T_heat 373 K, 10 kPa product vacuum) restarted from the reference's own state after
+adsorption, blowdown and 4000 s of heating (tests/golden/bench_state_8x8x32_heat4000.npz) at the
+reference's last step size, integrated for 2000 bed-seconds.  A "step" of this benchmark is one such
+window.  ``cycle_8x8x32`` / ``cycle_16x16x64`` / ``cycle_4x4x16`` make one full adsorption (8000 s) ->
+blowdown (60 s) -> heating (22400 s) -> cooling (400 s) cycle the step instead (GPU arm only).
 
 ours (default):
-  value  device-resident cycle (state stays on the GPU), CUDA events per cycle, L2 flushed between
-         cycles (a 256 MB buffer is written), max over ranks; N GPUs run N independent replicas
-  e2e    the same cycle through the public step-runner API with host numpy states and outlet
-         recording at every accepted step (the reference's steps/_runner.py usage)
-  roofline: per-kernel shares of one profiled cycle (CUDA events around each launch); the
-         dominant kernel (the sweep) timed back to back on its stream for its duration
-  cpu_baseline: the CPU oracle (numpy restatement of the reference) on a bounded sample, 1 core
---impl reference: the oracle timed on the host cores (one process per core) on a bounded sample.
+  value  device-resident (state stays on the GPU; the model is built once), CUDA events per step, L2
+         flushed between steps (a 256 MB write), max over ranks; N GPUs run N independent replicas
+  e2e    the same window through the public API the reference's runner uses (TRBDF2(...).integrate
+         with a host numpy state in and out), host copies inside the timed region
+  roofline: the dominant kernel of one profiled window, timed back to back on its stream
+  cpu_baseline: the CPU oracle (numpy restatement of the reference) on the same window, 1 core
+  cycles: full cycles of the 8x8x32 and 16x16x64 beds -- plain FP64, mixed-precision Krylov, and
+         learned predictor + mixed precision -- with their state difference to the FP64 cycle, the
+         8x8x32 cycle's step-end states against the reference's and its balance errors
+--impl reference: the oracle on the host cores (one process per core, up to 16), each process one
+  window per step.
 """
 from __future__ import annotations
 
@@ -33,12 +38,15 @@ sys.path.insert(0, ROOT)
 
 CYCLE_BED_S = 8000.0 + 60.0 + 22400.0 + 400.0
 WORKLOADS = {
+    "heat_window_8x8x32": {"grid": (8, 8, 32), "window": True},
     "cycle_8x8x32": {"grid": (8, 8, 32)},
+    "cycle_16x16x64": {"grid": (16, 16, 64)},
     "cycle_4x4x16": {"grid": (4, 4, 16)},
 }
 SAMPLE_STATE = os.path.join(ROOT, "tests", "golden", "bench_state_8x8x32_heat4000.npz")
-SAMPLE_BED_S = 2000.0        # CPU sample window: bed-seconds of heating restarted from SAMPLE_STATE
-CPU_FULL_CYCLE = "1779 s for the 30 860 bed-s cycle (17.3 bed-s/wall-s) on one core of the build host"
+REF_CYCLE = os.path.join(ROOT, "tests", "golden", "cycle_8x8x32.npz")
+WINDOW_BED_S = 2000.0
+CPU_FULL_CYCLE = "1838 s for the 30 860 bed-s 8x8x32 cycle (16.8 bed-s/wall-s) on one core of the build host"
 
 
 def overrides(grid):
@@ -48,47 +56,60 @@ def overrides(grid):
             "operation.P_vacuum": 1e4, "feed.T": 288.0, "feed.RH": 0.5, "ambient.T": 288.0}
 
 
-def setup(workload):
+def setup(grid, extra=None):
     from dac_vtsa_b200 import host
     from dac_vtsa_b200.config import load_config
-    cfg = load_config(override_dict=overrides(WORKLOADS[workload]["grid"]))
-    grid = host.Grid.from_config(cfg)
+    cfg = load_config(override_dict=dict(overrides(grid), **(extra or {})))
+    g = host.Grid.from_config(cfg)
     props = host.get_backend(cfg)
-    st = host.seeded_state(cfg, grid, props, seed=0)
-    return cfg, grid, props, st
+    st = host.seeded_state(cfg, g, props, seed=0)
+    return cfg, g, props, st
+
+
+def window_description():
+    return (f"heating step of the 8x8x32 cycle restarted from the reference's own state after adsorption, "
+            f"blowdown and 4000 s of heating (tests/golden/{os.path.basename(SAMPLE_STATE)}), at the reference's "
+            f"last step size, integrated for {WINDOW_BED_S:g} bed-s at the reference defaults (TR-BDF2)")
+
+
+class Window:
+    """The benchmark window: configuration, the restart state and the model's constants."""
+
+    def __init__(self, model_cls):
+        import numpy as np
+        from dac_vtsa_b200 import host
+        from dac_vtsa_b200.config import load_config
+        d = np.load(SAMPLE_STATE)
+        self.cfg = load_config(override_dict=json.loads(str(d["over"])))
+        self.grid = host.Grid.from_config(self.cfg)
+        self.props = host.get_backend(self.cfg)
+        self.y = np.ascontiguousarray(d["y"])
+        self.step = dict(self.cfg.cycle[2])
+        self.T_jacket = float(d["T_jacket"])
+        self.h_init = float(d["h_last"][-2])
+        st = host.seeded_state(self.cfg, self.grid, self.props, seed=0)
+        tmp = model_cls(self.cfg, self.grid, self.props, self.step, st)
+        c, q, e, Tw = tmp.unpack(self.y)
+        st.c, st.q, st.Tw = c.copy(), q.copy(), Tw.copy()
+        st.T = tmp.to_state(self.y, st, 0.0, "heating").T
+        self.state = st
+        self.h_max = self.cfg.solver.h_max_fraction * float(self.step["duration"])
+
+    def model(self, model_cls):
+        return model_cls(self.cfg, self.grid, self.props, self.step, self.state, self.T_jacket)
 
 
 # ---------------------------------------------------------------------------- CPU oracle sample
-def sample_description():
-    return (f"heating step of the 8x8x32 cycle restarted from the reference's own state after adsorption, "
-            f"blowdown and 4000 s of heating (tests/golden/{os.path.basename(SAMPLE_STATE)}), at the reference's "
-            f"last step size, integrated for {SAMPLE_BED_S:g} bed-s at the reference defaults.  Mid-heating is the "
-            f"CPU path's fastest regime (about 5x its cycle average), so this sample overstates the CPU "
-            f"throughput of a full cycle; the full reference cycle measured {CPU_FULL_CYCLE}")
-
-
-def _cpu_sample(workload, duration=SAMPLE_BED_S):
-    """The CPU oracle on the bounded sample; returns (bed-seconds, wall seconds)."""
+def _cpu_sample(workload, duration=WINDOW_BED_S):
+    """The CPU oracle on the window; returns (bed-seconds, wall seconds)."""
     os.environ.setdefault("OMP_NUM_THREADS", "1")
-    import numpy as np
     from oracle.residual import OracleModel
     from oracle.solver import OracleTRBDF2
-    from dac_vtsa_b200 import host
-    from dac_vtsa_b200.config import load_config
-    d = np.load(SAMPLE_STATE)
-    cfg = load_config(override_dict=json.loads(str(d["over"])))
-    grid = host.Grid.from_config(cfg)
-    props = host.get_backend(cfg)
-    y = d["y"]
-    step = dict(cfg.cycle[2])
-    st = host.seeded_state(cfg, grid, props, seed=0)
-    tmp = OracleModel(cfg, grid, props, step, st)
-    c, q, e, Tw = tmp.unpack(y)
-    st.c, st.q, st.T, st.Tw = c.copy(), q.copy(), tmp.temperature(e, c, q), Tw.copy()
-    m = OracleModel(cfg, grid, props, step, st, float(d["T_jacket"]))
+    w = Window(OracleModel)
+    m = w.model(OracleModel)
     t0 = time.perf_counter()
-    integ = OracleTRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * step["duration"], h_init=float(d["h_last"][-2]))
-    res = integ.integrate(y, duration, [duration])
+    integ = OracleTRBDF2(m, w.cfg, h_max=w.h_max, h_init=w.h_init)
+    res = integ.integrate(w.y, duration, [duration])
     return res.t, time.perf_counter() - t0
 
 
@@ -118,7 +139,7 @@ def cpu_model_name():
 
 def reference_arm(a, rank):
     """The reference's CPU path (the oracle port: the reference is Python and cannot travel) on the
-    host cores: each step is a batch of one bounded sample per core, run in parallel processes."""
+    host cores: each step is one window per core, run in parallel processes."""
     if rank != 0:
         return
     procs = max(1, min(os.cpu_count() or 1, 16))
@@ -133,9 +154,10 @@ def reference_arm(a, rank):
     line = {"impl": "reference", "metric": "bed-s simulated per wall-s", "value": value, "unit": "bed-s/wall-s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * wall / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": a.workload, "sample": sample_description(), "parallelism": f"{procs} processes"},
+            "config": {"workload": a.workload, "window": window_description(), "parallelism": f"{procs} processes"},
             "cpu_baseline": {"value": value, "unit": "bed-s/wall-s", "cores": procs, "kind": "port",
-                             "sample": f"{procs} processes x ({sample_description()}), {cpu_model_name()}"},
+                             "sample": f"{procs} processes x one window each per step ({window_description()}), "
+                                       f"{cpu_model_name()}"},
             "e2e": {"value": value, "unit": "bed-s/wall-s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -151,9 +173,9 @@ def max_over_ranks(x, dist=None, device=None):
     return float(t.item())
 
 
-def replica_throughput(world, cycles, seconds):
-    """Whole-job bed-seconds per wall-second: every rank runs `cycles` independent cycles."""
-    return world * cycles * CYCLE_BED_S / seconds
+def replica_throughput(world, steps, bed_s_per_step, seconds):
+    """Whole-job bed-seconds per wall-second: every rank integrates `steps` independent steps."""
+    return world * steps * bed_s_per_step / seconds
 
 
 # ---------------------------------------------------------------------------- clocks
@@ -213,7 +235,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# ---------------------------------------------------------------------------- GPU arm
+# ---------------------------------------------------------------------------- roofline
 ALG_BYTES_DOC = {
     "matvec": "FD matvec residual: reads z, u, s, f (4 n_core) + writes n_core doubles",
     "residual": "residual: reads y (+ rhs_known) and writes f: 2 n_core doubles",
@@ -221,24 +243,12 @@ ALG_BYTES_DOC = {
     "fd_jacobian": "reads y, f0 (2 n_core) + writes the 9*49*ncell block layout",
     "precond_factor": "assembly + factorisation: writes and re-reads 5 blocks per plane",
     "vector": "Krylov vector kernels: ~3 n_core doubles per launch (average)",
+    "spmv": "FP32 Jacobian product: reads 9*49*ncell floats + 2 n_core doubles, writes n_core doubles",
+    "mlp": "network kernels: features and activations",
 }
 
 
-def partition_sizes(m):
-    """Unknowns per z-partition of the preconditioner the solver builds for model m (block nb of
-    each partition): theta_block with >= 1 coupled ring = the innermost ring of all sectors plus
-    rings 1.. of each sector with its wall node; theta_block with 0 rings = whole sectors; full =
-    one partition (also for a single sector)."""
-    g, s, w = m.grid, m.cfg.solver, (1 if m.n_w else 0)
-    mode = s.preconditioner if g.Nth > 1 else "full"
-    if mode == "theta_block" and s.precond_theta_rings >= 1 and g.Nr >= 2:
-        return [6 * (g.Nr - 1) + w] * g.Nth + [6 * g.Nth]
-    if mode == "theta_block":
-        return [6 * g.Nr + w] * g.Nth
-    return [6 * g.Nr * g.Nth + w * g.Nth]
-
-
-def alg_bytes_per_launch(kind, m):
+def alg_bytes_per_launch(kind, m, nbs=None, fp32=False):
     n = m.n_core
     if kind == "matvec":
         return 5 * n * 8
@@ -246,7 +256,9 @@ def alg_bytes_per_launch(kind, m):
         return 2 * n * 8
     if kind == "fd_jacobian":
         return (2 * n + m.jac_doubles) * 8
-    blocks = m.grid.Nz * 5 * sum(nb * nb for nb in partition_sizes(m)) * 8
+    if kind == "spmv":
+        return m.jac_doubles * 4 + 3 * n * 8
+    blocks = m.grid.Nz * 5 * sum(nb * nb for nb in nbs) * (4 if fp32 else 8)
     if kind == "precond_apply":
         return blocks + 3 * n * 8
     if kind == "precond_factor":
@@ -254,15 +266,17 @@ def alg_bytes_per_launch(kind, m):
     return 3 * n * 8
 
 
-def sweep_seconds(m, y, launches=200):
-    """Average duration of the preconditioner sweep: the factors of I - dh J at state y (the
-    solver's partitions), then `launches` back-to-back dv_precond_solve calls bracketed by CUDA
-    events on the launching stream (the queue never drains, so no host latency is counted)."""
+def sweep_seconds(m, y, dh, launches=200):
+    """Average duration of the preconditioner sweep: the factors of I - dh J at state y (the solver's
+    partitions), then `launches` back-to-back dv_precond_solve calls bracketed by CUDA events on the
+    launching stream (the queue never drains, so no host latency is counted).  Returns (seconds,
+    block sizes of the partitions)."""
     import ctypes as C
     import torch
     from dac_vtsa_b200.jacobian import FDJacobian
     yd = y.contiguous() if isinstance(y, torch.Tensor) else torch.from_numpy(y).to(m.device)
-    m.precond_factor(FDJacobian(m).block(0.0, yd), 2.1)
+    m.precond_factor(FDJacobian(m).block(0.0, yd), dh)
+    _, _, nbs = m.precond_partitions()
     b = torch.randn(m.n_core, dtype=torch.float64, device=m.device)
     x = torch.empty_like(b)
     s = torch.cuda.current_stream()
@@ -275,14 +289,101 @@ def sweep_seconds(m, y, launches=200):
         m.lib.dv_precond_solve(*args)
     e1.record(s)
     e1.synchronize()
-    return e0.elapsed_time(e1) / 1e3 / launches
+    return e0.elapsed_time(e1) / 1e3 / launches, nbs
 
 
+def load_peaks():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------- cycles (extra keys)
+def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
+    """Device-resident full cycles of `grid` in each variant ("fp64", "mixed", "learned_mixed"):
+    throughput, solver totals and the end state's difference to the FP64 cycle."""
+    import numpy as np
+    import torch
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.predictor import NewtonPredictor
+    from dac_vtsa_b200.runner import run_cycle_device
+    out, y64 = {}, None
+    for var in variants:
+        extra = {} if var == "fp64" else {"gpu.krylov_precision": "fp32"}
+        cfg, g, props, st = setup(grid, extra)
+        m0 = TVSAModel(cfg, g, props, cfg.cycle[0], st)
+        y0 = torch.from_numpy(m0.pack(st)).to(dev)
+        net = None
+        if var == "learned_mixed":
+            if not os.path.exists(weights_path):
+                out[var] = {"skipped": f"no trained weights at {os.path.relpath(weights_path, ROOT)}"}
+                continue
+            net = NewtonPredictor.load(weights_path)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        y, stats, _ = run_cycle_device(y0, cfg, g, props, predictor=net, predict=net is not None)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        yh = y.cpu().numpy()
+        keys = ("steps", "rejected", "newton_iters", "gmres_iters", "gmres_polish", "balance_unclosed",
+                "pred_net", "pred_extrap", "pred_retry")
+        rec = {"value": CYCLE_BED_S / wall, "wall_s": wall,
+               "solver": {k: int(sum(s.get(k, 0) for s in stats)) for k in keys}}
+        if var == "fp64":
+            y64 = yh
+        elif y64 is not None:
+            sc = m0.atol + cfg.solver.rtol * np.abs(y64)
+            rec["state_diff_vs_fp64_rel_max"] = float(np.max(np.abs(yh - y64) / (np.abs(y64) + m0.atol)))
+            rec["state_diff_vs_fp64_scaled_rms"] = float(np.sqrt(np.mean(((yh - y64) / sc) ** 2)))
+            rec["speedup_vs_fp64"] = rec["value"] / out["fp64"]["value"]
+        out[var] = rec
+    return out
+
+
+def reference_cycle_parity(dev):
+    """The 8x8x32 cycle through the public step runner against the reference's own cycle: step-end
+    states (scaled by the solver's error scale) and the worst mass / energy balance errors."""
+    import numpy as np
+    from dac_vtsa_b200 import balances, host
+    from dac_vtsa_b200.config import load_config
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.runner import run_step
+    d = np.load(REF_CYCLE)
+    cfg = load_config(override_dict=json.loads(str(d["over"])))
+    g = host.Grid.from_config(cfg)
+    props = host.get_backend(cfg)
+    tmpl = host.initial_state(cfg, g, props)
+    m0 = TVSAModel(cfg, g, props, cfg.cycle[0], tmpl)
+    st = m0.to_state(d["y0"], tmpl, 0.0, "initial")
+    steps, T_prev, t_cycle, per_step = [], None, 0.0, []
+    t0 = time.perf_counter()
+    for k, step in enumerate(cfg.cycle):
+        st, sr = run_step(st, cfg, g, props, step, cycle_idx=1, t_cycle0=t_cycle, T_jacket_prev=T_prev,
+                          record_outlet=False)
+        y = m0.pack(st)
+        yr = d[f"s{k}_y"]
+        sc = m0.atol + cfg.solver.rtol * np.abs(yr)
+        per_step.append({"step": step["name"], "scaled_rms": float(np.sqrt(np.mean(((y - yr) / sc) ** 2))),
+                         "rel_max": float(np.max(np.abs(y - yr) / (np.abs(yr) + m0.atol)))})
+        t_cycle += sr.duration
+        T_prev = sr.T_jacket if sr.jacket_on else T_prev
+        steps.append(sr)
+    return {"wall_s": time.perf_counter() - t0, "step_end_vs_reference": per_step,
+            "balance_errors": balances.worst_balance_errors(steps, ("CO2", "H2O", "N2")),
+            "reference_balance_errors": {"mass": float(np.abs(d["mass_rel_err"]).max()),
+                                         "energy": float(np.abs(d["energy_rel_err"]).max())}}
+
+
+# ---------------------------------------------------------------------------- GPU arm
 def gpu_arm(a, rank, world, local_rank):
     import numpy as np
     import torch
     from dac_vtsa_b200 import _lib, counters
+    from dac_vtsa_b200.model import TVSAModel
     from dac_vtsa_b200.runner import run_cycle, run_cycle_device
+    from dac_vtsa_b200.solver import TRBDF2
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -291,11 +392,7 @@ def gpu_arm(a, rank, world, local_rank):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-    cfg, grid, props, st = setup(a.workload)
-    from dac_vtsa_b200.model import TVSAModel
-    m0 = TVSAModel(cfg, grid, props, cfg.cycle[0], st)
-    y0_host = torch.from_numpy(m0.pack(st)).pin_memory()
-    y0_dev = y0_host.to(dev)
+    wl = WORKLOADS[a.workload]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def barrier():
@@ -303,13 +400,29 @@ def gpu_arm(a, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    def one_cycle():
-        y, stats, _ = run_cycle_device(y0_dev.clone(), cfg, grid, props)
-        return y, stats
+    if wl.get("window"):
+        w = Window(TVSAModel)
+        model = w.model(TVSAModel)
+        integ = TRBDF2(model, w.cfg, h_max=w.h_max, h_init=w.h_init)
+        y0_dev = torch.from_numpy(w.y).to(dev)
+        bed_per_step = WINDOW_BED_S
+
+        def one_step():
+            r = integ.integrate(y0_dev, WINDOW_BED_S, [WINDOW_BED_S], keep_on_device=True)
+            return r.y, dict(integ.stats, steps=r.n_steps, rejected=r.n_reject)
+    else:
+        cfg, grid, props, st = setup(wl["grid"])
+        m0 = TVSAModel(cfg, grid, props, cfg.cycle[0], st)
+        y0_dev = torch.from_numpy(m0.pack(st)).to(dev)
+        bed_per_step = CYCLE_BED_S
+
+        def one_step():
+            y, stats, _ = run_cycle_device(y0_dev.clone(), cfg, grid, props)
+            return y, stats
 
     for _ in range(a.warmup):
-        one_cycle()
-    # ---- timed region: K device-resident cycles
+        one_step()
+    # ---- timed region: K device-resident steps
     sampler = ClockSampler(local_rank if "CUDA_VISIBLE_DEVICES" not in os.environ else
                            os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local_rank])
     sampler.start()
@@ -319,11 +432,11 @@ def gpu_arm(a, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     stats_last = None
     for _ in range(a.steps):
-        flush.fill_(1.0)                         # evict L2 between timed cycles (outside the events)
+        flush.fill_(1.0)                         # evict L2 between timed steps (outside the events)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        y_end, stats_last = one_cycle()
+        y_end, stats_last = one_step()
         e1.record(stream)
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
@@ -331,68 +444,41 @@ def gpu_arm(a, rank, world, local_rank):
     launches = _lib.launch_count() - launches0
     clocks = sampler.stop()
     total_ms = max_over_ranks(total_ms, dist, dev)
-    value = replica_throughput(world, a.steps, total_ms / 1e3)
-    # ---- e2e: public step-runner API, host states, outlet recording per accepted step
+    value = replica_throughput(world, a.steps, bed_per_step, total_ms / 1e3)
+    # ---- e2e: the public API with host states in and out
     counters.reset()
     barrier()
-    t0 = time.perf_counter()
-    for _ in range(max(1, a.e2e_steps)):
-        st_in = st.copy()
-        run_cycle(st_in, cfg, grid, props, record_outlet=True)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
     nE = max(1, a.e2e_steps)
-    e2e_s = max_over_ranks(e2e_s, dist, dev)
-    e2e = {"value": replica_throughput(world, nE, e2e_s), "unit": "bed-s/wall-s",
+    t0 = time.perf_counter()
+    for _ in range(nE):
+        if wl.get("window"):
+            m = w.model(TVSAModel)
+            r = TRBDF2(m, w.cfg, h_max=w.h_max, h_init=w.h_init).integrate(w.y, WINDOW_BED_S, [WINDOW_BED_S])
+            assert np.all(np.isfinite(r.y))
+        else:
+            run_cycle(st.copy(), cfg, grid, props, record_outlet=True)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e2e = {"value": replica_throughput(world, nE, bed_per_step, e2e_s), "unit": "bed-s/wall-s",
            "h2d_bytes_per_step": counters.TRAFFIC["h2d"] // nE, "d2h_bytes_per_step": counters.TRAFFIC["d2h"] // nE,
-           "path": "runner.run_cycle (steps/_runner.py-compatible run_step per cycle step, outlet recorded at "
-                   "every accepted step)"}
-    # ---- mixed precision (gpu.krylov_precision = fp32: FP32 factor storage in the preconditioner
-    # sweep), the same cycle, one warm-up and one timed cycle; state difference to the FP64 cycle
-    mixed = None
-    if not a.no_mixed:
-        from dac_vtsa_b200.config import load_config
-        cfg32 = load_config(override_dict=dict(overrides(WORKLOADS[a.workload]["grid"]),
-                                               **{"gpu.krylov_precision": "fp32"}))
-        run_cycle_device(y0_dev.clone(), cfg32, grid, props)
-        flush.fill_(1.0)
-        barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        y32, st32, _ = run_cycle_device(y0_dev.clone(), cfg32, grid, props)
-        e1.record(stream)
-        e1.synchronize()
-        ms32 = max_over_ranks(e0.elapsed_time(e1), dist, dev)
-        y64h, y32h = y_end.double().cpu().numpy(), y32.double().cpu().numpy()
-        sc = m0.atol + cfg.solver.rtol * np.abs(y64h)
-        dev_scaled = (y32h - y64h) / sc
-        mixed = {"value": replica_throughput(world, 1, ms32 / 1e3), "unit": "bed-s/wall-s", "ms_per_step": ms32,
-                 "precision": "FP32 preconditioner factors, FP64 residual/Jacobian/Newton/GMRES vectors",
-                 "state_diff_vs_fp64_scaled_rms": float(np.sqrt(np.mean(dev_scaled ** 2))),
-                 "state_diff_vs_fp64_scaled_max": float(np.abs(dev_scaled).max()),
-                 "state_diff_vs_fp64_rel_max": float(np.max(np.abs(y32h - y64h) / (np.abs(y64h) + m0.atol))),
-                 "solver": st32}
-    # ---- one profiled cycle: per-kernel device time from CUDA events around every launch
+           "path": ("TRBDF2(TVSAModel(...)).integrate(host numpy y0) per window, the reference runner's usage"
+                    if wl.get("window") else "runner.run_cycle, outlet recorded at every accepted step")}
+    # ---- one profiled step: per-kernel device time from CUDA events around every launch
     _lib.profile_enable(True)
-    _, _ = one_cycle()
+    one_step()
     prof = _lib.profile_read()
     _lib.profile_enable(False)
     kinds = {k: v for k, v in prof.items() if v[1] > 0}
-    # the roofline names one kernel; "vector" is the class of small Krylov kernels, not one kernel
     dom = max((k for k in kinds if k != "vector"), key=lambda k: kinds[k][2])
     n_l, n_t, ms = kinds[dom]
-    avg_cycle_s = ms / 1e3 / n_t
-    # the per-launch events of the profiled cycle also hold each launch's host latency (the GPU
-    # waits for the host there), so the kernel's own duration is timed back to back on its stream
-    avg_s = sweep_seconds(m0, y_end) if dom == "precond_apply" else avg_cycle_s
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        peak, peak_src = 6650.0, "fallback"
-    alg = alg_bytes_per_launch(dom, m0)
+    avg_step_s = ms / 1e3 / n_t
+    mref = model if wl.get("window") else m0
+    nbs = None
+    if dom in ("precond_apply", "precond_factor"):
+        sweep_s, nbs = sweep_seconds(mref, y_end, 0.29 * 100.0)
+    avg_s = sweep_s if dom == "precond_apply" else avg_step_s
+    peak, peak_src = load_peaks()
+    alg = alg_bytes_per_launch(dom, mref, nbs)
     achieved = alg / avg_s / 1e9
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -404,27 +490,37 @@ def gpu_arm(a, rank, world, local_rank):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 3), "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                 "alg_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
-                "avg_launch_us_in_cycle": avg_cycle_s * 1e6,
+                "avg_launch_us_in_step": avg_step_s * 1e6, "partition_nb": nbs,
                 "alg_bytes_rule": ALG_BYTES_DOC.get(dom, ""),
                 "kernel_share": {k: round(v[2] / sum(x[2] for x in kinds.values()), 4) for k, v in kinds.items()},
-                "launches_per_cycle": int(sum(x[0] for x in kinds.values())),
+                "launches_per_step": int(sum(x[0] for x in kinds.values())),
                 "kernel_avg_us": {k: round(1e3 * v[2] / v[1], 3) for k, v in kinds.items()}}
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu:
+    if rank == 0 and world == 1 and not a.no_cpu and wl.get("window"):
         bed, wall = _cpu_sample(a.workload)
         cpu = {"value": bed / wall, "unit": "bed-s/wall-s", "cores": 1, "kind": "port",
-               "sample": f"{sample_description()}; 1 process, {cpu_model_name()}"}
+               "sample": f"{window_description()}; the whole window, 1 process, {cpu_model_name()}"}
+    # ---- extra keys: full cycles (not part of the timed line)
+    cycles = None
+    if rank == 0 and not a.no_cycles:
+        weights = os.path.join(ROOT, "dac_vtsa_b200", "predictor_weights.npz")
+        cycles = {"8x8x32": cycle_runs((8, 8, 32), ("fp64", "mixed", "learned_mixed"), weights, dev)}
+        if os.path.exists(REF_CYCLE):
+            cycles["8x8x32"]["reference_parity"] = reference_cycle_parity(dev)
+        cycles["8x8x32"]["reference_cpu_cycle"] = CPU_FULL_CYCLE
+        if not a.no_big:
+            cycles["16x16x64"] = cycle_runs((16, 16, 64), ("fp64", "mixed", "learned_mixed"), weights, dev)
     if rank == 0:
         line = {"metric": "bed-s simulated per wall-s", "value": value, "unit": "bed-s/wall-s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": a.workload, "grid": list(WORKLOADS[a.workload]["grid"]),
-                           "cycle_bed_s": CYCLE_BED_S, "scheme": "trbdf2", "precision": "fp64",
-                           "l2": "flushed between timed cycles (256 MB write)",
+                "config": {"workload": a.workload, "grid": list(wl["grid"]),
+                           "step": window_description() if wl.get("window") else "full cycle",
+                           "bed_s_per_step": bed_per_step, "scheme": "trbdf2", "precision": "fp64",
+                           "l2": "flushed between timed steps (256 MB write)",
                            "parallelism": f"{world} independent replicas (one per GPU)"},
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu,
-                "mixed_precision": mixed,
-                "clocks": clocks, "solver": stats_last}
+                "clocks": clocks, "solver": stats_last, "cycles": cycles}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -434,13 +530,14 @@ def gpu_arm(a, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="cycle_8x8x32")
-    ap.add_argument("--e2e-steps", type=int, default=2, help="cycles of the e2e measurement (their mean)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="heat_window_8x8x32")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="steps of the e2e measurement (their mean)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision cycle")
+    ap.add_argument("--no-cycles", action="store_true", help="skip the full-cycle extra keys")
+    ap.add_argument("--no-big", action="store_true", help="skip the 16x16x64 cycles among them")
     a = ap.parse_args()
     if a.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -448,7 +545,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if a.impl == "reference":
-        reference_arm(a, rank)
+        if WORKLOADS[a.workload].get("window"):
+            reference_arm(a, rank)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU reference runs bounded windows only "
+                              "(heat_window_8x8x32); a full cycle takes 1838 s per core"}), flush=True)
         return
     gpu_arm(a, rank, world, local_rank)
 

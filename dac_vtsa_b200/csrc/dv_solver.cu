@@ -3,6 +3,7 @@
 // Control flow mirrors the reference exactly (core/solver.py); the arithmetic runs on the GPU
 // (dv_kernels.cu, dv_linalg.cu and the vector kernels below) and the host reads back a few
 // scalars per Krylov iteration to take the same branch decisions.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,7 +27,7 @@ struct ProfSlot {
     double ms = 0.0;
 };
 static ProfSlot g_prof[K_NKIND];
-static int64_t g_launches = 0;
+static std::atomic<int64_t> g_launches{0};   // launches of every thread (models run concurrently)
 static bool g_prof_on = false;
 struct Pending {
     int kind;
@@ -2002,7 +2003,7 @@ int dv_profile_read(int32_t kind, int64_t* launches, int64_t* timed, double* tot
     return DV_OK;
 }
 
-int64_t dv_launch_count(void) { return g_launches; }
+int64_t dv_launch_count(void) { return g_launches.load(); }
 size_t dv_step_params_size(void) { return sizeof(dv_step_params); }
 const char* dv_last_error(void) { return g_err.c_str(); }
 

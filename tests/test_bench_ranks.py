@@ -21,7 +21,7 @@ def _worker(rank, world, port, out):
     try:
         import bench
         slowest = bench.max_over_ranks(1.5 + rank, dist)            # rank 1 is the slow one
-        value = bench.replica_throughput(world, 2, slowest)
+        value = bench.replica_throughput(world, 2, bench.WINDOW_BED_S, slowest)
         ran_reference = (bench.reference_arm(None, rank) is not None) if rank != 0 else None
         out[rank] = (slowest, value, ran_reference)
     finally:
@@ -36,11 +36,11 @@ def test_two_ranks_time_is_the_slowest_and_throughput_counts_every_replica():
     for rank in range(world):
         slowest, value, _ = out[rank]
         assert slowest == pytest.approx(2.5)
-        assert value == pytest.approx(world * 2 * bench.CYCLE_BED_S / 2.5)
+        assert value == pytest.approx(world * 2 * bench.WINDOW_BED_S / 2.5)
     assert out[1][2] is False                                    # rank 1 does no reference work
 
 
 def test_single_process_needs_no_process_group():
     import bench
     assert bench.max_over_ranks(3.0) == 3.0
-    assert bench.replica_throughput(1, 1, 10.0) == pytest.approx(bench.CYCLE_BED_S / 10.0)
+    assert bench.replica_throughput(1, 1, bench.CYCLE_BED_S, 10.0) == pytest.approx(bench.CYCLE_BED_S / 10.0)
