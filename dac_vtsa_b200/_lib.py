@@ -90,7 +90,7 @@ class DvSolverOpts(C.Structure):
     _fields_ = [("scheme", I32), ("max_newton_iter", I32), ("jacobian_max_age", I32), ("gmres_refresh", I32),
                 ("precond_mode", I32), ("krylov_fp32", I32), ("max_steps", I64),
                 ("rtol", D), ("newton_kappa", D), ("refactor_ratio", D), ("conservation_tol", D),
-                ("h_max", D), ("h_init", D)]
+                ("h_max", D), ("h_init", D), ("newton_mode", I32), ("pad_", I32)]
 
 
 class DvTuning(C.Structure):
@@ -103,7 +103,7 @@ class DvStepReport(C.Structure):
                 ("n_lu", I64), ("nfev", I64), ("gmres_iters", I64), ("gmres_polish", I64),
                 ("balance_unclosed", I64), ("jac_refresh_in_newton", I64), ("krylov_ok", I64),
                 ("krylov_fail", I64), ("acc", D * DV_NACC), ("newton_iters", I64), ("pred_net", I64),
-                ("pred_extrap", I64), ("pred_retry", I64)]
+                ("pred_extrap", I64), ("pred_retry", I64), ("modified_fail", I64)]
 
 
 P = C.c_void_p
@@ -125,6 +125,7 @@ SIGNATURES = [
     ("dv_rhs_diag", C.c_int, [P, D, P, P, P]),
     ("dv_outlet_row", C.c_int, [P, D, P, D, P, P]),
     ("dv_precond_partitions", C.c_int, [P, C.POINTER(I32), C.POINTER(I32), P, I32, C.POINTER(I32)]),
+    ("dv_precond_check_maps", C.c_int, [C.POINTER(DvStepParams), I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(I64)]),
     ("dv_colour_columns", C.c_int, [I32, I32, I32, I32, P, C.POINTER(I32)]),
     ("dv_fd_jacobian", C.c_int, [P, D, P, P, P, P]),
     ("dv_precond_factor", C.c_int, [P, P, D, I32, P]),
@@ -152,6 +153,7 @@ SIGNATURES = [
     ("dv_mlp_clear_samples", C.c_int, [P]),
     ("dv_mlp_forward_host", C.c_int, [P, P, I64, P]),
     ("dv_mlp_gradient_host", C.c_int, [P, P, P, I64, P, C.POINTER(D)]),
+    ("dv_mlp_gemm_host", C.c_int, [I32, I32, I32, P, P, P]),
     ("dv_mlp_train", C.c_int, [P, I32, C.c_float, C.c_uint64, I32, P, P]),
     ("dv_integrator_set_predictor", C.c_int, [P, P, I32, I32, I32]),
 ]

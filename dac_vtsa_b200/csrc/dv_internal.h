@@ -119,6 +119,7 @@ struct dv_model {
     float* d_J32;                   // [DV_NSLOT][DV_NB][DV_NB][ncell] (allocated on first use)
     int pc_cap_nb, pc_cap_parts;
     double* d_pc;                   // [parts][Nz][5][nb*nb]
+    int64_t pc_doubles;             // entries allocated for d_pc (and d_pc32)
     double* d_pc_work;              // [parts][2][nb*nb] factorisation scratch
     int* d_pc_piv;                  // [parts][nb] pivot work
     int* d_pc_info;                 // [parts] singular-pivot flags
@@ -154,6 +155,8 @@ int64_t precond_doubles(int nb, int nparts, int Nz);
 // Partition mode, twisted separator plane and block size of every partition of the current factors
 // (nb_out up to cap entries); returns the number of partitions (0 before the first factorisation).
 int precond_partitions(const dv_model* m, int* mode, int* zs, int* nb_out, int cap);
+// Host check of a geometry's partition maps (number of violations; 0 = consistent).
+int64_t precond_check_maps(const dv_step_params& p, int mode, int* nparts, int* nb);
 // Largest block, partition count and storage over the partition modes a model of p can factorise.
 void precond_capacity(const dv_step_params& p, int* cap_nb, int* cap_parts, int64_t* pc_need, int64_t* work_need);
 int64_t precond_work_doubles(int nb, int nparts, int Nz);

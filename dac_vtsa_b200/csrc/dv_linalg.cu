@@ -25,6 +25,7 @@
 // contributions of both sides, and their 2 nb x 2 nb system is inverted by blocks.  Half the
 // sequential plane chain of the one-directional form, for the same matrix.
 #include <algorithm>
+#include <vector>
 #include <type_traits>
 #include "dv_internal.h"
 #include "dv_physics.cuh"
@@ -37,7 +38,18 @@ struct PcGeom {
     int zs;                // twisted factorisation: separator planes zs, zs+1 (0: one direction, top-down)
     int ncv;               // cell unknowns (6 per cell) of the partition; nb - ncv wall nodes follow
     int64_t nc, bs;        // bs: block stride in doubles (nb*ld rounded up to even: 16-byte multiple)
+    // self-checks of the kernels: factor storage (entries; < 0: unchecked), state length, error word
+    int64_t cap, nstate;
+    int* err;
 };
+
+// Error word bit of an index that fell outside its storage (the access is skipped, not made).
+#define PC_ERR_RANGE 32
+static __device__ __forceinline__ bool pc_range_ok(const PcGeom& g, int64_t first, int64_t count) {
+    if (g.cap < 0 || (first >= 0 && first + count <= g.cap)) return true;
+    if (g.err) atomicOr(g.err, PC_ERR_RANGE);
+    return false;
+}
 
 // Mode 3 (mode 2 split for large cross-sections): contiguous groups of n items in G groups, the
 // first n % G groups one item larger.  Ring groups cover rings 1..Nr-1 of a sector (the wall node
@@ -78,7 +90,7 @@ static __host__ __device__ __forceinline__ PcGeom pc_part(const PcGeom& g, int p
 }
 
 // partition of the cell unknowns of cell (i, j)
-static __device__ __forceinline__ int pc_part_of(const PcGeom& g, int i, int j) {
+static __host__ __device__ __forceinline__ int pc_part_of(const PcGeom& g, int i, int j) {
     if (g.mode == 0) return j;
     if (g.mode == 2) return (i == 0) ? g.Nth : j;
     if (g.mode == 3)
@@ -101,7 +113,7 @@ static inline int pc_lds(int nb, size_t budget) {
     return (size_t)9 * nb * l * sizeof(double) <= budget ? l : l4;
 }
 
-static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int k, int l) {
+static __host__ __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int k, int l) {
     const int64_t offw = (int64_t)DV_NV * g.nc;
     if (g.mode == 3) {
         int a0, a1;
@@ -144,7 +156,7 @@ static __device__ __forceinline__ int64_t pc_glob(const PcGeom& g, int part, int
 }
 
 // local index of (cell (i, j), var v) / wall (j) inside its partition
-static __device__ __forceinline__ int pc_local(const PcGeom& g, int i, int j, int v) {
+static __host__ __device__ __forceinline__ int pc_local(const PcGeom& g, int i, int j, int v) {
     if (g.mode == 3) {
         int a0, a1;
         if (v == DV_NV) {                       // the wall node follows the cells of the outer group
@@ -208,7 +220,13 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
     const int part = pc_part_of(g, i, j);
     if (!ok || pc_part_of(g, ni, nj) != part) return;      // coupling across partitions: dropped
     const int d = nk - k;
-    double* B = A + (((int64_t)part * g.Nz + k) * 5 + (d + 2)) * g.bs;
+    const int64_t boff = (((int64_t)part * g.Nz + k) * 5 + (d + 2)) * g.bs;
+    if (part >= g.nparts || !pc_range_ok(g, boff, g.bs)) {
+        if (part >= g.nparts && g.err) atomicOr(g.err, PC_ERR_RANGE);
+        return;
+    }
+    double* B = A + boff;
+    const int pnb = pc_part(g, part).nb;
     const bool row_wall_ok = g.wall && i == g.Nr - 1;
     const bool col_wall_ok = g.wall && ni == g.Nr - 1;
     for (int rv = 0; rv < DV_NB; ++rv) {
@@ -220,6 +238,10 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
             const double jv = J[((int64_t)(slot * DV_NB + rv) * DV_NB + cv) * g.nc + c];
             double val = -dh * jv;
             if (slot == 0 && rv == cv) val += 1.0;
+            if (lr >= pnb || lc >= pnb) {
+                if (g.err) atomicOr(g.err, PC_ERR_RANGE);
+                continue;
+            }
             B[(int64_t)lr * g.ld + lc] = val;
         }
     }
@@ -648,7 +670,11 @@ __global__ void __launch_bounds__(256) k_pc_factor_smem(PcGeom gin, double* __re
     // block (local plane t, local slot sl)
     auto B = [&](int t, int sl) -> double* {
         const int P = (rank == 0) ? t : Nz - 1 - t;
-        return base + ((int64_t)P * 5 + ((rank == 0) ? sl : 4 - sl)) * g.bs;
+        const int64_t off = ((int64_t)P * 5 + ((rank == 0) ? sl : 4 - sl)) * g.bs;
+        // outside the partition's planes or the storage: recorded, and the partition's first block
+        // stands in (the factors are then wrong and the error word says so)
+        if (P < 0 || P >= Nz || !pc_range_ok(g, (int64_t)part * Nz * 5 * g.bs + off, g.bs)) return base;
+        return base + off;
     };
     int bad = 0;
     for (int k = 0; k < n; ++k) {
@@ -1061,6 +1087,9 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             nblk = 3;
         }
         const uint32_t tot = (nblk + (src2 ? 1u : 0u)) * b1;
+        // a copy from outside the factor storage is not issued (its stage then times out)
+        if (!pc_range_ok(g, (int64_t)(src - A), (int64_t)nblk * bs) || (src2 && !pc_range_ok(g, (int64_t)(src2 - A), bs)))
+            return;
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tot) : "memory");
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                      ::"r"(dst), "l"(src), "r"(nblk * b1), "r"(bar) : "memory");
@@ -1087,8 +1116,13 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         for (int u = 0; u < PA_IO; ++u) {
             const int q = q0 + u * PA_THREADS;
             const int t = q / LD, l = q - t * LD;
-            const bool in = q < Nz * LD && l < nb && t < nio;
+            bool in = q < Nz * LD && l < nb && t < nio;
             gi[u] = in ? pc_glob(g, part, fr.gp(t), l) : -1;
+            if (in && (gi[u] < 0 || gi[u] >= g.nstate)) {
+                if (g.err) atomicOr(g.err, PC_ERR_RANGE);
+                in = false;
+                gi[u] = -1;
+            }
             bv[u] = in ? src[gi[u]] : 0.0;
             sv[u] = (in && sc) ? sc[gi[u]] : 1.0;
         }
@@ -1259,8 +1293,13 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             for (int u = 0; u < PA_IO; ++u) {
                 const int q = q0 + u * PA_THREADS;
                 const int t = q / LD, l = q - t * LD;
-                const bool in = q < Nz * LD && l < nb && t < nio;
+                bool in = q < Nz * LD && l < nb && t < nio;
                 gi[u] = in ? pc_glob(g, part, fr.gp(t), l) : -1;
+                if (in && (gi[u] < 0 || gi[u] >= g.nstate)) {
+                    if (g.err) atomicOr(g.err, PC_ERR_RANGE);
+                    in = false;
+                    gi[u] = -1;
+                }
                 sv[u] = (in && sc) ? sc[gi[u]] : 1.0;
             }
 #pragma unroll
@@ -1357,6 +1396,9 @@ static PcGeom geom_of_params(const dv_step_params& p, int mode) {
     g.Nz = p.Nz;
     g.wall = p.wall_on;
     g.rg = g.tg = 1;
+    g.cap = -1;
+    g.nstate = (int64_t)DV_NV * p.Nr * p.Nth * p.Nz + (p.wall_on ? (int64_t)p.Nth * p.Nz : 0);
+    g.err = nullptr;
     // mode 2 needs a second ring and a second sector; below that it is mode 0 (or 1 for one sector)
     if (mode == 2 && (p.Nr < 2 || p.Nth < 2)) mode = 0;
     g.mode = (p.Nth > 1 && (mode == 0 || mode == 2)) ? mode : 1;
@@ -1410,7 +1452,12 @@ static PcGeom geom_of_params(const dv_step_params& p, int mode) {
     return g;
 }
 
-static PcGeom geom_of(const dv_model* m, int mode) { return geom_of_params(m->p, mode); }
+static PcGeom geom_of(const dv_model* m, int mode) {
+    PcGeom g = geom_of_params(m->p, mode);
+    g.cap = m->pc_doubles;
+    g.err = m->d_err;
+    return g;
+}
 
 void precond_capacity(const dv_step_params& p, int* cap_nb, int* cap_parts, int64_t* pc_need, int64_t* work_need) {
     int nb = 0, parts = 0;
@@ -1426,6 +1473,47 @@ void precond_capacity(const dv_step_params& p, int* cap_nb, int* cap_parts, int6
     *cap_parts = parts;
     *pc_need = need;
     *work_need = precond_work_doubles(nb, parts, p.Nz);
+}
+
+// Host check of the partition maps of a geometry (tests): every (partition, plane, local index) maps
+// to an unknown inside the state, each unknown exactly once, and the inverse map (cell / wall ->
+// partition, local index) agrees.  Returns the number of violations.
+int64_t precond_check_maps(const dv_step_params& p, int mode, int* nparts_out, int* nb_out) {
+    const PcGeom g = geom_of_params(p, mode);
+    const int64_t nc = g.nc, offw = (int64_t)DV_NV * nc, n = offw + (g.wall ? (int64_t)g.Nth * g.Nz : 0);
+    std::vector<int> seen(n, 0);
+    int64_t bad = 0;
+    for (int part = 0; part < g.nparts; ++part) {
+        const PcGeom q = pc_part(g, part);
+        if (q.nb > g.nb || q.ncv > q.nb || q.nb < 1) ++bad;
+        for (int k = 0; k < g.Nz; ++k)
+            for (int l = 0; l < q.nb; ++l) {
+                const int64_t gi = pc_glob(q, part, k, l);
+                if (gi < 0 || gi >= n) { ++bad; continue; }
+                seen[gi] += 1;
+            }
+    }
+    for (int64_t u = 0; u < n; ++u)
+        if (seen[u] != 1) ++bad;
+    for (int i = 0; i < g.Nr; ++i)
+        for (int j = 0; j < g.Nth; ++j)
+            for (int k = 0; k < g.Nz; ++k) {
+                const int part = pc_part_of(g, i, j);
+                if (part < 0 || part >= g.nparts) { ++bad; continue; }
+                const PcGeom q = pc_part(g, part);
+                const int64_t cell = ((int64_t)i * g.Nth + j) * g.Nz + k;
+                for (int v = 0; v < DV_NV; ++v) {
+                    const int l = pc_local(g, i, j, v);
+                    if (l < 0 || l >= q.ncv || pc_glob(q, part, k, l) != v * nc + cell) ++bad;
+                }
+                if (g.wall && i == g.Nr - 1) {
+                    const int l = pc_local(g, i, j, DV_NV);
+                    if (l < q.ncv || l >= q.nb || pc_glob(q, part, k, l) != offw + (int64_t)j * g.Nz + k) ++bad;
+                }
+            }
+    *nparts_out = g.nparts;
+    *nb_out = g.nb;
+    return bad;
 }
 
 int precond_partitions(const dv_model* m, int* mode, int* zs, int* nb_out, int cap) {

@@ -696,6 +696,51 @@ int dv_mlp_forward_host(dv_mlp* n, const float* X, int64_t rows, float* out) {
     return DV_OK;
 }
 
+// One tensor-core product D [M][N] = A [M][K] B[N][K]^T of host fp32 matrices rounded to BF16 (M a
+// multiple of 128, N a multiple of 16 up to 128, K a multiple of 16), FP32 result: the check of the
+// product kernel itself.  Allocates its device buffers.
+int dv_mlp_gemm_host(int32_t M, int32_t N, int32_t K, const float* A, const float* B, float* D) {
+    if (M <= 0 || M % 128 || N < 16 || N > 128 || N % 16 || K <= 0 || K % 16 || !A || !B || !D) {
+        set_error("dv_mlp_gemm_host: M multiple of 128, N in 16..128 multiple of 16, K multiple of 16");
+        return DV_ERR_ARG;
+    }
+    std::vector<uint16_t> ab, bb;
+    bf16_round_host(A, (int64_t)M * K, ab);
+    bf16_round_host(B, (int64_t)N * K, bb);
+    std::vector<uint16_t> ap((size_t)M * K), bp((size_t)N * K);
+    for (int64_t r = 0; r < M; ++r)
+        for (int k = 0; k < K; ++k) ap[pidx(r, k, M)] = ab[r * K + k];
+    for (int64_t r = 0; r < N; ++r)
+        for (int k = 0; k < K; ++k) bp[pidx(r, k, N)] = bb[r * K + k];
+    bf16 *dA = nullptr, *dB = nullptr;
+    float *dD = nullptr, *dz = nullptr;
+    int* derr = nullptr;
+    int rc = DV_OK;
+    if (cudaMalloc((void**)&dA, ap.size() * 2) != cudaSuccess || cudaMalloc((void**)&dB, bp.size() * 2) != cudaSuccess ||
+        cudaMalloc((void**)&dD, sizeof(float) * (size_t)M * N) != cudaSuccess ||
+        cudaMalloc((void**)&dz, sizeof(float) * N) != cudaSuccess || cudaMalloc((void**)&derr, sizeof(int)) != cudaSuccess)
+        rc = cuda_fail(cudaGetLastError(), "cudaMalloc(gemm check)");
+    if (rc == DV_OK) {
+        cudaMemcpy(dA, ap.data(), ap.size() * 2, cudaMemcpyHostToDevice);
+        cudaMemcpy(dB, bp.data(), bp.size() * 2, cudaMemcpyHostToDevice);
+        cudaMemset(dz, 0, sizeof(float) * N);
+        cudaMemset(derr, 0, sizeof(int));
+        GemmP g;
+        memset(&g, 0, sizeof g);
+        g.A = dA; g.ra = M; g.B = dB; g.rb = N; g.N = N; g.kpanels = K / 8; g.mode = E_OUT; g.rows_valid = M;
+        g.bias = dz; g.of = dD; g.ldf = N; g.err = derr;
+        rc = gemm(g, M / 128, 0);
+        if (rc == DV_OK && cudaDeviceSynchronize() != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "k_gemm");
+        int e = 0;
+        if (rc == DV_OK) cudaMemcpy(&e, derr, sizeof(int), cudaMemcpyDeviceToHost);
+        if (rc == DV_OK && e) { set_error("dv_mlp: a tensor-core product's completion wait timed out"); rc = DV_ERR_CUDA; }
+        if (rc == DV_OK) cudaMemcpy(D, dD, sizeof(float) * (size_t)M * N, cudaMemcpyDeviceToHost);
+    }
+    for (void* q : {(void*)dA, (void*)dB, (void*)dD, (void*)dz, (void*)derr})
+        if (q) cudaFree(q);
+    return rc;
+}
+
 // Gradient of the batch loss mean((O - T)^2) over the used outputs for host features X [rows][NIN] and
 // targets T [rows][8] (already scaled; rows <= DV_MLP_BATCH), into grad [DV_MLP_NPARAM]; *loss = the mean.
 int dv_mlp_gradient_host(dv_mlp* n, const float* X, const float* T, int64_t rows, float* grad, double* loss) {

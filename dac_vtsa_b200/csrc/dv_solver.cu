@@ -631,6 +631,7 @@ static int check_device_error(dv_model* m);
 // the model's device error word: bit 1 a preconditioner sweep's bulk-copy wait timed out, bit 4 a
 // grid barrier of the cooperative Gram-Schmidt kernel timed out
 static const char* device_error_text(int e) {
+    if (e & 32) return "a preconditioner index fell outside its storage (the access was skipped)";
     if (e & 1) return "a bounded device wait (preconditioner bulk copy) timed out";
     if (e & 4) return "a bounded device wait (GMRES grid barrier) timed out";
     return "a bounded device wait timed out";
@@ -1675,6 +1676,89 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
 
 }  // namespace dv
 
+namespace dv {
+// newton_modified (core/solver.py:111-151): Newton iterations with the stored factors as the
+// Jacobian, dz = -M^-1 R; positivity truncation; accepted on the contraction estimate
+// rate / (1 - rate) |dz| <= kappa (never on the first iterate), then the conservation check of
+// the next residual.  One synchronisation per iteration (the host takes the branch decisions).
+static int newton_modified(dv_model* m, double t, const double* z0, const double* rhs_known, double dh, int max_iter,
+                           double kappa, double fail_rate, double cons_tol, double rtol, double* zout, bool* ok,
+                           int* iters, double* rate, cudaStream_t st) {
+    Work& W = *m->W;
+    const int64_t n = m->n;
+    const int64_t npos = (int64_t)(DV_NG + DV_NA) * m->nc;
+    const unsigned g = vgrid(n);
+    auto copy = [&](const double* a, double* b) {
+        return cudaMemcpyAsync(b, a, sizeof(double) * n, cudaMemcpyDeviceToDevice, st) == cudaSuccess
+                   ? DV_OK : cuda_fail(cudaGetLastError(), "cudaMemcpyAsync");
+    };
+    auto finish = [&](const double* z, bool good, int it) -> int {
+        DV_TRY(copy(z, zout));
+        *ok = good;
+        *iters = it;
+        return DV_OK;
+    };
+    DV_TRY(copy(z0, W.z));
+    double nrm_prev = -1.0;
+    *rate = 0.0;
+    bool done = false;
+    for (int it = 0; it < max_iter + 2; ++it) {
+        DV_TRY(launch_rhs(m, t, W.z, W.f, nullptr, st));
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.z, -dh, W.f, W.R));
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.R, -1.0, rhs_known, W.R));
+        double rr = 0.0;
+        DV_TRY(rms_ratio(W, n, W.R, nullptr, &rr, st));
+        if (!std::isfinite(rr)) {
+            *rate = INFINITY;
+            return finish(z0, false, it);
+        }
+        if (done) {                                  // converged in the step norm: the balances
+            bool cok = true;
+            DV_LAUNCH(dv::K_VECTOR, st, k_scale<<<g, VB, 0, st>>>(m->nc, n, W.z, m->d_atol7, rtol, W.tmp));
+            DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<cons_grid(m->nc), VB, 0, st>>>(m->p, W.R, W.tmp, W.apart,
+                                                                                  W.tickets + 5, W.scal));
+            double v[8];
+            DV_TRY(fetch(W, W.scal, 8, v, st));
+            for (int q = 0; q < 4; ++q)
+                if (!(std::fabs(v[q]) <= cons_tol * v[4 + q])) cok = false;
+            if (cok || it >= max_iter + 1) return finish(W.z, true, it);
+        } else if (it >= max_iter) {
+            break;
+        }
+        DV_TRY(precond_apply(m, W.R, nullptr, W.dz, st));                    // z_new = z - M^-1 R
+        DV_LAUNCH(dv::K_VECTOR, st, k_truncate<<<g, VB, 0, st>>>(n, npos, W.z, -1.0, W.dz, W.zt));
+        DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.zt, -1.0, W.z, W.r));
+        DV_LAUNCH(dv::K_VECTOR, st, k_scale<<<g, VB, 0, st>>>(m->nc, n, W.zt, m->d_atol7, rtol, W.s));
+        double nrm = 0.0;
+        DV_TRY(rms_ratio(W, n, W.r, W.s, &nrm, st));
+        DV_TRY(copy(W.zt, W.z));
+        if (!std::isfinite(nrm)) {
+            *rate = INFINITY;
+            return finish(z0, false, it + 1);
+        }
+        if (done) continue;
+        // no acceptance on the first iterate: a stale factorisation can give a small update while the
+        // residual is still large; the rate estimate needs two iterates
+        if (nrm_prev >= 0.0) {
+            *rate = nrm / std::max(nrm_prev, 1e-300);
+            if (*rate >= fail_rate) return finish(W.z, false, it + 1);
+            if (*rate / (1.0 - *rate) * nrm <= kappa) {
+                if (cons_tol <= 0.0) return finish(W.z, true, it + 1);
+                done = true;
+            }
+        } else if (nrm < 1e-8) {
+            if (cons_tol <= 0.0) {
+                *rate = 0.0;
+                return finish(W.z, true, it + 1);
+            }
+            done = true;
+        }
+        nrm_prev = nrm;
+    }
+    return finish(W.z, false, max_iter);
+}
+}  // namespace dv
+
 // ================================================================== integrator (TRBDF2, core/solver.py:297-511)
 namespace dv {
 
@@ -1746,6 +1830,7 @@ struct dv_integrator {
     double h_prev;                // size of the last accepted step
     bool have_prev;               // yprev and h_prev hold the step before the current state
     int64_t *d_pick, *h_pick;     // [0] network guess chosen, [1] extrapolation chosen (device; pinned copy)
+    int mode;                     // Newton mode: 0 krylov, 1 hybrid, 2 modified (TRBDF2.mode)
 };
 
 namespace dv {
@@ -1803,6 +1888,66 @@ static int predict_stage(dv_integrator* g, const mlp::StageInputs& in, double t,
 }
 
 // A bounded device wait that gave up leaves a flag in the model; surface it as an error.
+// One implicit stage (TRBDF2._solve_stage, core/solver.py:339-368) from g->pred: modified Newton first
+// in the hybrid (at most 4 iterations, rate limit 0.5) and modified (max_newton_iter, 0.9) modes, and
+// Newton-Krylov otherwise or when the hybrid attempt fails.  With the learned predictor, a failure
+// from the network's start is repeated from the extrapolation (g->zext, saved by predict_stage).
+// `no` carries the step's refresh permission (the reference's self._fresh, set before stage 1).
+static int solve_stage(dv_integrator* g, const dv_newton_opts& no, double ts, const double* rhs, double dh, bool saved,
+                       double* out, bool* ok_out, double* rate_out, cudaStream_t st) {
+    dv_model* m = g->m;
+    Work& W = *m->W;
+    dv_step_report& R = g->rep;
+    const int64_t n = g->n, npos = (int64_t)(DV_NG + DV_NA) * m->nc;
+    *ok_out = false;
+    *rate_out = INFINITY;
+    const double* starts[2] = {g->pred, (saved && g->pred_on) ? g->zext : nullptr};
+    for (int attempt = 0; attempt < 2 && starts[attempt]; ++attempt) {
+        dv_newton_opts o = no;
+        if (attempt == 1) {
+            R.pred_retry += 1;
+            o.allow_refresh = g->fresh ? 0 : 1;
+        }
+        if (g->mode != 0) {
+            bool okm = false;
+            int it = 0;
+            double rate = 0.0;
+            DV_TRY(newton_modified(m, ts, starts[attempt], rhs, dh, g->mode == 2 ? o.max_iter : 4, o.kappa,
+                                   g->mode == 2 ? 0.9 : 0.5, o.cons_tol, o.rtol, out, &okm, &it, &rate, st));
+            R.newton_iters += it;
+            if (okm || g->mode == 2) {
+                *ok_out = okm;
+                *rate_out = rate;
+                if (okm) return DV_OK;
+                continue;
+            }
+            R.modified_fail += 1;
+        }
+        dv_newton_result r;
+        memset(&r, 0, sizeof r);
+        NewtonCtx C{m, &W, m->d_atol7, n, npos, o, &r, &g->gm};
+        DV_TRY(newton_krylov(C, ts, starts[attempt], rhs, dh, out, st));
+        R.n_krylov += 1;
+        R.newton_iters += r.iters;
+        R.gmres_iters += r.gmres_iters;
+        R.gmres_polish += r.gmres_polish;
+        R.balance_unclosed += r.balance_unclosed;
+        R.jac_refresh_in_newton += r.jac_refresh_in_newton;
+        if (r.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
+        if (r.refreshed) {                // Jacobian and factors were replaced inside the stage
+            R.n_jac += 1;
+            R.n_lu += 1;
+            g->h_lu = dh / D_;
+            g->jac_age = 0;
+            g->fresh = true;
+        }
+        *ok_out = r.ok != 0;
+        *rate_out = r.ok ? 0.0 : r.rate;
+        if (r.ok) return DV_OK;
+    }
+    return DV_OK;
+}
+
 // After a reported timeout nothing of the abandoned wait is in flight (the caller synchronised):
 // clear the error word and the ticket counters the abandoned reduction or barrier left behind, so
 // the model's next call starts clean.
@@ -2078,6 +2223,7 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
         pc_need = std::max(pc_need, cneed);
     }
     int64_t work_need = precond_work_doubles(m->pc_cap_nb, m->pc_cap_parts, p->Nz);
+    m->pc_doubles = pc_need;
     const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
     bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
                 cudaMalloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
@@ -2196,6 +2342,15 @@ int dv_precond_partitions(const dv_model* m, int32_t* mode, int32_t* zs, int32_t
     return DV_OK;
 }
 
+int dv_precond_check_maps(const dv_step_params* p, int32_t mode, int32_t* nparts, int32_t* nb, int64_t* violations) {
+    if (!p || !nparts || !nb || !violations) { set_error("null argument"); return DV_ERR_ARG; }
+    int np = 0, b = 0;
+    *violations = precond_check_maps(*p, mode, &np, &b);
+    *nparts = np;
+    *nb = b;
+    return DV_OK;
+}
+
 int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream) {
     if (!m || !b || !x) { set_error("null argument"); return DV_ERR_ARG; }
     return precond_apply(m, b, nullptr, x, (cudaStream_t)stream);
@@ -2245,6 +2400,14 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
     g->o = *o;
     g->n = m->n;
     g->log_refactor = std::log(o->refactor_ratio);
+    if (o->newton_mode < 0 || o->newton_mode > 2) {
+        delete g;
+        set_error("newton_mode must be 0 (krylov), 1 (hybrid) or 2 (modified)");
+        return DV_ERR_ARG;
+    }
+    // modified Newton needs exact factors; with partitioned (approximate) ones it keeps the Krylov
+    // fallback (core/solver.py:328-329)
+    g->mode = (o->newton_mode == 2 && o->precond_mode != 1) ? 1 : o->newton_mode;
     m->op32 = (o->krylov_fp32 & DV_KRYLOV_FP32_OPERATOR) ? 1 : 0;
     if (m->pc_fp32 != ((o->krylov_fp32 & DV_KRYLOV_FP32_FACTORS) ? 1 : 0)) {   // factors rebuilt in the requested storage
         m->pc_fp32 = (o->krylov_fp32 & DV_KRYLOV_FP32_FACTORS) ? 1 : 0;
@@ -2392,7 +2555,7 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
             g->fresh = true;
             g->have_lu = false;
         }
-        if (!g->have_lu || std::fabs(std::log(h / g->h_lu)) > g->log_refactor) {
+        if (!g->have_lu || std::fabs(std::log(h / g->h_lu)) > (g->mode == 2 ? 0.35 : g->log_refactor)) {
             DV_TRY(precond_factor(m, W.J, D_ * h, g->o.precond_mode, st));
             g->h_lu = h;
             R.n_lu += 1;
@@ -2428,47 +2591,11 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
             DV_TRY(predict_stage(g, in1, g->t + c_mid * h, g->rhs1, dh, first1, cnt1, &saved1, st));
         }
         no.allow_refresh = g->fresh ? 0 : 1;          // self._fresh = fresh (set before stage 1)
-        dv_newton_result r1;
-        memset(&r1, 0, sizeof r1);
-        NewtonCtx C1{m, &W, m->d_atol7, n, npos, no, &r1, &g->gm};
-        DV_TRY(newton_krylov(C1, g->t + c_mid * h, g->pred, g->rhs1, dh, g->z1, st));
-        R.n_krylov += 1;
-        R.newton_iters += r1.iters;
-        R.gmres_iters += r1.gmres_iters;
-        R.gmres_polish += r1.gmres_polish;
-        R.balance_unclosed += r1.balance_unclosed;
-        R.jac_refresh_in_newton += r1.jac_refresh_in_newton;
-        if (r1.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
-        if (!r1.ok && saved1 && g->pred_on) {         // the network's start failed: again from the extrapolation
-            R.pred_retry += 1;
-            no.allow_refresh = (g->fresh || r1.refreshed) ? 0 : 1;
-            if (r1.refreshed) {
-                R.n_jac += 1;
-                R.n_lu += 1;
-                g->h_lu = dh / D_;
-                g->jac_age = 0;
-                g->fresh = true;
-            }
-            memset(&r1, 0, sizeof r1);
-            DV_TRY(newton_krylov(C1, g->t + c_mid * h, g->zext, g->rhs1, dh, g->z1, st));
-            R.n_krylov += 1;
-            R.newton_iters += r1.iters;
-            R.gmres_iters += r1.gmres_iters;
-            R.gmres_polish += r1.gmres_polish;
-            R.balance_unclosed += r1.balance_unclosed;
-            R.jac_refresh_in_newton += r1.jac_refresh_in_newton;
-            if (r1.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
-        }
-        if (r1.ok && saved1 && g->rec_stride > 0)
+        bool ok = false;
+        double r1 = 0.0, r2 = 0.0;
+        DV_TRY(solve_stage(g, no, g->t + c_mid * h, g->rhs1, dh, saved1, g->z1, &ok, &r1, st));
+        if (ok && saved1 && g->rec_stride > 0)
             DV_TRY(mlp::record_targets(g->mlp, in1, g->z1, g->zext, first1, g->rec_stride, cnt1, st));
-        if (r1.refreshed) {
-            R.n_jac += 1;
-            R.n_lu += 1;
-            g->h_lu = dh / D_;
-            g->jac_age = 0;
-            g->fresh = true;
-        }
-        bool ok = r1.ok != 0;
         if (ok) {
             if (sd) {
                 DV_LAUNCH(dv::K_VECTOR, st, k_sd_rhs2<<<gr, VB, 0, st>>>(n, g->y, g->z1, dh, (1.0 - G_SD_) * h, g->rhs2));
@@ -2484,48 +2611,9 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
                 in2 = stage_inputs(g, g->z1, g->y, W.f, (1.0 - c_mid) * h, c_mid * h, h, 1);
                 DV_TRY(predict_stage(g, in2, g->t + h, g->rhs2, dh, first2, cnt2, &saved2, st));
             }
-            dv_newton_result r2;
-            memset(&r2, 0, sizeof r2);
-            NewtonCtx C2{m, &W, m->d_atol7, n, npos, no, &r2, &g->gm};
-            DV_TRY(newton_krylov(C2, g->t + h, g->pred, g->rhs2, dh, g->z2, st));
-            R.n_krylov += 1;
-            R.newton_iters += r2.iters;
-            R.gmres_iters += r2.gmres_iters;
-            R.gmres_polish += r2.gmres_polish;
-            R.balance_unclosed += r2.balance_unclosed;
-            R.jac_refresh_in_newton += r2.jac_refresh_in_newton;
-            if (r2.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
-            if (!r2.ok && saved2 && g->pred_on) {
-                R.pred_retry += 1;
-                if (r2.refreshed) {
-                    R.n_jac += 1;
-                    R.n_lu += 1;
-                    g->h_lu = dh / D_;
-                    g->jac_age = 0;
-                    g->fresh = true;
-                }
-                no.allow_refresh = g->fresh ? 0 : 1;
-                memset(&r2, 0, sizeof r2);
-                NewtonCtx C2b{m, &W, m->d_atol7, n, npos, no, &r2, &g->gm};
-                DV_TRY(newton_krylov(C2b, g->t + h, g->zext, g->rhs2, dh, g->z2, st));
-                R.n_krylov += 1;
-                R.newton_iters += r2.iters;
-                R.gmres_iters += r2.gmres_iters;
-                R.gmres_polish += r2.gmres_polish;
-                R.balance_unclosed += r2.balance_unclosed;
-                R.jac_refresh_in_newton += r2.jac_refresh_in_newton;
-                if (r2.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
-            }
-            if (r2.ok && saved2 && g->rec_stride > 0)
+            DV_TRY(solve_stage(g, no, g->t + h, g->rhs2, dh, saved2, g->z2, &ok, &r2, st));
+            if (ok && saved2 && g->rec_stride > 0)
                 DV_TRY(mlp::record_targets(g->mlp, in2, g->z2, g->zext, first2, g->rec_stride, cnt2, st));
-            if (r2.refreshed) {
-                R.n_jac += 1;
-                R.n_lu += 1;
-                g->h_lu = dh / D_;
-                g->jac_age = 0;
-                g->fresh = true;
-            }
-            ok = r2.ok != 0;
         }
         if (!ok) {
             R.n_newton_fail += 1;
@@ -2592,7 +2680,8 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
         g->j32_fresh = false;
         g->jac_age += 1;
         g->fresh = false;
-        if (g->gm - gm0 > g->o.gmres_refresh) g->jac_age = g->o.jacobian_max_age;
+        if ((g->mode == 2 && std::max(r1, r2) > 0.5) || g->gm - gm0 > g->o.gmres_refresh)
+            g->jac_age = g->o.jacobian_max_age;       // stale Jacobian / factors: refresh next step
         double fac = (en < 1e-8) ? 4.0 : std::min(4.0, std::max(0.2, 0.9 * std::pow(en, -1.0 / 3.0)));
         if (1.0 <= fac && fac < 1.25) fac = 1.0;
         double hn = truncated ? std::max(h * fac, h_desired) : h * fac;

@@ -126,7 +126,7 @@ def _(model, t, z0, rhs_known, dh, max_iter, kappa, rtol, cons_tol, precond_mode
 
 REPORT_FIELDS = ("t", "h_used", "err_norm", "n_steps", "n_reject", "n_newton_fail", "n_krylov", "n_jac", "n_lu",
                  "nfev", "gmres_iters", "gmres_polish", "balance_unclosed", "jac_refresh_in_newton", "krylov_ok",
-                 "krylov_fail", "newton_iters", "pred_net", "pred_extrap", "pred_retry")
+                 "krylov_fail", "newton_iters", "pred_net", "pred_extrap", "pred_retry", "modified_fail")
 
 
 @torch.library.custom_op("dacvtsa::step", mutates_args=())

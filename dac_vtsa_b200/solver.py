@@ -59,8 +59,6 @@ class TRBDF2:
         self.m = model
         self.lib = load()
         s = cfg.solver
-        if s.newton_mode != "krylov":
-            raise NotImplementedError("the GPU integrator implements newton_mode = krylov (the default)")
         self.rtol = s.rtol
         self.atol = model.atol
         self.h_max = h_max
@@ -92,6 +90,9 @@ class TRBDF2:
         o.conservation_tol = float(s.conservation_tol or 0.0)
         o.h_max = h_max
         o.h_init = self.h_init
+        # newton_mode: krylov (default), hybrid (modified Newton first, Krylov fallback) or modified
+        o.newton_mode = {"krylov": 0, "hybrid": 1, "modified": 2}[s.newton_mode]
+        self.mode = "hybrid" if (s.newton_mode == "modified" and self.precond == "theta_block") else s.newton_mode
         # gpu.krylov_precision: fp64 (default, the parity path); fp32 (GMRES on the FP32 assembled
         # Jacobian with FP32 preconditioner factors, FP64 residual / Newton update as refinement);
         # fp32_factors (only the factors in FP32)
@@ -220,6 +221,7 @@ class TRBDF2:
                                "balance_unclosed": rep.balance_unclosed,
                                "jac_refresh_in_newton": rep.jac_refresh_in_newton,
                                "newton_iters": rep.newton_iters, "pred_net": rep.pred_net,
-                               "pred_extrap": rep.pred_extrap, "pred_retry": rep.pred_retry})
+                               "pred_extrap": rep.pred_extrap, "pred_retry": rep.pred_retry,
+                               "modified_fail": rep.modified_fail})
             res.wall_time = time.time() - wall0
             return res

@@ -212,6 +212,10 @@ int dv_model_set_krylov_fp32(dv_model* m, int32_t mask);
  * core ring in theta groups), the first twisted separator plane (0: one direction), and each
  * partition's block size (up to cap entries).  Host call. */
 int dv_precond_partitions(const dv_model* m, int32_t* mode, int32_t* zs, int32_t* nb, int32_t cap, int32_t* nparts);
+/* Host self-check of the partition maps the factorisation and sweep use for grid p in `mode` (no
+ * reference counterpart; no device work): *violations counts unknowns not covered exactly once,
+ * indices outside the state and disagreements between the forward and inverse maps. */
+int dv_precond_check_maps(const dv_step_params* p, int32_t mode, int32_t* nparts, int32_t* nb, int64_t* violations);
 /* x = M^-1 b with the stored factors (lu.solve). b and x may alias. */
 int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream);
 
@@ -242,6 +246,9 @@ typedef struct dv_solver_opts {
     int32_t krylov_fp32;       /* DV_KRYLOV_FP32_* mask (see dv_model_set_krylov_fp32) */
     int64_t max_steps;
     double rtol, newton_kappa, refactor_ratio, conservation_tol, h_max, h_init;
+    int32_t newton_mode;       /* 0 krylov (default), 1 hybrid, 2 modified (solver.newton_mode); modified with
+                                  partitioned factors runs as hybrid, as the reference does (core/solver.py:328) */
+    int32_t pad_;
 } dv_solver_opts;
 
 typedef struct dv_step_report {
@@ -252,6 +259,7 @@ typedef struct dv_step_report {
     int64_t newton_iters;      /* Newton iterations of all stage solves */
     int64_t pred_net, pred_extrap;   /* stage starts taken from the network / from the extrapolation */
     int64_t pred_retry;        /* stage solves repeated from the extrapolation after the network's start failed */
+    int64_t modified_fail;     /* hybrid mode: modified-Newton attempts that fell back to Newton-Krylov */
 } dv_step_report;
 
 /* TRBDF2(model, cfg, h_max, h_init) (core/solver.py:298-329) */
@@ -320,6 +328,10 @@ int64_t dv_mlp_sample_count(const dv_mlp* net);
 int dv_mlp_clear_samples(dv_mlp* net);
 /* Forward pass of host feature rows X [rows][DV_MLP_NIN] (rounded to BF16) -> out [rows][DV_MLP_NOUT]. */
 int dv_mlp_forward_host(dv_mlp* net, const float* X, int64_t rows, float* out);
+/* One BF16 tensor-core product D[M][N] = A[M][K] B[N][K]^T (host fp32 in, rounded to BF16; FP32 out)
+ * by the network's product kernel: M a multiple of 128, N in 16..128 a multiple of 16, K a multiple
+ * of 16.  A check of the kernel; allocates its own device buffers. */
+int dv_mlp_gemm_host(int32_t M, int32_t N, int32_t K, const float* A, const float* B, float* D);
 /* Gradient of the mean squared error of the first 6 outputs against T [rows][8] (rows <= DV_MLP_BATCH)
  * by the backward kernels, into grad [DV_MLP_NPARAM]; *loss = the mean squared error. */
 int dv_mlp_gradient_host(dv_mlp* net, const float* X, const float* T, int64_t rows, float* grad, double* loss);

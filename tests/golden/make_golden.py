@@ -20,6 +20,7 @@ Writes (all small, committed):
                          (core/solver.py:370-511)
   state_csv/seeded_3x4x6*  (--csv) a seeded state written by the reference's save_state_csv
                          (the 17-digit hand-off format, simio/checkpoint.py:27-53)
+  newton_modes_4x4x16.npz (--modes) 200 s adsorption with newton_mode hybrid and modified
   stop_young2021.npz     (--stop) the young2021 1-D case's adsorption step, stopped by its
                          end_saturation criterion (core/residual.py:445-482, core/solver.py:
                          476-494): stop time, stop value, end state
@@ -456,9 +457,11 @@ def make_stop_golden(ref_root):
 if __name__ == "__main__":
     if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
         raise SystemExit("usage: make_golden.py <reference checkout> [--outlet | --bench-state | "
-                         "--bench-state-heating | --cycle [--rtol X] | --stop | --csv]")
+                         "--bench-state-heating | --cycle [--rtol X] | --stop | --csv | --modes]")
     root = sys.argv[1]
-    if "--stop" in sys.argv:
+    if "--modes" in sys.argv:
+        pass                        # handled below
+    elif "--stop" in sys.argv:
         make_stop_golden(root)
     elif "--csv" in sys.argv:
         make_csv_golden(root)
@@ -473,3 +476,48 @@ if __name__ == "__main__":
         make_bench_state_heating(root)
     else:
         main(root)
+
+
+def make_modes_golden(ref_root):
+    """200 s adsorption of the 4x4x16 bed from the seeded constant-pressure state with the
+    reference's other Newton modes (core/solver.py:111-151,339-347): hybrid with its theta-block
+    factors, and modified with the full factorisation: end states, accepted steps and counters."""
+    sys.path.insert(0, ref_root)
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.residual import TVSAModel
+    from core.solver import TRBDF2
+    from core.state import initial_state
+    from properties import R_GAS, get_backend
+    out = {}
+    for name, extra in (("hybrid", {"solver.newton_mode": "hybrid"}),
+                        ("modified", {"solver.newton_mode": "modified", "solver.preconditioner": "full"})):
+        over = dict(CYCLE_POINT, **{"grid.Nr": 4, "grid.Ntheta": 4, "grid.Nz": 16}, **extra)
+        cfg = rp.load_config(override_dict=over)
+        g = Grid.from_config(cfg)
+        props = get_backend(cfg)
+        st = initial_state(cfg, g, props)
+        rng = np.random.default_rng(0)
+        T = 288.0 * (1.0 + 0.01 * (2.0 * rng.random(g.shape) - 1.0))
+        st.c = (st.c / st.c.sum(axis=0)) * (101325.0 / (R_GAS * T))[None]
+        st.T = T
+        st.Tw = np.full(g.wall_shape, 288.0)
+        step = dict(cfg.cycle[0])
+        step["duration"] = 200.0
+        m = TVSAModel(cfg, g, props, step, st)
+        integ = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * 200.0)
+        y0 = m.pack(st)
+        res = integ.integrate(y0, 200.0, [200.0])
+        out[f"{name}_over"] = np.array(json.dumps(over))
+        out[f"{name}_y0"] = y0
+        out[f"{name}_P0"] = st.P
+        out[f"{name}_y"] = res.y
+        out[f"{name}_stats"] = np.array(json.dumps({"steps": res.n_steps, "rejected": res.n_reject,
+                                                    "newton_fail": res.n_newton_fail, "krylov": res.n_krylov,
+                                                    **{k: int(v) for k, v in integ.stats.items()}}))
+        print(name, res.n_steps, integ.stats, flush=True)
+    np.savez_compressed(os.path.join(HERE, "newton_modes_4x4x16.npz"), **out)
+
+
+if __name__ == "__main__" and "--modes" in sys.argv:
+    make_modes_golden(sys.argv[1])
