@@ -96,7 +96,7 @@ _DEFAULTS: Dict[str, Any] = {
                "jacobian_max_age": 40, "limiter": "van_albada", "max_steps_per_step": 200000,
                "outlet_record_every": 1},
     # GPU-only knobs live in their own namespace so reference configs stay valid.
-    "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation", "predictor_weights": ""},
+    "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation", "predictor_weights": "", "max_polish": 2},
 }
 
 # Choices checked by validate(); everything else is type-checked against the default.
@@ -204,6 +204,13 @@ def _check(key: str, value: Any, default: Any) -> Any:
         if not isinstance(value, bool):
             raise ConfigError(f"{key} must be a bool")
         return value
+    if isinstance(default, (int, float)) and isinstance(value, str):
+        # YAML 1.1 (PyYAML) reads e.g. 2.0e4 as a string: numeric strings count as numbers, as in the
+        # reference's schema (config/schema.py:386-391)
+        try:
+            value = float(value)
+        except ValueError:
+            raise ConfigError(f"{key}: expected a number, got {value!r}") from None
     if isinstance(default, int) and not isinstance(default, bool):
         if isinstance(value, bool) or not isinstance(value, (int, float)) or int(value) != value:
             raise ConfigError(f"{key} must be an integer")
@@ -218,6 +225,11 @@ def _check(key: str, value: Any, default: Any) -> Any:
 
 
 def _resolve(raw: Dict, value: Any) -> Any:
+    if isinstance(value, str):
+        try:                                   # a numeric string (YAML 1.1 reads 2.0e4 as one) is a number
+            return float(value)
+        except ValueError:
+            pass
     if isinstance(value, str) and "." in value:
         try:
             return float(_get_dotted(raw, value))

@@ -921,6 +921,7 @@ __global__ void __launch_bounds__(256) k_pc_factor_glob(PcGeom gin, double* __re
     const int nb = g.nb, ld = g.ld;
     const int64_t n2 = (int64_t)nb * ld;
     const int64_t bs = g.bs;
+    if (!pc_range_ok(g, (int64_t)part * g.Nz * 5 * bs, (int64_t)g.Nz * 5 * bs)) return;   // geometry beyond the storage
     double* base = A + (int64_t)part * g.Nz * 5 * bs;
     const int64_t n2w = (int64_t)gin.nb * ld;          // workspace stride: the largest partition's block
     double* T = work + (int64_t)part * 4 * n2w;
@@ -1349,6 +1350,7 @@ __global__ void __launch_bounds__(512) k_pc_apply_glob(PcGeom gin, const TS* __r
     const int tid = threadIdx.x;
     const int64_t bs = g.bs;
     double* xs = xs_all + (int64_t)part * g.Nz * ld;
+    if (!pc_range_ok(g, (int64_t)part * g.Nz * 5 * bs, (int64_t)g.Nz * 5 * bs)) return;   // geometry beyond the storage
     const TS* base = A + (int64_t)part * g.Nz * 5 * bs;
     for (int64_t q = tid; q < (int64_t)g.Nz * nb; q += blockDim.x) {
         int k = (int)(q / nb), l = (int)(q % nb);
@@ -1399,6 +1401,8 @@ static PcGeom geom_of_params(const dv_step_params& p, int mode) {
     g.cap = -1;
     g.nstate = (int64_t)DV_NV * p.Nr * p.Nth * p.Nz + (p.wall_on ? (int64_t)p.Nth * p.Nz : 0);
     g.err = nullptr;
+    // mode 3 is the split form of mode 2 (a factorisation records it as the mode it used): derive it again
+    if (mode == 3) mode = 2;
     // mode 2 needs a second ring and a second sector; below that it is mode 0 (or 1 for one sector)
     if (mode == 2 && (p.Nr < 2 || p.Nth < 2)) mode = 0;
     g.mode = (p.Nth > 1 && (mode == 0 || mode == 2)) ? mode : 1;

@@ -439,8 +439,10 @@ __global__ void k_pack_weights(const float* __restrict__ P, bf16* W1, bf16* W2, 
 static unsigned g1(int64_t n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
 static int pack(dv_mlp* net, cudaStream_t s) {
-    DV_LAUNCH(dv::K_MLP, s, k_pack_weights<<<g1((int64_t)NH * NIN), 256, 0, s>>>(net->P, net->W1, net->W2, net->W3,
-                                                                                 net->W4, net->W2t, net->W3t, net->W4t));
+    // one thread per entry of the largest matrix (W2, W3: NH x NH)
+    const int64_t most = std::max<int64_t>((int64_t)NH * NIN, std::max<int64_t>((int64_t)NH * NH, (int64_t)NOUT * NH));
+    DV_LAUNCH(dv::K_MLP, s, k_pack_weights<<<g1(most), 256, 0, s>>>(net->P, net->W1, net->W2, net->W3, net->W4, net->W2t,
+                                                                     net->W3t, net->W4t));
     return launch_ok("k_pack_weights");
 }
 

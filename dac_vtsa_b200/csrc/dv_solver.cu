@@ -627,6 +627,7 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
 
 
 static int check_device_error(dv_model* m);
+static void clear_device_error(dv_model* m);
 
 // the model's device error word: bit 1 a preconditioner sweep's bulk-copy wait timed out, bit 4 a
 // grid barrier of the cooperative Gram-Schmidt kernel timed out
@@ -1374,6 +1375,8 @@ static int gmres_graph_collect(Work& W, dv_model* m, int* info, int64_t* inner) 
     if (g_prof_on && !g_pending.empty()) prof_flush();
     if (hst->err != 0) {                  // (read back with the results: no extra round trip)
         set_error(device_error_text(hst->err));
+        hst->err = 0;
+        clear_device_error(m);
         return DV_ERR_CUDA;
     }
     return DV_OK;
@@ -1641,7 +1644,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
                 r.ok = 1; r.iters = it + 1; r.rate = rate;
                 return DV_OK;
             }
-            if (polish < 2) {
+            if (polish < (C.o.max_polish > 0 ? C.o.max_polish : 2)) {
                 polish += 1;
                 step_prev = -1.0;
                 continue;
@@ -2100,6 +2103,8 @@ int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps,
     no.eta = 1e-2;
     no.rtol = 1e-4;
     no.cons_tol = 0.0;
+    no.max_polish = 2;
+    no.pad_ = 0;
     bestv = INFINITY;
     int rc = DV_OK;
     const int64_t nfev0 = m->nfev;
@@ -2524,6 +2529,7 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
     no.eta = 1e-2;
     no.rtol = g->o.rtol;
     no.cons_tol = g->o.conservation_tol;
+    no.max_polish = g->o.max_polish;
     while (g->t < g->t_end * (1.0 - 1e-12)) {
         const int64_t gm0 = g->gm;
         if (R.n_steps + R.n_reject + R.n_newton_fail > g->o.max_steps) {

@@ -223,6 +223,8 @@ int dv_precond_solve(dv_model* m, const double* b, double* x, void* stream);
 typedef struct dv_newton_opts {
     int32_t max_iter, krylov_dim, allow_refresh, precond_mode;
     double kappa, eta, rtol, cons_tol;
+    int32_t max_polish;        /* conservation-polish iterations after convergence (reference: 2; 0 = 2) */
+    int32_t pad_;
 } dv_newton_opts;
 
 typedef struct dv_newton_result {
@@ -248,7 +250,7 @@ typedef struct dv_solver_opts {
     double rtol, newton_kappa, refactor_ratio, conservation_tol, h_max, h_init;
     int32_t newton_mode;       /* 0 krylov (default), 1 hybrid, 2 modified (solver.newton_mode); modified with
                                   partitioned factors runs as hybrid, as the reference does (core/solver.py:328) */
-    int32_t pad_;
+    int32_t max_polish;        /* conservation-polish iterations of a stage (reference: 2; 0 = 2) */
 } dv_solver_opts;
 
 typedef struct dv_step_report {
