@@ -77,7 +77,8 @@ class DvStepParams(C.Structure):
 
 class DvNewtonOpts(C.Structure):
     _fields_ = [("max_iter", I32), ("krylov_dim", I32), ("allow_refresh", I32), ("precond_mode", I32),
-                ("kappa", D), ("eta", D), ("rtol", D), ("cons_tol", D), ("max_polish", I32), ("pad_", I32)]
+                ("kappa", D), ("eta", D), ("rtol", D), ("cons_tol", D), ("max_polish", I32),
+                ("polish_cycles", I32)]
 
 
 class DvNewtonResult(C.Structure):
@@ -90,7 +91,8 @@ class DvSolverOpts(C.Structure):
     _fields_ = [("scheme", I32), ("max_newton_iter", I32), ("jacobian_max_age", I32), ("gmres_refresh", I32),
                 ("precond_mode", I32), ("krylov_fp32", I32), ("max_steps", I64),
                 ("rtol", D), ("newton_kappa", D), ("refactor_ratio", D), ("conservation_tol", D),
-                ("h_max", D), ("h_init", D), ("newton_mode", I32), ("max_polish", I32)]
+                ("h_max", D), ("h_init", D), ("newton_mode", I32), ("max_polish", I32), ("polish_cycles", I32),
+                ("pad_", I32)]
 
 
 class DvTuning(C.Structure):

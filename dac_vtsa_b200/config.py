@@ -96,7 +96,8 @@ _DEFAULTS: Dict[str, Any] = {
                "jacobian_max_age": 40, "limiter": "van_albada", "max_steps_per_step": 200000,
                "outlet_record_every": 1},
     # GPU-only knobs live in their own namespace so reference configs stay valid.
-    "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation", "predictor_weights": "", "max_polish": 2},
+    "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation", "predictor_weights": "", "max_polish": 2,
+            "polish_cycles": 1},
 }
 
 # Choices checked by validate(); everything else is type-checked against the default.

@@ -534,16 +534,14 @@ static int gmres(Work& W, const Op& op, const double* b, double rtol, double ato
     DV_TRY(fetch(W, W.scal + 9, 1, &bn2, st));
     const double atol_eff = std::max(atol, rtol * bn2);
     *info = 0;
-    if (bn2 == 0.0) {
+    if (bn2 == 0.0 || bn2 < atol_eff) {       // ||r0|| < atol with x0 = 0: x = 0, u = prec(x) = 0, r = b
         DV_CUDA(cudaMemsetAsync(W.x, 0, sizeof(double) * n, st));
+        DV_CUDA(cudaMemsetAsync(W.u, 0, sizeof(double) * n, st));
+        if (b != W.r) DV_CUDA(cudaMemcpyAsync(W.r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
         return DV_OK;
     }
     double ptol = bn2 * std::min(1.0, atol_eff / bn2);
     const double eps = std::numeric_limits<double>::epsilon();
-    if (bn2 < atol_eff) {       // ||r0|| < atol with x0 = 0
-        DV_CUDA(cudaMemsetAsync(W.x, 0, sizeof(double) * n, st));
-        return DV_OK;
-    }
     const int64_t ldv = n;
     DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<vgrid(n), VB, 0, st>>>(n, 1.0 / bn2, b, 0.0, nullptr, W.V));      // v0 = r / ||r||
     std::vector<double> H((size_t)kdim * (kdim + 1), 0.0), S(kdim + 1, 0.0), gc(kdim), gs(kdim);
@@ -1576,6 +1574,30 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             r.gmres_iters += inner2;
             if (C.gm_counter) *C.gm_counter += inner2;
         }
+        // polish: further restart cycles on the true linear residual r = b - A P^-1 x until the
+        // polish tolerance (1e-3 of ||b||) or the cycle limit; prec() is linear, so the cycles'
+        // corrections u = P^-1 x add up.  The speculation queued behind the first cycle is void.
+        const int pcyc = std::min(std::max(C.o.polish_cycles, 1), 8);
+        if (polish && info != 0 && pcyc > 1) {
+            spec_ok = false;
+            m->nfev -= 1;
+            double bn0 = 0.0;
+            DV_TRY(rms_ratio(W, n, W.b, nullptr, &bn0, st));
+            DV_TRY(copy(W.u, W.dz));                          // dz: the summed correction
+            for (int cyc = 1; cyc < pcyc && info != 0; ++cyc) {
+                double rk = 0.0;
+                DV_TRY(rms_ratio(W, n, W.r, nullptr, &rk, st));
+                if (!(rk > 0.0) || !std::isfinite(rk)) break;
+                DV_TRY(copy(W.r, W.b));
+                int64_t inner2 = 0;
+                DV_TRY(gmres_any(W, op, W.b, std::min(1.0, 1e-3 * bn0 / rk), floor_, C.o.krylov_dim, &info,
+                                 &inner2, st));
+                r.gmres_polish += inner2;
+                DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.dz, 1.0, W.u, W.dz));
+            }
+            DV_TRY(copy(W.dz, W.u));
+            DV_LAUNCH(dv::K_VECTOR, st, k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.b));     // b = -R/s again
+        }
         if (!spec_ok) {
             DV_TRY(speculate());
             DV_CUDA(cudaStreamSynchronize(st));
@@ -1878,11 +1900,15 @@ static int predict_stage(dv_integrator* g, const mlp::StageInputs& in, double t,
     if (g->rec_stride > 0) DV_TRY(mlp::record_features(g->mlp, in, first, g->rec_stride, cnt, st));
     if (!g->pred_on) return DV_OK;
     DV_TRY(mlp::predict(g->mlp, in, in.stage == 0 ? in.A : in.B, g->pred, st));
+    // each start is judged by its simplified Newton correction ||M^-1 R / s||, the distance to the
+    // stage solution that the Newton iteration measures progress by: the raw ||R / s|| is dominated
+    // by the stiff pressure couplings, where a state error far below tolerance leaves a large residual
     const double* cands[2] = {g->pred, g->zext};
     for (int q = 0; q < 2; ++q) {
         DV_TRY(launch_stage_residual(m, t, cands[q], dh, rhs_known, W.Rt, st));
+        DV_TRY(precond_apply(m, W.Rt, nullptr, W.tmp, st));
         DV_LAUNCH(dv::K_VECTOR, st, k_scale<<<gr, VB, 0, st>>>(m->nc, n, cands[q], m->d_atol7, g->o.rtol, W.w));
-        DV_TRY(rms_ratio_dev(W, n, W.Rt, W.w, 0, W.scal + 26 + q, st));
+        DV_TRY(rms_ratio_dev(W, n, W.tmp, W.w, 0, W.scal + 26 + q, st));
     }
     m->nfev += 2;
     DV_LAUNCH(dv::K_VECTOR, st, k_pick<<<gr, VB, 0, st>>>(n, W.scal + 26, g->zext, g->pred, g->d_pick));
@@ -2104,7 +2130,7 @@ int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps,
     no.rtol = 1e-4;
     no.cons_tol = 0.0;
     no.max_polish = 2;
-    no.pad_ = 0;
+    no.polish_cycles = 1;
     bestv = INFINITY;
     int rc = DV_OK;
     const int64_t nfev0 = m->nfev;
@@ -2530,6 +2556,7 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
     no.rtol = g->o.rtol;
     no.cons_tol = g->o.conservation_tol;
     no.max_polish = g->o.max_polish;
+    no.polish_cycles = g->o.polish_cycles;
     while (g->t < g->t_end * (1.0 - 1e-12)) {
         const int64_t gm0 = g->gm;
         if (R.n_steps + R.n_reject + R.n_newton_fail > g->o.max_steps) {

@@ -94,6 +94,8 @@ class TRBDF2:
         o.newton_mode = {"krylov": 0, "hybrid": 1, "modified": 2}[s.newton_mode]
         # gpu.max_polish: conservation-polish iterations per stage (the reference's 2 by default)
         o.max_polish = int(gpu_option(cfg, "max_polish", 2))
+        # gpu.polish_cycles: GMRES restart cycles of one polish iteration (the reference runs one)
+        o.polish_cycles = int(gpu_option(cfg, "polish_cycles", 1))
         self.mode = "hybrid" if (s.newton_mode == "modified" and self.precond == "theta_block") else s.newton_mode
         # gpu.krylov_precision: fp64 (default, the parity path); fp32 (GMRES on the FP32 assembled
         # Jacobian with FP32 preconditioner factors, FP64 residual / Newton update as refinement);

@@ -88,8 +88,17 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default="predictor_weights.npz")
     ap.add_argument("--eval", action="store_true", help="compare a held-out point's cycle with and without")
+    ap.add_argument("--load", default="", help="evaluate these weights (no recording or training)")
+    ap.add_argument("--eval-grid", type=int, nargs=3, default=None, help="grid of the evaluation (default --grid)")
     a = ap.parse_args(argv)
     torch.cuda.init()
+    eval_grid = tuple(a.eval_grid or a.grid)
+    if a.load:
+        held_out = operating_points(a.points + 1, a.seed)[-1]
+        net = NewtonPredictor.load(a.load)
+        print(json.dumps({"weights": a.load, "grid": list(eval_grid), "held_out_point": held_out,
+                          "gain": evaluate(net, eval_grid, held_out)}), flush=True)
+        return
     ncell = a.grid[0] * a.grid[1] * a.grid[2]
     # about 1200 converged stage solves per cycle: pick the stride for ~1e6 samples in total
     stride = a.stride or max(1, int(round(ncell * 1200 * a.points / 1.0e6)))
@@ -110,7 +119,7 @@ def main(argv=None):
            "weights": a.out}
     if a.eval:
         out["held_out_point"] = held_out
-        out["gain"] = evaluate(net, tuple(a.grid), held_out)
+        out["gain"] = evaluate(net, eval_grid, held_out)
     print(json.dumps(out), flush=True)
 
 

@@ -224,7 +224,8 @@ typedef struct dv_newton_opts {
     int32_t max_iter, krylov_dim, allow_refresh, precond_mode;
     double kappa, eta, rtol, cons_tol;
     int32_t max_polish;        /* conservation-polish iterations after convergence (reference: 2; 0 = 2) */
-    int32_t pad_;
+    int32_t polish_cycles;     /* GMRES restart cycles of one polish iteration's linear solve, stopping at its
+                                  tolerance (reference: 1, scipy gmres maxiter=1; 0 = 1; at most 8) */
 } dv_newton_opts;
 
 typedef struct dv_newton_result {
@@ -251,6 +252,8 @@ typedef struct dv_solver_opts {
     int32_t newton_mode;       /* 0 krylov (default), 1 hybrid, 2 modified (solver.newton_mode); modified with
                                   partitioned factors runs as hybrid, as the reference does (core/solver.py:328) */
     int32_t max_polish;        /* conservation-polish iterations of a stage (reference: 2; 0 = 2) */
+    int32_t polish_cycles;     /* GMRES restart cycles of a polish iteration (reference: 1; 0 = 1; at most 8) */
+    int32_t pad_;
 } dv_solver_opts;
 
 typedef struct dv_step_report {
