@@ -301,7 +301,14 @@ __global__ void k_features(StageInputs in, const double* __restrict__ nrm, int64
     }
 }
 
-// pred[v][c] = max(pred + out * oscale_v * s_v, 0.1 max(ytr, 0)) (the floor for c and q only)
+// The network's correction of the extrapolated start, per cell and variable, in units of that
+// cell's extrapolated increment |z_ext - A| plus 1 % of the error scale s: the extrapolation error
+// grows with the local rate of change (fronts, blowdown) and vanishes in quiet stages, so a target
+// in fixed error-scale units would give the network a constant error floor that quiet stages, where
+// the extrapolation is already close, cannot afford.
+__device__ __forceinline__ double increment_unit(double zext, double a, double sc) { return fabs(zext - a) + 1e-2 * sc; }
+
+// pred[v][c] = max(pred + out * oscale_v * unit, 0.1 max(ytr, 0)) (the floor for c and q only)
 __global__ void k_apply(StageInputs in, const double* __restrict__ nrm, const float* __restrict__ O,
                         const double* __restrict__ ytr, double* __restrict__ pred) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -310,7 +317,7 @@ __global__ void k_apply(StageInputs in, const double* __restrict__ nrm, const fl
     for (int v = 0; v < 6; ++v) {
         const int64_t q = v * in.nc + c;
         const double sc = in.atol7[v] + in.rtol * fabs(in.A[q]);
-        double z = pred[q] + (double)O[c * NOUT + v] * nrm[13 + v] * sc;
+        double z = pred[q] + (double)O[c * NOUT + v] * nrm[13 + v] * increment_unit(pred[q], in.A[q], sc);
         if (v < 5) z = fmax(z, 0.1 * fmax(ytr[q], 0.0));
         pred[q] = z;
     }
@@ -326,7 +333,7 @@ __global__ void k_targets(StageInputs in, const double* __restrict__ zs, const d
     for (int v = 0; v < 6; ++v) {
         const int64_t q = v * in.nc + c;
         const double sc = in.atol7[v] + in.rtol * fabs(in.A[q]);
-        t[v] = (float)((zs[q] - ze[q]) / sc);
+        t[v] = (float)((zs[q] - ze[q]) / increment_unit(ze[q], in.A[q], sc));
     }
     t[6] = 1.0f;
     t[7] = 0.0f;

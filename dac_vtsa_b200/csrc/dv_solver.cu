@@ -524,6 +524,15 @@ static int apply_AP(Work& W, const Op& op, const double* w, double* out, cudaStr
     return DV_OK;
 }
 
+// out = b - A u for a correction u in scaled variables (the GMRES operator without the preconditioner)
+static int op_residual(Work& W, const Op& op, const double* b, const double* u, double* out, cudaStream_t st) {
+    DV_TRY(rms_ratio_dev(W, op.n, u, nullptr, 0, W.scal + 0, st));     // scal[0] = rms(u): the FD step
+    if (op.m->op32) DV_TRY(launch_spmv32(op.m, u, op.s, op.dh, nullptr, out, st));
+    else DV_TRY(launch_matvec(op.m, op.t, op.z, u, op.s, op.f, op.dh, W.scal, out, st));
+    DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<vgrid(op.n), VB, 0, st>>>(op.n, 1.0, b, -1.0, out, out));
+    return DV_OK;
+}
+
 // scipy.sparse.linalg.gmres(AP, b, rtol, atol, restart=kdim, maxiter=1) with M = identity
 // (scipy/sparse/linalg/_isolve/iterative.py); x written to W.x.  Returns info (0 = converged).
 static int gmres(Work& W, const Op& op, const double* b, double rtol, double atol, int kdim, int* info,
@@ -1574,29 +1583,32 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             r.gmres_iters += inner2;
             if (C.gm_counter) *C.gm_counter += inner2;
         }
-        // polish: further restart cycles on the true linear residual r = b - A P^-1 x until the
-        // polish tolerance (1e-3 of ||b||) or the cycle limit; prec() is linear, so the cycles'
-        // corrections u = P^-1 x add up.  The speculation queued behind the first cycle is void.
+        // polish: further restart cycles until the polish tolerance (1e-3 of ||b||) or the cycle
+        // limit.  Each cycle solves for the linear residual of the summed correction u (prec() is
+        // linear, so the cycles' corrections P^-1 x add up), recomputed from u: the speculation
+        // queued behind the first cycle reused the GMRES residual vector, and is void anyway.
         const int pcyc = std::min(std::max(C.o.polish_cycles, 1), 8);
         if (polish && info != 0 && pcyc > 1) {
             spec_ok = false;
             m->nfev -= 1;
+            DV_LAUNCH(dv::K_VECTOR, st, k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.tmp));   // b0 = -R/s
             double bn0 = 0.0;
-            DV_TRY(rms_ratio(W, n, W.b, nullptr, &bn0, st));
-            DV_TRY(copy(W.u, W.dz));                          // dz: the summed correction
+            DV_TRY(rms_ratio(W, n, W.tmp, nullptr, &bn0, st));
+            DV_TRY(copy(W.u, W.dz));                          // dz: the summed correction u
             for (int cyc = 1; cyc < pcyc && info != 0; ++cyc) {
+                DV_TRY(op_residual(W, op, W.tmp, W.dz, W.b, st));   // b = b0 - A u
                 double rk = 0.0;
-                DV_TRY(rms_ratio(W, n, W.r, nullptr, &rk, st));
-                if (!(rk > 0.0) || !std::isfinite(rk)) break;
-                DV_TRY(copy(W.r, W.b));
+                DV_TRY(rms_ratio(W, n, W.b, nullptr, &rk, st));
+                if (!(rk > 1e-3 * bn0) || !std::isfinite(rk)) break;
                 int64_t inner2 = 0;
                 DV_TRY(gmres_any(W, op, W.b, std::min(1.0, 1e-3 * bn0 / rk), floor_, C.o.krylov_dim, &info,
                                  &inner2, st));
                 r.gmres_polish += inner2;
+                m->nfev += 1;                                 // the residual's operator product
                 DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.dz, 1.0, W.u, W.dz));
             }
             DV_TRY(copy(W.dz, W.u));
-            DV_LAUNCH(dv::K_VECTOR, st, k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.b));     // b = -R/s again
+            DV_TRY(copy(W.tmp, W.b));
         }
         if (!spec_ok) {
             DV_TRY(speculate());

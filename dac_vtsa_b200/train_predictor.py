@@ -7,7 +7,7 @@
 2. For each point one full adsorption -> blowdown -> heating -> cooling cycle runs with the plain
    extrapolation predictor while the network records every ``stride``-th cell of every converged
    stage (features of the two latest levels, target = the stage solution's offset from the
-   extrapolation in the solver's error-scale units).
+   extrapolation in units of the cell's extrapolated increment plus 1 % of its error scale).
 3. Adam on those samples with the library's BF16 tensor-core forward / backward kernels.
 4. The gain: a held-out operating point's cycle with and without the network (Newton iterations,
    GMRES iterations, wall time).

@@ -309,7 +309,9 @@ int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps,
  * layers of DV_MLP_NH -> DV_MLP_NOUT outputs, BF16 weights and activations, FP32 accumulation on the
  * tcgen05 tensor cores) predicts a correction to that extrapolation for the six cell unknowns, from the
  * cell's and its six face neighbours' states at the two latest levels, f at the latest level, the step-
- * size ratio, the stage and the cycle step.  Parameters (fp32, DV_MLP_NPARAM): W1 [NH x NIN], b1 [NH],
+ * size ratio, the stage and the cycle step.  The correction of unknown v is out_v * norm[13 + v] *
+ * (|z_ext - A| + 0.01 s): in units of the cell's extrapolated increment plus 1 % of its error scale
+ * s = atol + rtol |A|.  Parameters (fp32, DV_MLP_NPARAM): W1 [NH x NIN], b1 [NH],
  * W2 [NH x NH], b2, W3 [NH x NH], b3, W4 [NOUT x NH], b4 [NOUT]; normalisation constants (double,
  * DV_MLP_NNORM): [0,6) level scales, [6,12) neighbour-difference scales, [12] scale of the solver-unit
  * features, [13,19) output scale per unknown, [19] target clip. */
