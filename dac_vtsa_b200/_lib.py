@@ -78,13 +78,13 @@ class DvStepParams(C.Structure):
 class DvNewtonOpts(C.Structure):
     _fields_ = [("max_iter", I32), ("krylov_dim", I32), ("allow_refresh", I32), ("precond_mode", I32),
                 ("kappa", D), ("eta", D), ("rtol", D), ("cons_tol", D), ("max_polish", I32),
-                ("polish_cycles", I32)]
+                ("polish_cycles", I32), ("balance_projection", I32), ("pad_", I32)]
 
 
 class DvNewtonResult(C.Structure):
     _fields_ = [("ok", I32), ("iters", I32), ("refreshed", I32), ("pad_", I32), ("rate", D),
                 ("gmres_iters", I64), ("gmres_polish", I64), ("balance_unclosed", I64),
-                ("jac_refresh_in_newton", I64)]
+                ("jac_refresh_in_newton", I64), ("balance_projected", I64)]
 
 
 class DvSolverOpts(C.Structure):
@@ -92,7 +92,7 @@ class DvSolverOpts(C.Structure):
                 ("precond_mode", I32), ("krylov_fp32", I32), ("max_steps", I64),
                 ("rtol", D), ("newton_kappa", D), ("refactor_ratio", D), ("conservation_tol", D),
                 ("h_max", D), ("h_init", D), ("newton_mode", I32), ("max_polish", I32), ("polish_cycles", I32),
-                ("pad_", I32)]
+                ("balance_projection", I32)]
 
 
 class DvTuning(C.Structure):
@@ -105,7 +105,8 @@ class DvStepReport(C.Structure):
                 ("n_lu", I64), ("nfev", I64), ("gmres_iters", I64), ("gmres_polish", I64),
                 ("balance_unclosed", I64), ("jac_refresh_in_newton", I64), ("krylov_ok", I64),
                 ("krylov_fail", I64), ("acc", D * DV_NACC), ("newton_iters", I64), ("pred_net", I64),
-                ("pred_extrap", I64), ("pred_retry", I64), ("modified_fail", I64)]
+                ("pred_extrap", I64), ("pred_retry", I64), ("modified_fail", I64),
+                ("balance_projected", I64)]
 
 
 P = C.c_void_p
@@ -153,6 +154,7 @@ SIGNATURES = [
     ("dv_mlp_get_params", C.c_int, [P, P, P]),
     ("dv_mlp_sample_count", I64, [P]),
     ("dv_mlp_clear_samples", C.c_int, [P]),
+    ("dv_mlp_get_samples", C.c_int, [P, I64, I64, P, P]),
     ("dv_mlp_forward_host", C.c_int, [P, P, I64, P]),
     ("dv_mlp_gradient_host", C.c_int, [P, P, P, I64, P, C.POINTER(D)]),
     ("dv_mlp_gemm_host", C.c_int, [I32, I32, I32, P, P, P]),

@@ -97,7 +97,7 @@ _DEFAULTS: Dict[str, Any] = {
                "outlet_record_every": 1},
     # GPU-only knobs live in their own namespace so reference configs stay valid.
     "gpu": {"krylov_precision": "fp64", "predictor": "extrapolation", "predictor_weights": "", "max_polish": 2,
-            "polish_cycles": 1},
+            "polish_cycles": 1, "balance_projection": False},
 }
 
 # Choices checked by validate(); everything else is type-checked against the default.

@@ -197,42 +197,7 @@ __global__ void k_pc_to_f32(const double* __restrict__ A, float* __restrict__ B,
         B[q] = (float)A[q];
 }
 
-// Conservative lumping of the couplings a partitioning drops.  Each conserved quantity m (moles of a
-// species, gas + adsorbed; bed + wall energy) is a weighted sum W_m y whose internal fluxes cancel:
-// W_m (I - dh J) differs from W_m only by boundary terms.  Dropping the couplings across a partition
-// boundary breaks that, so a preconditioned Newton step leaves a balance error the true operator
-// would not.  With lumping, every dropped entry J[(v, a), (w, b)] is added to the same-variable entry
-// J[(v, b), (w, b)] of the column cell's own block, scaled by the ratio of the two rows' weights
-// (ring volumes V_a / V_b for cell unknowns, 1 between wall nodes), which keeps every weighted column
-// sum: W M = W (I - dh J) exactly, and W is a left eigenvector of A M^-1 with eigenvalue 1.
-struct PcLump {
-    double vr[DV_MAX_NR];   // cell volume of each ring
-    int on;
-};
-
-// Sum over the neighbours a of cell (i, j, k) in other partitions of J[(rv, a), (cv, this cell)]
-// times the weight ratio: the lumped part of this cell's self-block entry (rv, cv).
-static __device__ double pc_lumped(const PcGeom& g, const PcLump& L, const double* __restrict__ J, int i, int j,
-                                   int k, int part, int rv, int cv) {
-    double s = 0.0;
-    for (int sl = 5; sl <= 8; ++sl) {
-        int ai = i, aj = j;
-        bool ex;
-        if (sl == 5) { ai = i - 1; ex = ai >= 0; }
-        else if (sl == 6) { ai = i + 1; ex = ai < g.Nr; }
-        else if (sl == 7) { ex = g.Nth > 1; aj = (j == 0) ? g.Nth - 1 : j - 1; }
-        else { ex = g.Nth > 1; aj = (j == g.Nth - 1) ? 0 : j + 1; }
-        if (!ex || pc_part_of(g, ai, aj) == part) continue;
-        if (rv == DV_NV && !(g.wall && ai == g.Nr - 1)) continue;          // a has no wall row
-        const int back = (sl == 5) ? 6 : (sl == 6) ? 5 : (sl == 7) ? 8 : 7;  // a's slot pointing here
-        const int64_t a = ((int64_t)ai * g.Nth + aj) * g.Nz + k;
-        const double w = (rv == DV_NV) ? 1.0 : L.vr[ai] / L.vr[i];
-        s += J[((int64_t)(back * DV_NB + rv) * DV_NB + cv) * g.nc + a] * w;
-    }
-    return s;
-}
-
-__global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, double* __restrict__ A, PcLump L) {
+__global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, double* __restrict__ A) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= g.nc) return;
     const int slot = blockIdx.y;
@@ -273,7 +238,6 @@ __global__ void k_pc_scatter(PcGeom g, const double* __restrict__ J, double dh, 
             const double jv = J[((int64_t)(slot * DV_NB + rv) * DV_NB + cv) * g.nc + c];
             double val = -dh * jv;
             if (slot == 0 && rv == cv) val += 1.0;
-            if (slot == 0 && L.on) val -= dh * pc_lumped(g, L, J, i, j, k, part, rv, cv);
             if (lr >= pnb || lc >= pnb) {
                 if (g.err) atomicOr(g.err, PC_ERR_RANGE);
                 continue;
@@ -1623,12 +1587,6 @@ static int pc_twist_zs(const PcGeom& g, size_t tsize, bool factor_smem) {
     return (g.Nz - 2) / 2;
 }
 
-// DVTSA_PC_LUMP=1: partitioned factors with the dropped couplings lumped conservatively (PcLump)
-static bool pc_lump_enabled() {
-    const char* e = getenv("DVTSA_PC_LUMP");
-    return e && e[0] == '1';
-}
-
 int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream_t s) {
     PcGeom g = geom_of(m, mode);
     if (g.nb > m->pc_cap_nb || g.nparts > m->pc_cap_parts) {
@@ -1642,10 +1600,7 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
     const int64_t total = (int64_t)g.nparts * g.Nz * 5 * g.bs;
     DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_zero<<<std::min<int64_t>((total + 255) / 256, 4096), 256, 0, s>>>(m->d_pc, total));
     dim3 grid((unsigned)((m->nc + 127) / 128), DV_NSLOT);
-    PcLump L;
-    for (int r = 0; r < DV_MAX_NR; ++r) L.vr[r] = r < m->p.Nr ? m->p.V[r] : 1.0;
-    L.on = pc_lump_enabled() && mode != 1;
-    DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_scatter<<<grid, 128, 0, s>>>(g, J, dh, m->d_pc, L));
+    DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_scatter<<<grid, 128, 0, s>>>(g, J, dh, m->d_pc));
     const int optin = smem_optin();
     const size_t budget = (size_t)optin - 2048;             // static shared memory of the kernel
     const int lds = pc_lds(g.nb, budget);

@@ -680,6 +680,30 @@ int dv_mlp_get_params(const dv_mlp* n, float* params, double* norm) {
 
 int64_t dv_mlp_sample_count(const dv_mlp* n) { return n ? n->count : -1; }
 
+int dv_mlp_get_samples(const dv_mlp* n, int64_t first, int64_t count, float* X, float* T) {
+    if (!n || first < 0 || count < 0 || first + count > n->count || (!X && !T)) {
+        set_error("dv_mlp_get_samples: bad argument");
+        return DV_ERR_ARG;
+    }
+    if (count == 0) return DV_OK;
+    if (X) {        // the store is in panels of 8 features: copy each panel's rows, then transpose
+        std::vector<uint16_t> pan((size_t)count * 8);
+        for (int p = 0; p < NIN / 8; ++p) {
+            DV_CUDA(cudaMemcpy(pan.data(), n->Xs + pidx(first, p * 8, n->cap), sizeof(uint16_t) * pan.size(),
+                               cudaMemcpyDeviceToHost));
+            for (int64_t r = 0; r < count; ++r)
+                for (int q = 0; q < 8; ++q) {
+                    const uint32_t bits = (uint32_t)pan[(size_t)r * 8 + q] << 16;
+                    float v;
+                    memcpy(&v, &bits, sizeof v);
+                    X[(size_t)r * NIN + p * 8 + q] = v;
+                }
+        }
+    }
+    if (T) DV_CUDA(cudaMemcpy(T, n->Ts + first * 8, sizeof(float) * (size_t)count * 8, cudaMemcpyDeviceToHost));
+    return DV_OK;
+}
+
 int dv_mlp_clear_samples(dv_mlp* n) {
     if (!n) { set_error("null argument"); return DV_ERR_ARG; }
     n->count = 0;

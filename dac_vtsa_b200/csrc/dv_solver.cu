@@ -353,6 +353,68 @@ __global__ void __launch_bounds__(VB) k_cons(dv_step_params p, const double* __r
     if (last && threadIdx.x == 0) *ticket = 0u;
 }
 
+// Balance projection (no reference counterpart).  The conserved quantity an unknown belongs to
+// (rows of W): species k for c_k and, for k < DV_NA, the loading q_k; 3 for e and the wall.
+__device__ __forceinline__ int cons_quantity(int64_t i, int64_t nc) {
+    const int64_t blk = i / nc;
+    return blk < DV_NG ? (int)blk : (blk < DV_NG + DV_NA ? (int)(blk - DV_NG) : DV_NG);
+}
+
+// Basis direction b_q of the projection, in scaled variables (u = b / s): a relative change of the
+// species' concentrations and loadings (b = z, keeps them positive), an additive change of one error
+// scale for the energy and wall unknowns (b = s); 0 outside quantity q.
+__global__ void k_cons_basis(int64_t nc, int64_t n, int q, const double* __restrict__ z, const double* __restrict__ s,
+                             double* __restrict__ u) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int w = cons_quantity(i, nc);
+    u[i] = (w != q) ? 0.0 : (q < DV_NG ? z[i] / s[i] : 1.0);
+}
+
+// z += sum_q lam_q b_q
+__global__ void k_cons_shift(int64_t nc, int64_t n, double l0, double l1, double l2, double l3,
+                             const double* __restrict__ s, double* __restrict__ z) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int w = cons_quantity(i, nc);
+    const double l = w == 0 ? l0 : (w == 1 ? l1 : (w == 2 ? l2 : l3));
+    z[i] = (w < DV_NG) ? z[i] * (1.0 + l) : z[i] + l * s[i];
+}
+
+// Solve G lam = rhs (4 x 4, row-major) over the quantities with active[q]; lam = 0 elsewhere.
+// Gaussian elimination with partial pivoting; false if the active system is singular.
+static bool solve_small(const double* G, const double* rhs, const bool* active, double* lam) {
+    int idx[4], k = 0;
+    for (int q = 0; q < 4; ++q) {
+        lam[q] = 0.0;
+        if (active[q]) idx[k++] = q;
+    }
+    double A[4][5];
+    for (int a = 0; a < k; ++a) {
+        for (int b = 0; b < k; ++b) A[a][b] = G[idx[a] * 4 + idx[b]];
+        A[a][k] = rhs[idx[a]];
+    }
+    for (int c = 0; c < k; ++c) {
+        int piv = c;
+        for (int a = c + 1; a < k; ++a)
+            if (std::fabs(A[a][c]) > std::fabs(A[piv][c])) piv = a;
+        if (!(std::fabs(A[piv][c]) > 0.0)) return false;
+        if (piv != c)
+            for (int b = 0; b <= k; ++b) std::swap(A[c][b], A[piv][b]);
+        for (int a = c + 1; a < k; ++a) {
+            const double f = A[a][c] / A[c][c];
+            for (int b = c; b <= k; ++b) A[a][b] -= f * A[c][b];
+        }
+    }
+    for (int c = k - 1; c >= 0; --c) {
+        double v = A[c][k];
+        for (int b = c + 1; b < k; ++b) v -= A[c][b] * lam[idx[b]];
+        lam[idx[c]] = v / A[c][c];
+        if (!std::isfinite(lam[idx[c]])) return false;
+    }
+    return true;
+}
+
 static unsigned cons_grid(int64_t nc) {
     const int64_t b = (nc + VB - 1) / VB;
     return (unsigned)(b < 1 ? 1 : (b > 64 ? 64 : b));
@@ -1492,6 +1554,45 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
         return DV_OK;
     };
 
+    // Balance projection of a converged stage solution W.z whose balances are not closed: the
+    // correction z += sum_q lam_q b_q, one direction per conserved quantity (k_cons_basis), with
+    // W A B lam = -W R (A = I - dh J applied to each b_q by the finite-difference operator), closes
+    // the linearised balances exactly; the state moves by about |W R| / |W z| relative, far below
+    // the tolerance.  Recomputes f and R at the new state; *okp = balances closed after it.
+    auto project = [&](bool* okp) -> int {
+        *okp = false;
+        if (4 * (W.kdim + 2) < 40) return DV_OK;    // hbuf too small for the 40 sums
+        double* H = W.hbuf;                  // 5 x 8 balance sums (free outside GMRES)
+        DV_TRY(rms_ratio_dev(W, n, W.z, W.s, 1, W.scal + 1, st));       // the FD step's max(1, rms(z/s))
+        for (int q = 0; q < 4; ++q) {
+            DV_LAUNCH(dv::K_VECTOR, st, k_cons_basis<<<g, VB, 0, st>>>(m->nc, n, q, W.z, W.s, W.dz));
+            DV_TRY(rms_ratio_dev(W, n, W.dz, nullptr, 0, W.scal + 0, st));
+            DV_TRY(launch_matvec(m, t, W.z, W.dz, W.s, W.f, dh, W.scal, W.r, st));     // (A b_q) / s
+            DV_LAUNCH(dv::K_VECTOR, st, k_mul<<<g, VB, 0, st>>>(n, W.r, W.s, W.w));
+            DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<cons_grid(m->nc), VB, 0, st>>>(m->p, W.w, W.s, W.apart,
+                                                                                  W.tickets + 5, H + 8 * q));
+        }
+        DV_LAUNCH(dv::K_VECTOR, st, k_cons<<<cons_grid(m->nc), VB, 0, st>>>(m->p, W.R, W.s, W.apart, W.tickets + 5,
+                                                                              H + 32));
+        m->nfev += 4;
+        double h[40];
+        DV_TRY(fetch(W, H, 40, h, st));
+        double G[16], rhs[4], lam[4];
+        bool active[4];
+        for (int q = 0; q < 4; ++q) {
+            rhs[q] = -h[32 + q];
+            active[q] = std::fabs(h[8 * q + q]) > 1e-12 * h[32 + 4 + q];     // quantity present
+            for (int b = 0; b < 4; ++b) G[q * 4 + b] = h[8 * b + q];         // row q: W_q (A b_b)
+        }
+        if (!solve_small(G, rhs, active, lam)) return DV_OK;
+        for (int q = 0; q < DV_NG; ++q)
+            if (!(std::fabs(lam[q]) <= 1e-2)) return DV_OK;                  // not a small correction
+        if (!(std::fabs(lam[DV_NG]) <= 1.0)) return DV_OK;
+        DV_LAUNCH(dv::K_VECTOR, st, k_cons_shift<<<g, VB, 0, st>>>(m->nc, n, lam[0], lam[1], lam[2], lam[3], W.s, W.z));
+        DV_TRY(stage(W.z, W.f, W.R));
+        return cons_ok(W.R, W.z, okp);
+    };
+
     auto cons_eval = [&](const double* v) -> bool {
         if (C.o.cons_tol <= 0.0) return true;
         bool ok = true;
@@ -1539,6 +1640,7 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
     bool have_best = false;
     double best_rn = 0.0;
     bool new_lu = false;
+    bool projected = false;      // the balance projection was tried in this solve
     int it = -1;
     const double sqrt_n = std::sqrt((double)n);
     while (it + 1 < C.o.max_iter + polish) {
@@ -1584,9 +1686,10 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             if (C.gm_counter) *C.gm_counter += inner2;
         }
         // polish: further restart cycles until the polish tolerance (1e-3 of ||b||) or the cycle
-        // limit.  Each cycle solves for the linear residual of the summed correction u (prec() is
-        // linear, so the cycles' corrections P^-1 x add up), recomputed from u: the speculation
-        // queued behind the first cycle reused the GMRES residual vector, and is void anyway.
+        // limit.  Each cycle solves A P^-1 x_c = b0 - A P^-1 (x_1 + .. x_c-1), the linear residual
+        // of the summed solution recomputed from it (the speculation queued behind the first cycle
+        // reused the GMRES residual vector, and is void anyway); the Newton step is then formed
+        // from x = sum x_c, as from a single cycle's solution.
         const int pcyc = std::min(std::max(C.o.polish_cycles, 1), 8);
         if (polish && info != 0 && pcyc > 1) {
             spec_ok = false;
@@ -1594,9 +1697,10 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             DV_LAUNCH(dv::K_VECTOR, st, k_div<<<g, VB, 0, st>>>(n, -1.0, W.R, W.s, W.tmp));   // b0 = -R/s
             double bn0 = 0.0;
             DV_TRY(rms_ratio(W, n, W.tmp, nullptr, &bn0, st));
-            DV_TRY(copy(W.u, W.dz));                          // dz: the summed correction u
+            DV_TRY(copy(W.x, W.dz));                          // dz: the summed solution x
             for (int cyc = 1; cyc < pcyc && info != 0; ++cyc) {
-                DV_TRY(op_residual(W, op, W.tmp, W.dz, W.b, st));   // b = b0 - A u
+                DV_TRY(precond_apply(m, W.dz, W.s, W.u, st));       // u = P^-1 x
+                DV_TRY(op_residual(W, op, W.tmp, W.u, W.b, st));    // b = b0 - A u
                 double rk = 0.0;
                 DV_TRY(rms_ratio(W, n, W.b, nullptr, &rk, st));
                 if (!(rk > 1e-3 * bn0) || !std::isfinite(rk)) break;
@@ -1605,9 +1709,9 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
                                  &inner2, st));
                 r.gmres_polish += inner2;
                 m->nfev += 1;                                 // the residual's operator product
-                DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.dz, 1.0, W.u, W.dz));
+                DV_LAUNCH(dv::K_VECTOR, st, k_axpby<<<g, VB, 0, st>>>(n, 1.0, W.dz, 1.0, W.x, W.dz));
             }
-            DV_TRY(copy(W.dz, W.u));
+            DV_TRY(copy(W.dz, W.x));
             DV_TRY(copy(W.tmp, W.b));
         }
         if (!spec_ok) {
@@ -1677,6 +1781,21 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
                 DV_TRY(copy(W.z, zout));
                 r.ok = 1; r.iters = it + 1; r.rate = rate;
                 return DV_OK;
+            }
+            if (C.o.balance_projection && !projected) {
+                projected = true;
+                bool okp = false;
+                DV_TRY(project(&okp));
+                if (okp) {
+                    r.balance_projected += 1;
+                    DV_TRY(copy(W.z, zout));
+                    r.ok = 1; r.iters = it + 1; r.rate = rate;
+                    return DV_OK;
+                }
+                // not closed: the reference's polish continues from the (projected) state
+                scale(W.z, W.s);
+                DV_TRY(rms_ratio(W, n, W.R, W.s, &rn, st));
+                DV_TRY(pnorm(W.R, W.s, &pn));
             }
             if (polish < (C.o.max_polish > 0 ? C.o.max_polish : 2)) {
                 polish += 1;
@@ -1973,6 +2092,7 @@ static int solve_stage(dv_integrator* g, const dv_newton_opts& no, double ts, co
         R.gmres_iters += r.gmres_iters;
         R.gmres_polish += r.gmres_polish;
         R.balance_unclosed += r.balance_unclosed;
+        R.balance_projected += r.balance_projected;
         R.jac_refresh_in_newton += r.jac_refresh_in_newton;
         if (r.ok) R.krylov_ok += 1; else R.krylov_fail += 1;
         if (r.refreshed) {                // Jacobian and factors were replaced inside the stage
@@ -2143,6 +2263,8 @@ int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps,
     no.cons_tol = 0.0;
     no.max_polish = 2;
     no.polish_cycles = 1;
+    no.balance_projection = 0;
+    no.pad_ = 0;
     bestv = INFINITY;
     int rc = DV_OK;
     const int64_t nfev0 = m->nfev;
@@ -2569,6 +2691,8 @@ int dv_integrator_advance(dv_integrator* g, double t_target, dv_step_report* rep
     no.cons_tol = g->o.conservation_tol;
     no.max_polish = g->o.max_polish;
     no.polish_cycles = g->o.polish_cycles;
+    no.balance_projection = g->o.balance_projection;
+    no.pad_ = 0;
     while (g->t < g->t_end * (1.0 - 1e-12)) {
         const int64_t gm0 = g->gm;
         if (R.n_steps + R.n_reject + R.n_newton_fail > g->o.max_steps) {

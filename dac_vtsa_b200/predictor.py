@@ -72,6 +72,15 @@ class NewtonPredictor:
     def samples(self) -> int:
         return int(self.lib.dv_mlp_sample_count(self.handle))
 
+    def get_samples(self, first: int = 0, count=None):
+        """Recorded (features [count][112], targets [count][8]) as numpy arrays."""
+        count = self.samples - first if count is None else count
+        X = np.empty((count, NIN), dtype=np.float32)
+        T = np.empty((count, 8), dtype=np.float32)
+        check(self.lib.dv_mlp_get_samples(self.handle, int(first), int(count), X.ctypes.data, T.ctypes.data),
+              "dv_mlp_get_samples")
+        return X, T
+
     def clear_samples(self):
         check(self.lib.dv_mlp_clear_samples(self.handle), "dv_mlp_clear_samples")
 

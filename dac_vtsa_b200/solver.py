@@ -96,6 +96,9 @@ class TRBDF2:
         o.max_polish = int(gpu_option(cfg, "max_polish", 2))
         # gpu.polish_cycles: GMRES restart cycles of one polish iteration (the reference runs one)
         o.polish_cycles = int(gpu_option(cfg, "polish_cycles", 1))
+        # gpu.balance_projection: close the balances of a converged stage by the balance projection
+        # before the reference's polish iterations (no reference counterpart)
+        o.balance_projection = int(bool(gpu_option(cfg, "balance_projection", False)))
         self.mode = "hybrid" if (s.newton_mode == "modified" and self.precond == "theta_block") else s.newton_mode
         # gpu.krylov_precision: fp64 (default, the parity path); fp32 (GMRES on the FP32 assembled
         # Jacobian with FP32 preconditioner factors, FP64 residual / Newton update as refinement);
@@ -226,6 +229,6 @@ class TRBDF2:
                                "jac_refresh_in_newton": rep.jac_refresh_in_newton,
                                "newton_iters": rep.newton_iters, "pred_net": rep.pred_net,
                                "pred_extrap": rep.pred_extrap, "pred_retry": rep.pred_retry,
-                               "modified_fail": rep.modified_fail})
+                               "modified_fail": rep.modified_fail, "balance_projected": rep.balance_projected})
             res.wall_time = time.time() - wall0
             return res

@@ -226,12 +226,17 @@ typedef struct dv_newton_opts {
     int32_t max_polish;        /* conservation-polish iterations after convergence (reference: 2; 0 = 2) */
     int32_t polish_cycles;     /* GMRES restart cycles of one polish iteration's linear solve, stopping at its
                                   tolerance (reference: 1, scipy gmres maxiter=1; 0 = 1; at most 8) */
+    int32_t balance_projection;   /* 1: a converged stage whose balances are not closed is first corrected
+                                     by the balance projection (no reference counterpart; 0 = the
+                                     reference's polish only) */
+    int32_t pad_;
 } dv_newton_opts;
 
 typedef struct dv_newton_result {
     int32_t ok, iters, refreshed, pad_;
     double rate;
     int64_t gmres_iters, gmres_polish, balance_unclosed, jac_refresh_in_newton;
+    int64_t balance_projected;    /* stage solutions closed by the balance projection */
 } dv_newton_result;
 
 /* Inexact Newton for R(z) = z - dh f(t, z) - rhs_known = 0 from z0 (newton_krylov,
@@ -253,7 +258,7 @@ typedef struct dv_solver_opts {
                                   partitioned factors runs as hybrid, as the reference does (core/solver.py:328) */
     int32_t max_polish;        /* conservation-polish iterations of a stage (reference: 2; 0 = 2) */
     int32_t polish_cycles;     /* GMRES restart cycles of a polish iteration (reference: 1; 0 = 1; at most 8) */
-    int32_t pad_;
+    int32_t balance_projection;   /* see dv_newton_opts */
 } dv_solver_opts;
 
 typedef struct dv_step_report {
@@ -265,6 +270,7 @@ typedef struct dv_step_report {
     int64_t pred_net, pred_extrap;   /* stage starts taken from the network / from the extrapolation */
     int64_t pred_retry;        /* stage solves repeated from the extrapolation after the network's start failed */
     int64_t modified_fail;     /* hybrid mode: modified-Newton attempts that fell back to Newton-Krylov */
+    int64_t balance_projected;    /* stage solutions closed by the balance projection */
 } dv_step_report;
 
 /* TRBDF2(model, cfg, h_max, h_init) (core/solver.py:298-329) */
@@ -333,6 +339,10 @@ int dv_mlp_set_params(dv_mlp* net, const float* params, int64_t nparams, const d
 int dv_mlp_get_params(const dv_mlp* net, float* params, double* norm);
 int64_t dv_mlp_sample_count(const dv_mlp* net);
 int dv_mlp_clear_samples(dv_mlp* net);
+/* Recorded samples [first, first + count) to host: features X [count][DV_MLP_NIN] (fp32 values of the
+ * stored BF16) and targets T [count][8] (the six corrections in increment units, then 1, 0); either
+ * pointer may be NULL.  Synchronous. */
+int dv_mlp_get_samples(const dv_mlp* net, int64_t first, int64_t count, float* X, float* T);
 /* Forward pass of host feature rows X [rows][DV_MLP_NIN] (rounded to BF16) -> out [rows][DV_MLP_NOUT]. */
 int dv_mlp_forward_host(dv_mlp* net, const float* X, int64_t rows, float* out);
 /* One BF16 tensor-core product D[M][N] = A[M][K] B[N][K]^T (host fp32 in, rounded to BF16; FP32 out)

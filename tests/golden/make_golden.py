@@ -24,6 +24,10 @@ Writes (all small, committed):
   stop_young2021.npz     (--stop) the young2021 1-D case's adsorption step, stopped by its
                          end_saturation criterion (core/residual.py:445-482, core/solver.py:
                          476-494): stop time, stop value, end state
+  css_3x4x6.npz          (--css) the reference's cyclic-steady-state measures
+                         (validation/cyclic_steady_state.py:22-44) between two seeded 3x4x6 states,
+                         and its step flows / cycle CO2 balance (postprocessing/reporting.py:30-41)
+                         of the 8x8x32 cycle golden's steps
   cycle_8x8x32[_rtolX].npz  (--cycle [--rtol X]) one full adsorption -> blowdown -> heating ->
                          cooling cycle of the 8x8x32 bed through the reference's own step runner
                          (steps/_runner.py:87-188, states handed over in memory as vtsa_cycle.py:
@@ -457,9 +461,9 @@ def make_stop_golden(ref_root):
 if __name__ == "__main__":
     if len(sys.argv) < 2 or sys.argv[1].startswith("--"):
         raise SystemExit("usage: make_golden.py <reference checkout> [--outlet | --bench-state | "
-                         "--bench-state-heating | --cycle [--rtol X] | --stop | --csv | --modes]")
+                         "--bench-state-heating | --cycle [--rtol X] | --stop | --csv | --modes | --css]")
     root = sys.argv[1]
-    if "--modes" in sys.argv:
+    if "--modes" in sys.argv or "--css" in sys.argv:
         pass                        # handled below
     elif "--stop" in sys.argv:
         make_stop_golden(root)
@@ -521,3 +525,60 @@ def make_modes_golden(ref_root):
 
 if __name__ == "__main__" and "--modes" in sys.argv:
     make_modes_golden(sys.argv[1])
+
+
+def make_css_golden(ref_root):
+    """The reference's CSS test quantities: state_change between two seeded 3x4x6 states, is_css at
+    cycles 1..4, and the CO2 flows and cycle balance of the 8x8x32 cycle golden's steps."""
+    sys.path.insert(0, ref_root)
+    from types import SimpleNamespace
+    import config.parameters as rp
+    from core.grid import Grid
+    from core.state import initial_state
+    from postprocessing.reporting import step_flows
+    from properties import get_backend
+    from validation.cyclic_steady_state import cycle_co2_balance, is_css, state_change
+    over = {"grid.Nr": 3, "grid.Ntheta": 4, "grid.Nz": 6}
+    cfg = rp.load_config(override_dict=over)
+    g = Grid.from_config(cfg)
+    props = get_backend(cfg)
+    states = []
+    for seed in (21, 22):
+        st = initial_state(cfg, g, props)
+        rng = np.random.default_rng(seed)
+        st.T = st.T + 9.0 * rng.random(st.T.shape)
+        st.q = st.q + 0.5 * rng.random(st.q.shape)
+        st.c = st.c * (1.0 + 0.2 * rng.random(st.c.shape))
+        states.append(st)
+    ch = state_change(states[0], states[1], g, cfg)
+    cyc = np.load(os.path.join(HERE, "cycle_8x8x32.npz"))
+    ccfg = rp.load_config(override_dict=json.loads(str(cyc["over"])))
+    names = [f"{p}_{v}_{s}" for v in ("V1", "V2", "V3") for p in ("n_in", "n_out") for s in ("CO2", "H2O", "N2")]
+    acc_names = []
+    for v in ("V1", "V2", "V3"):
+        acc_names += [f"n_in_{v}_{s}" for s in ("CO2", "H2O", "N2")] + [f"n_out_{v}_{s}" for s in ("CO2", "H2O", "N2")]
+        acc_names += [f"H_in_{v}", f"H_out_{v}", f"W_pump_{v}", f"W_fan_{v}"]
+    acc_names += ["Q_jac_pos", "Q_jac_neg", "Q_amb", "Q_wb", "Q_hx_pos", "Q_hx_neg"]
+    tot = {"fed": 0.0, "product": 0.0, "vented": 0.0}
+    for k, step in enumerate(ccfg.cycle):
+        sr = SimpleNamespace(acc=dict(zip(acc_names, cyc[f"s{k}_acc"])), product_port=step.get("product_port", "V3"),
+                             valves=dict(step["valves"]))
+        fl = step_flows(sr, ["CO2", "H2O", "N2"])["CO2"]
+        for key in tot:
+            tot[key] += fl[key]
+    kp = {"CO2_fed_mol": tot["fed"], "CO2_product_mol": tot["product"], "CO2_vented_mol": tot["vented"]}
+    flags = [bool(is_css(ch, kp, cfg, n)) for n in range(1, 5)]
+    run0 = {"min_cycles": cfg.run.min_cycles, "css_tolerance": cfg.run.css_tolerance,
+            "css_mb_tolerance": cfg.run.css_mb_tolerance}
+    relaxed = rp.load_config(override_dict=dict(over, **{"run.css_tolerance": 1.0, "run.css_mb_tolerance": 0.5}))
+    flags_relaxed = [bool(is_css(ch, kp, relaxed, n)) for n in range(1, 5)]     # both criteria met
+    np.savez_compressed(os.path.join(HERE, "css_3x4x6.npz"), over=np.array(json.dumps(over)),
+                        **{f"s{i}_{f}": getattr(st, f) for i, st in enumerate(states) for f in ("c", "q", "T", "Tw")},
+                        change=np.array(json.dumps(ch)), flows=np.array(json.dumps(kp)),
+                        co2_balance=np.array(cycle_co2_balance(kp)), is_css=np.array(flags),
+                        is_css_relaxed=np.array(flags_relaxed), run=np.array(json.dumps(run0)))
+    print(ch, kp, flags, flags_relaxed)
+
+
+if __name__ == "__main__" and "--css" in sys.argv:
+    make_css_golden(sys.argv[1])
