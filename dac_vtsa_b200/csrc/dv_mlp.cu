@@ -308,16 +308,22 @@ __global__ void k_features(StageInputs in, const double* __restrict__ nrm, int64
 // the extrapolation is already close, cannot afford.
 __device__ __forceinline__ double increment_unit(double zext, double a, double sc) { return fabs(zext - a) + 1e-2 * sc; }
 
-// pred[v][c] = max(pred + out * oscale_v * unit, 0.1 max(ytr, 0)) (the floor for c and q only)
+// pred[v][c] = max(pred + out * oscale_v * unit, 0.1 max(ytr, 0)) (the floor for c and q only).
+// Corrections smaller than nrm[20] increment units are not applied: where the extrapolation is
+// already close (most cells of most stages, within a few percent of the increment) the network's
+// own error is of the same size, and leaving those cells alone keeps its gain at the fronts.
 __global__ void k_apply(StageInputs in, const double* __restrict__ nrm, const float* __restrict__ O,
                         const double* __restrict__ ytr, double* __restrict__ pred) {
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= in.nc) return;
+    const double gate = nrm[20];
 #pragma unroll
     for (int v = 0; v < 6; ++v) {
         const int64_t q = v * in.nc + c;
         const double sc = in.atol7[v] + in.rtol * fabs(in.A[q]);
-        double z = pred[q] + (double)O[c * NOUT + v] * nrm[13 + v] * increment_unit(pred[q], in.A[q], sc);
+        const double corr = (double)O[c * NOUT + v] * nrm[13 + v];
+        if (fabs(corr) < gate) continue;
+        double z = pred[q] + corr * increment_unit(pred[q], in.A[q], sc);
         if (v < 5) z = fmax(z, 0.1 * fmax(ytr[q], 0.0));
         pred[q] = z;
     }

@@ -320,7 +320,8 @@ int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps,
  * s = atol + rtol |A|.  Parameters (fp32, DV_MLP_NPARAM): W1 [NH x NIN], b1 [NH],
  * W2 [NH x NH], b2, W3 [NH x NH], b3, W4 [NOUT x NH], b4 [NOUT]; normalisation constants (double,
  * DV_MLP_NNORM): [0,6) level scales, [6,12) neighbour-difference scales, [12] scale of the solver-unit
- * features, [13,19) output scale per unknown, [19] target clip. */
+ * features, [13,19) output scale per unknown, [19] target clip, [20] gate: corrections smaller than
+ * this (in increment units) are not applied. */
 #define DV_MLP_NIN 112
 #define DV_MLP_NH 128
 #define DV_MLP_NOUT 16
