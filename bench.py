@@ -16,9 +16,9 @@ ours (default):
          with a host numpy state in and out), host copies inside the timed region
   roofline: the dominant kernel of one profiled window, timed back to back on its stream
   cpu_baseline: the CPU oracle (numpy restatement of the reference) on the same window, 1 core
-  cycles: full cycles of the 8x8x32 and 16x16x64 beds -- plain FP64, mixed-precision Krylov, and
-         learned predictor + mixed precision -- with their state difference to the FP64 cycle, the
-         8x8x32 cycle's step-end states against the reference's and its balance errors
+  cycles: full cycles of the 8x8x32 and 16x16x64 beds -- plain FP64, mixed precision (FP32
+         preconditioner factors), learned predictor, and both -- with their state difference to the
+         FP64 cycle, the 8x8x32 cycle's step-end states against the reference's and its balance errors
 --impl reference: the oracle on the host cores (one process per core, up to 16), each process one
   window per step.
 """
@@ -301,9 +301,15 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------- cycles (extra keys)
+# Cycle variants: the plain FP64 path (the reference's algorithm), mixed precision (FP32 preconditioner
+# factors and sweep, FP64 operator, residual and Newton update), the learned predictor, and both.
+VARIANTS = {"fp64": {}, "mixed": {"gpu.krylov_precision": "fp32_factors"}, "learned": {},
+            "learned_mixed": {"gpu.krylov_precision": "fp32_factors"}}
+
+
 def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
-    """Device-resident full cycles of `grid` in each variant ("fp64", "mixed", "learned_mixed"):
-    throughput, solver totals and the end state's difference to the FP64 cycle."""
+    """Device-resident full cycles of `grid` in each variant of VARIANTS: throughput, solver totals
+    and the end state's difference to the FP64 cycle."""
     import numpy as np
     import torch
     from dac_vtsa_b200.model import TVSAModel
@@ -311,12 +317,11 @@ def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
     from dac_vtsa_b200.runner import run_cycle_device
     out, y64 = {}, None
     for var in variants:
-        extra = {} if var == "fp64" else {"gpu.krylov_precision": "fp32"}
-        cfg, g, props, st = setup(grid, extra)
+        cfg, g, props, st = setup(grid, VARIANTS[var])
         m0 = TVSAModel(cfg, g, props, cfg.cycle[0], st)
         y0 = torch.from_numpy(m0.pack(st)).to(dev)
         net = None
-        if var == "learned_mixed":
+        if var.startswith("learned"):
             if not os.path.exists(weights_path):
                 out[var] = {"skipped": f"no trained weights at {os.path.relpath(weights_path, ROOT)}"}
                 continue
@@ -329,7 +334,7 @@ def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
         yh = y.cpu().numpy()
         keys = ("steps", "rejected", "newton_iters", "gmres_iters", "gmres_polish", "balance_unclosed",
                 "pred_net", "pred_extrap", "pred_retry")
-        rec = {"value": CYCLE_BED_S / wall, "wall_s": wall,
+        rec = {"value": CYCLE_BED_S / wall, "wall_s": wall, "config": VARIANTS[var],
                "solver": {k: int(sum(s.get(k, 0) for s in stats)) for k in keys}}
         if var == "fp64":
             y64 = yh
@@ -504,12 +509,12 @@ def gpu_arm(a, rank, world, local_rank):
     cycles = None
     if rank == 0 and not a.no_cycles:
         weights = os.path.join(ROOT, "dac_vtsa_b200", "predictor_weights.npz")
-        cycles = {"8x8x32": cycle_runs((8, 8, 32), ("fp64", "mixed", "learned_mixed"), weights, dev)}
+        cycles = {"8x8x32": cycle_runs((8, 8, 32), tuple(VARIANTS), weights, dev)}
         if os.path.exists(REF_CYCLE):
             cycles["8x8x32"]["reference_parity"] = reference_cycle_parity(dev)
         cycles["8x8x32"]["reference_cpu_cycle"] = CPU_FULL_CYCLE
         if not a.no_big:
-            cycles["16x16x64"] = cycle_runs((16, 16, 64), ("fp64", "mixed", "learned_mixed"), weights, dev)
+            cycles["16x16x64"] = cycle_runs((16, 16, 64), tuple(VARIANTS), weights, dev)
     if rank == 0:
         line = {"metric": "bed-s simulated per wall-s", "value": value, "unit": "bed-s/wall-s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,

@@ -1584,13 +1584,34 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             active[q] = std::fabs(h[8 * q + q]) > 1e-12 * h[32 + 4 + q];     // quantity present
             for (int b = 0; b < 4; ++b) G[q * 4 + b] = h[8 * b + q];         // row q: W_q (A b_b)
         }
-        if (!solve_small(G, rhs, active, lam)) return DV_OK;
-        for (int q = 0; q < DV_NG; ++q)
-            if (!(std::fabs(lam[q]) <= 1e-2)) return DV_OK;                  // not a small correction
-        if (!(std::fabs(lam[DV_NG]) <= 1.0)) return DV_OK;
+        // a quantity whose closure would need more than a small correction (a species whose
+        // inventory is at its absolute-tolerance floor, such as N2 under vacuum) leaves the system
+        bool solved = false;
+        for (int pass = 0; pass < 4 && !solved; ++pass) {
+            if (!solve_small(G, rhs, active, lam)) return DV_OK;
+            solved = true;
+            for (int q = 0; q < 4; ++q)
+                if (active[q] && !(std::fabs(lam[q]) <= (q < DV_NG ? 1e-2 : 1.0))) {
+                    active[q] = false;
+                    solved = false;
+                }
+        }
+        if (!solved) return DV_OK;
         DV_LAUNCH(dv::K_VECTOR, st, k_cons_shift<<<g, VB, 0, st>>>(m->nc, n, lam[0], lam[1], lam[2], lam[3], W.s, W.z));
         DV_TRY(stage(W.z, W.f, W.R));
         return cons_ok(W.R, W.z, okp);
+    };
+
+    // An unclosed stage returns its best converged state (by rms(R/s), as the reference does); with
+    // the balance projection on, the quantities that can be closed are closed on that state first.
+    auto return_best = [&]() -> int {
+        if (!C.o.balance_projection) return copy(W.best, zout);
+        DV_TRY(copy(W.best, W.z));
+        scale(W.z, W.s);
+        DV_TRY(stage(W.z, W.f, W.R));
+        bool okp = false;
+        DV_TRY(project(&okp));
+        return copy(W.z, zout);
     };
 
     auto cons_eval = [&](const double* v) -> bool {
@@ -1777,6 +1798,15 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             bool ok;
             if (cons_spec) ok = cons_eval(sv + 16);
             else DV_TRY(cons_ok(W.R, W.z, &ok));
+            if (getenv("DVTSA_TRACE_CONS")) {   // TEMPORARY diagnostic
+                double v[8];
+                if (cons_spec) memcpy(v, sv + 16, sizeof v);
+                else DV_TRY(fetch(W, W.scal, 8, v, st));
+                fprintf(stderr, "CONS it=%d pol=%d info=%d inner=%lld lam=%g step=%.3g pn=%.3g rn=%.3g dh=%.4g r=[%.3g %.3g %.3g %.3g] ok=%d\n",
+                        it, polish, info, (long long)inner, lam, step, pn, rn, dh,
+                        v[0] / (C.o.cons_tol * v[4]), v[1] / (C.o.cons_tol * v[5]), v[2] / (C.o.cons_tol * v[6]),
+                        v[3] / (C.o.cons_tol * v[7]), (int)ok);
+            }
             if (ok) {
                 DV_TRY(copy(W.z, zout));
                 r.ok = 1; r.iters = it + 1; r.rate = rate;
@@ -1803,13 +1833,13 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
                 continue;
             }
             r.balance_unclosed += 1;
-            DV_TRY(copy(W.best, zout));
+            DV_TRY(return_best());
             r.ok = 1; r.iters = it + 1; r.rate = rate;
             return DV_OK;
         }
         if (have_best) {
             r.balance_unclosed += 1;
-            DV_TRY(copy(W.best, zout));
+            DV_TRY(return_best());
             r.ok = 1; r.iters = it + 1; r.rate = rate;
             return DV_OK;
         }
