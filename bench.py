@@ -16,9 +16,10 @@ ours (default):
          with a host numpy state in and out), host copies inside the timed region
   roofline: the dominant kernel of one profiled window, timed back to back on its stream
   cpu_baseline: the CPU oracle (numpy restatement of the reference) on the same window, 1 core
-  cycles: full cycles of the 8x8x32 and 16x16x64 beds -- plain FP64, mixed precision (FP32
-         preconditioner factors), learned predictor, and both -- with their state difference to the
-         FP64 cycle, the 8x8x32 cycle's step-end states against the reference's and its balance errors
+  cycles: full cycles of the 8x8x32 and 16x16x64 beds -- plain FP64 (the reference's algorithm),
+         with the balance projection, and with it mixed precision (FP32 preconditioner factors) and
+         the learned predictor -- with their balance errors and state difference to the FP64 cycle,
+         and the 8x8x32 cycle's step-end states against the reference's
 --impl reference: the oracle on the host cores (one process per core, up to 16), each process one
   window per step.
 """
@@ -301,10 +302,13 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------- cycles (extra keys)
-# Cycle variants: the plain FP64 path (the reference's algorithm), mixed precision (FP32 preconditioner
-# factors and sweep, FP64 operator, residual and Newton update), the learned predictor, and both.
-VARIANTS = {"fp64": {}, "mixed": {"gpu.krylov_precision": "fp32_factors"}, "learned": {},
-            "learned_mixed": {"gpu.krylov_precision": "fp32_factors"}}
+# Cycle variants: the plain FP64 path (the reference's algorithm, the defaults), the same with the
+# balance projection, and with it mixed precision (FP32 preconditioner factors and sweep; FP64
+# operator, residual and Newton update) and the learned predictor.
+PROJ = {"gpu.balance_projection": True}
+VARIANTS = {"fp64": {}, "fp64_projection": PROJ,
+            "mixed_projection": dict(PROJ, **{"gpu.krylov_precision": "fp32_factors"}),
+            "learned_mixed_projection": dict(PROJ, **{"gpu.krylov_precision": "fp32_factors"})}
 
 
 def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
@@ -314,7 +318,7 @@ def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
     import torch
     from dac_vtsa_b200.model import TVSAModel
     from dac_vtsa_b200.predictor import NewtonPredictor
-    from dac_vtsa_b200.runner import run_cycle_device
+    from dac_vtsa_b200.runner import cycle_balance_errors, run_cycle_device
     out, y64 = {}, None
     for var in variants:
         cfg, g, props, st = setup(grid, VARIANTS[var])
@@ -328,13 +332,15 @@ def cycle_runs(grid, variants, weights_path, dev, y_ref_fp64=None):
             net = NewtonPredictor.load(weights_path)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        y, stats, _ = run_cycle_device(y0, cfg, g, props, predictor=net, predict=net is not None)
+        y, stats, _ = run_cycle_device(y0, cfg, g, props, predictor=net, predict=net is not None, inventories=True)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
+        wall = time.perf_counter() - t0                # (includes two host copies of the state per step)
         yh = y.cpu().numpy()
         keys = ("steps", "rejected", "newton_iters", "gmres_iters", "gmres_polish", "balance_unclosed",
                 "pred_net", "pred_extrap", "pred_retry")
+        keys += ("balance_projected",)
         rec = {"value": CYCLE_BED_S / wall, "wall_s": wall, "config": VARIANTS[var],
+               "balance_errors": cycle_balance_errors(cfg, stats),
                "solver": {k: int(sum(s.get(k, 0) for s in stats)) for k in keys}}
         if var == "fp64":
             y64 = yh

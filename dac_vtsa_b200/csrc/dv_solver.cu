@@ -1798,15 +1798,6 @@ static int newton_krylov(NewtonCtx& C, double t, const double* z0, const double*
             bool ok;
             if (cons_spec) ok = cons_eval(sv + 16);
             else DV_TRY(cons_ok(W.R, W.z, &ok));
-            if (getenv("DVTSA_TRACE_CONS")) {   // TEMPORARY diagnostic
-                double v[8];
-                if (cons_spec) memcpy(v, sv + 16, sizeof v);
-                else DV_TRY(fetch(W, W.scal, 8, v, st));
-                fprintf(stderr, "CONS it=%d pol=%d info=%d inner=%lld lam=%g step=%.3g pn=%.3g rn=%.3g dh=%.4g r=[%.3g %.3g %.3g %.3g] ok=%d\n",
-                        it, polish, info, (long long)inner, lam, step, pn, rn, dh,
-                        v[0] / (C.o.cons_tol * v[4]), v[1] / (C.o.cons_tol * v[5]), v[2] / (C.o.cons_tol * v[6]),
-                        v[3] / (C.o.cons_tol * v[7]), (int)ok);
-            }
             if (ok) {
                 DV_TRY(copy(W.z, zout));
                 r.ok = 1; r.iters = it + 1; r.rate = rate;

@@ -214,7 +214,7 @@ class _PState:
 
 
 def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predictor=None, predict=True,
-                     record_stride=0, writer=None, handoff=None):
+                     record_stride=0, writer=None, handoff=None, inventories=False):
     """Device-resident cycle: y stays on the GPU from step to step; returns (y_end, per-step stats).
 
     Per step only the start pressure field (for the valve ramps) is evaluated, through the model's
@@ -222,7 +222,9 @@ def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predic
     which is what the reference's T round trip (pack(to_state(y))) reproduces to round-off.
     predictor: a NewtonPredictor attached to every step's integrator (predict and/or record samples).
     writer + handoff (template state, cycle index, directory): each step's end state is also written
-    as the reference's hand-off CSV by the AsyncStateWriter while the next step runs."""
+    as the reference's hand-off CSV by the AsyncStateWriter while the next step runs.
+    inventories: each step's stats also carry the bed inventories at its start and end ("inv_start",
+    "inv_end"; two host copies of the state per step), the inputs of the balance rows."""
     y = y0
     stats = []
     last_model = None
@@ -233,11 +235,14 @@ def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predic
         integ = TRBDF2(model, cfg, h_max=cfg.solver.h_max_fraction * dur)
         if predictor is not None:
             predictor.attach(integ, step["type"], predict=predict, record_stride=record_stride)
+        inv0 = model.inventories(y) if inventories else None
         res = integ.integrate(y, dur, np.array([dur]), keep_on_device=True)
         y = res.y
         stats.append({"step": step["name"], "steps": res.n_steps, "rejected": res.n_reject, "nfev": res.nfev,
                       "jac": res.n_jac, "lu": res.n_lu, **integ.stats, "t": res.t,
                       "acc": dict(zip(model.acc_names, (float(a) for a in res.acc)))})
+        if inventories:
+            stats[-1].update(inv_start=inv0, inv_end=model.inventories(y))
         if writer is not None:
             template, cyc, folder = handoff
             writer.submit(y, model, template, template.t + res.t, step["name"], cyc, grid,
@@ -245,6 +250,17 @@ def run_cycle_device(y0: torch.Tensor, cfg, grid, props, T_jac_prev=None, predic
         T_jac_prev = model.T_jacket(res.t) if model.jacket_on else T_jac_prev
         last_model = model
     return y, stats, T_jac_prev
+
+
+def cycle_balance_errors(cfg, stats) -> Dict[str, float]:
+    """Worst mass / energy balance errors (validation/conservation_checks.py:29-67) of a device cycle
+    run with ``inventories=True``."""
+    from types import SimpleNamespace
+    from . import balances
+    steps = [SimpleNamespace(cycle=1, name=st["step"], acc=st["acc"], inv_start=st["inv_start"], inv_end=st["inv_end"],
+                             product_port=step.get("product_port", "V3"), valves=dict(step["valves"]))
+             for step, st in zip(cfg.cycle, stats)]
+    return balances.worst_balance_errors(steps, ("CO2", "H2O", "N2"))
 
 
 def _pressure_host(cfg, grid, props, y):

@@ -62,3 +62,54 @@ def test_cycle_matches_the_reference_cycle():
     # the same input in the reference: energy closes as tightly, species within a small factor
     assert worst["energy"] <= 2.0 * float(np.abs(d["energy_rel_err"]).max()), worst
     assert worst["mass"] <= 10.0 * float(np.abs(d["mass_rel_err"]).max()), worst
+
+
+def test_cycle_with_restarted_polish_closes_balances_better_than_the_reference():
+    """gpu.polish_cycles 4: the polish iterations' linear solves reach their tolerance as the
+    reference's exact sparse-LU solves do, and both balances close at least as tightly as in the
+    reference's own cycle from the same input; the states stay within the error scale."""
+    from dac_vtsa_b200 import balances
+    d, cfg, m0, steps, ys = _run_cycle({"gpu.polish_cycles": 4})
+    for k, (sr, y) in enumerate(zip(steps, ys)):
+        yr = d[f"s{k}_y"]
+        assert (np.abs(y - yr) / (m0.atol + cfg.solver.rtol * np.abs(yr))).max() <= 1.0, sr.name
+    worst = balances.worst_balance_errors(steps, ("CO2", "H2O", "N2"))
+    assert worst["mass"] <= float(np.abs(d["mass_rel_err"]).max()), worst
+    assert worst["energy"] <= float(np.abs(d["energy_rel_err"]).max()), worst
+
+
+def test_cycle_with_balance_projection():
+    """gpu.balance_projection: balances better than the reference's on the same input; the step-end
+    states within the error scale; the accepted steps within 35 % (the projection moves each stage
+    solution by about |W R| / |W z|, which the step-size control sees)."""
+    from dac_vtsa_b200 import balances
+    d, cfg, m0, steps, ys = _run_cycle({"gpu.balance_projection": True})
+    for k, (sr, y) in enumerate(zip(steps, ys)):
+        yr = d[f"s{k}_y"]
+        assert (np.abs(y - yr) / (m0.atol + cfg.solver.rtol * np.abs(yr))).max() <= 1.0, sr.name
+        ref_steps = json.loads(str(d[f"s{k}_solver"]))["steps"]
+        assert sr.solver["steps"] <= 1.35 * ref_steps + 3, (sr.name, sr.solver["steps"], ref_steps)
+    worst = balances.worst_balance_errors(steps, ("CO2", "H2O", "N2"))
+    assert worst["mass"] <= float(np.abs(d["mass_rel_err"]).max()), worst
+    assert worst["energy"] <= float(np.abs(d["energy_rel_err"]).max()), worst
+
+
+def test_16x16x64_cycle_with_balance_projection():
+    """The 16x16x64 bed (99 328 unknowns; the reference cannot run it): one full cycle from the
+    seeded constant-pressure state with the balance projection closes mass and energy to 1e-6 (the
+    reference's stored default-run errors are 6.77e-6 / 4.37e-6)."""
+    import torch
+    from dac_vtsa_b200 import host
+    from dac_vtsa_b200.config import load_config
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.runner import BENCH_POINT, cycle_balance_errors, run_cycle_device
+    cfg = load_config(override_dict=dict(BENCH_POINT, **{"grid.Nr": 16, "grid.Ntheta": 16, "grid.Nz": 64,
+                                                         "gpu.balance_projection": True}))
+    g = host.Grid.from_config(cfg)
+    props = host.get_backend(cfg)
+    st = host.seeded_state(cfg, g, props, seed=0)
+    y0 = torch.from_numpy(TVSAModel(cfg, g, props, cfg.cycle[0], st).pack(st)).cuda()
+    y, stats, _ = run_cycle_device(y0, cfg, g, props, inventories=True)
+    assert np.all(np.isfinite(y.cpu().numpy()))
+    worst = cycle_balance_errors(cfg, stats)
+    assert worst["mass"] <= 1e-6 and worst["energy"] <= 1e-6, worst
