@@ -4,6 +4,8 @@
 // (dv_kernels.cu, dv_linalg.cu and the vector kernels below) and the host reads back a few
 // scalars per Krylov iteration to take the same branch decisions.
 #include <atomic>
+#include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1216,7 +1218,11 @@ static void op_count(const dv_model* m, int64_t* cnt) {
     else cnt[K_MATVEC] += 3;
 }
 
-static int gm_build(dv_model* m, Work& W, int kdim) {
+// A capture that another host thread invalidated (for instance by the first launch of a kernel,
+// which loads it into the context while this thread captures): gm_build tries again.
+static constexpr int GM_CAPTURE_RETRY = 1000;
+
+static int gm_build_once(dv_model* m, Work& W, int kdim) {
     if (W.gm_exec) { cudaGraphExecDestroy(W.gm_exec); W.gm_exec = nullptr; }
     if (W.gm_graph) { cudaGraphDestroy(W.gm_graph); W.gm_graph = nullptr; }
     if (!W.gm_cs) DV_CUDA(cudaStreamCreateWithFlags(&W.gm_cs, cudaStreamNonBlocking));
@@ -1385,11 +1391,12 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         coop_ok = false;
-        return gm_build(m, W, kdim);
+        return gm_build_once(m, W, kdim);
     }
     if (e != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
+        if (e == cudaErrorStreamCaptureInvalidated) return GM_CAPTURE_RETRY;
         return cuda_fail(e, "building the GMRES graph");
     }
     W.gm_graph = graph;
@@ -1408,6 +1415,15 @@ static int gm_build(dv_model* m, Work& W, int kdim) {
         W.gm_iter[k] = iter[k];
     }
     return DV_OK;
+}
+
+static int gm_build(dv_model* m, Work& W, int kdim) {
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        const int rc = gm_build_once(m, W, kdim);
+        if (rc != GM_CAPTURE_RETRY) return rc;
+        std::this_thread::sleep_for(std::chrono::microseconds(200 << std::min(attempt, 6)));
+    }
+    return cuda_fail(cudaErrorStreamCaptureInvalidated, "building the GMRES graph (capture invalidated 16 times)");
 }
 
 // gmres() run by the graph; same contract.  b, op.z, op.f, op.s must be the workspace's own
