@@ -96,7 +96,8 @@ class DvSolverOpts(C.Structure):
 
 
 class DvTuning(C.Structure):
-    _fields_ = [("gmres_prefix", I32), ("sweep_nbuf", I32), ("spmv_block", I32), ("fdjac_block", I32)]
+    _fields_ = [("gmres_prefix", I32), ("sweep_nbuf", I32), ("spmv_block", I32), ("fdjac_block", I32),
+                ("gmres_body", I32), ("pad_", I32)]
 
 
 class DvStepReport(C.Structure):

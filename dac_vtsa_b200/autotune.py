@@ -20,9 +20,10 @@ import torch
 
 from ._lib import DvTuning, check, load
 
-FIELDS = ("gmres_prefix", "sweep_nbuf", "spmv_block", "fdjac_block")
+FIELDS = ("gmres_prefix", "sweep_nbuf", "spmv_block", "fdjac_block", "gmres_body")
 TIMES = ("fdjac_64", "fdjac_128", "sweep_nbuf2", "sweep_nbuf3", "spmv_64", "spmv_128", "spmv_256",
-         "stage_prefix0", "stage_prefix2", "stage_prefix4", "stage_prefix6", "stage_prefix8")
+         "stage_prefix0", "stage_prefix2", "stage_prefix4", "stage_prefix6", "stage_prefix8",
+         "stage_body1", "stage_body2")
 
 
 def cache_path() -> str:

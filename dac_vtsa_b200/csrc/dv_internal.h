@@ -67,6 +67,7 @@ struct Work {
     cudaStream_t gm_cs = nullptr;             // capture stream
     int gm_kdim = 0, gm_mode = -1, gm_nb = 0, gm_nparts = 0, gm_fp32 = -1, gm_zs = -1, gm_op32 = -1, gm_tuned = -2;
     int gm_prefix = 0;                        // Arnoldi steps captured ahead of the WHILE node
+    int gm_body = 1;                          // Arnoldi steps per pass through the WHILE body
     int64_t gm_fixed[K_NKIND] = {}, gm_iter[K_NKIND] = {};   // launches per graph run: fixed + per iteration
 };
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);

@@ -1197,6 +1197,19 @@ static int gmres_prefix() {
     return v;
 }
 
+// Arnoldi steps per pass through the WHILE body: the model's tuning, else DVTSA_GMRES_BODY=<1|2> from
+// the environment (read once per process), else 2.  Each pass costs a device-side relaunch; a second
+// step after the stop returns at once (the sweep sees the stop flag, the operator a zero direction).
+static int gmres_body(const dv_model* m) {
+    if (m->tune.gmres_body == 1 || m->tune.gmres_body == 2) return m->tune.gmres_body;
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("DVTSA_GMRES_BODY");
+        v = (e && e[0] == '1' && e[1] == 0) ? 1 : 2;
+    }
+    return v;
+}
+
 // DVTSA_GMRES_COOP=0 keeps the three-kernel CGS2 in the GMRES graph (read once per process)
 static bool gmres_coop_enabled() {
     static int v = -1;
@@ -1300,6 +1313,7 @@ static int gm_build_once(dv_model* m, Work& W, int kdim) {
     // two steps and most take five or more, and each pass through the WHILE body costs a device-side
     // relaunch (~20 us on B200) that a plain node does not; a step after the stop returns at once.
     const int prefix = fused ? std::min(m->tune.gmres_prefix >= 0 ? m->tune.gmres_prefix : gmres_prefix(), kdim) : 0;
+    const int body_steps = fused ? gmres_body(m) : 1;        // Arnoldi steps per pass through the WHILE body
     if (e == cudaSuccess) {
         for (int q = 0; q < prefix && e == cudaSuccess; ++q) {
             if (arnoldi_step(cs) != DV_OK) e = cudaErrorUnknown;
@@ -1325,10 +1339,12 @@ static int gm_build_once(dv_model* m, Work& W, int kdim) {
         // body: one Arnoldi step
         int rc = DV_OK;
         if (fused) {
-            rc = arnoldi_step(body_cs);
-            iter[K_PC_APPLY] += 1;
-            op_count(m, iter);
-            iter[K_VECTOR] += ncgs;
+            for (int q = 0; q < body_steps && rc == DV_OK; ++q) {
+                rc = arnoldi_step(body_cs);
+                iter[K_PC_APPLY] += 1;
+                op_count(m, iter);
+                iter[K_VECTOR] += ncgs;
+            }
         } else {
             k_gm_norm<<<g, VB, 0, body_cs>>>(n, st, W.b, W.wout, W.V, ldv, W.vin);
             iter[K_VECTOR] += 1;
@@ -1410,6 +1426,7 @@ static int gm_build_once(dv_model* m, Work& W, int kdim) {
     W.gm_fp32 = m->pc_fp32;
     W.gm_op32 = m->op32;
     W.gm_tuned = m->tune.gmres_prefix;
+    W.gm_body = body_steps;
     for (int k = 0; k < K_NKIND; ++k) {
         W.gm_fixed[k] = fixed[k];
         W.gm_iter[k] = iter[k];
@@ -1433,7 +1450,8 @@ static int gmres_graph(Work& W, const Op& op, const double* b, double rtol, doub
     dv_model* m = op.m;
     if (!W.gm_exec || W.gm_kdim != kdim || W.gm_mode != m->pc_mode || W.gm_nb != m->pc_nb ||
         W.gm_nparts != m->pc_nparts || W.gm_fp32 != m->pc_fp32 || W.gm_zs != m->pc_zs ||
-        W.gm_op32 != m->op32 || W.gm_tuned != m->tune.gmres_prefix)
+        W.gm_op32 != m->op32 || W.gm_tuned != m->tune.gmres_prefix ||
+        (precond_apply_fusable(m) && W.gm_body != gmres_body(m)))
         DV_TRY(gm_build(m, W, kdim));
     GmHost* hst = (GmHost*)W.gm_host;
     hst->args[0] = op.t;
@@ -1455,7 +1473,7 @@ static int gmres_graph_collect(Work& W, dv_model* m, int* info, int64_t* inner) 
     *info = hst->res[4];
     *inner += iters;
     m->nfev += iters + (skip ? 0 : 1);
-    const int looped = std::max(iters - W.gm_prefix, 0);      // passes through the WHILE body
+    const int looped = (std::max(iters - W.gm_prefix, 0) + W.gm_body - 1) / std::max(W.gm_body, 1);   // WHILE passes
     for (int k = 0; k < K_NKIND; ++k) count_launches(k, W.gm_fixed[k] + W.gm_iter[k] * looped);
     if (g_prof_on && !g_pending.empty()) prof_flush();
     if (hst->err != 0) {                  // (read back with the results: no extra round trip)
@@ -2224,7 +2242,8 @@ int dv_selftest_wait_timeout(int32_t polls, int32_t* bits) {
 int dv_model_set_tuning(dv_model* m, const dv_tuning* t) {
     if (!m || !t || t->gmres_prefix < -1 || t->gmres_prefix > 8 || (t->sweep_nbuf != 0 && t->sweep_nbuf != 2 &&
         t->sweep_nbuf != 3) || (t->spmv_block != 0 && t->spmv_block != 64 && t->spmv_block != 128 &&
-        t->spmv_block != 256) || (t->fdjac_block != 0 && t->fdjac_block != 64 && t->fdjac_block != 128)) {
+        t->spmv_block != 256) || (t->fdjac_block != 0 && t->fdjac_block != 64 && t->fdjac_block != 128) ||
+        t->gmres_body < 0 || t->gmres_body > 2) {
         set_error("dv_model_set_tuning: parameter outside its candidates");
         return DV_ERR_ARG;
     }
@@ -2314,6 +2333,18 @@ int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps,
             return newton_krylov(C, t + dh, z0, y, dh, zo, st);
         }, &tm[7 + q]);
         if (rc == DV_OK && tm[7 + q] < bestv) { bestv = tm[7 + q]; tu.gmres_prefix = 2 * q; }
+    }
+    m->tune.gmres_prefix = tu.gmres_prefix;
+    bestv = INFINITY;
+    for (int q = 0; q < 2 && rc == DV_OK; ++q) {          // steps per WHILE pass, with the chosen prefix
+        m->tune.gmres_body = 1 + q;
+        rc = time_us(st, std::max(1, reps / 10), [&] {
+            dv_newton_result r;
+            memset(&r, 0, sizeof r);
+            NewtonCtx C{m, &W, m->d_atol7, n, (int64_t)(DV_NG + DV_NA) * m->nc, no, &r, nullptr};
+            return newton_krylov(C, t + dh, z0, y, dh, zo, st);
+        }, &tm[12 + q]);
+        if (rc == DV_OK && tm[12 + q] < bestv) { bestv = tm[12 + q]; tu.gmres_body = 1 + q; }
     }
     m->nfev = nfev0;
     cudaFree(z0);

@@ -292,10 +292,13 @@ int dv_integrator_copy_y(const dv_integrator* g, double* dst, void* stream);
  * No reference counterpart.  Launch parameters of the hot kernels, per model: the Arnoldi steps the
  * GMRES graph runs ahead of its WHILE node (gmres_prefix, -1 = library default), the depth of the
  * preconditioner sweep's shared-memory ring of factor blocks (sweep_nbuf 2 or 3, 0 = deepest that
- * fits), the block sizes of the FP32 Jacobian product and of the FD Jacobian (0 = 128).  None of them
- * changes a result bit; they only change the time. */
+ * fits), the block sizes of the FP32 Jacobian product and of the FD Jacobian (0 = 128), and the Arnoldi
+ * steps per pass through the WHILE node (gmres_body 1 or 2, 0 = library default: every pass costs a
+ * device-side relaunch; a step after the stop returns at once).  None of them changes a result bit;
+ * they only change the time. */
 typedef struct dv_tuning {
     int32_t gmres_prefix, sweep_nbuf, spmv_block, fdjac_block;
+    int32_t gmres_body, pad_;
 } dv_tuning;
 int dv_model_set_tuning(dv_model* m, const dv_tuning* t);
 int dv_model_get_tuning(const dv_model* m, dv_tuning* t);
@@ -303,9 +306,9 @@ int dv_model_get_tuning(const dv_model* m, dv_tuning* t);
  * candidate of each parameter (`reps` launches each; the GMRES prefix by whole Newton stage solves)
  * with CUDA events on `stream`, keep the fastest in the model and return it in *best.  times_us
  * (optional, ntimes entries) receives the measured per-launch times in the order: fdjac 64, 128;
- * sweep nbuf 2, 3; spmv 64, 128, 256; stage solve with prefix 0, 2, 4, 6, 8 (0 where a candidate does
- * not apply).  Synchronises. */
-#define DV_TUNE_NTIMES 12
+ * sweep nbuf 2, 3; spmv 64, 128, 256; stage solve with prefix 0, 2, 4, 6, 8; stage solve with the
+ * chosen prefix and body 1, 2 (0 where a candidate does not apply).  Synchronises. */
+#define DV_TUNE_NTIMES 14
 int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps, dv_tuning* best, double* times_us,
                 int32_t ntimes, void* stream);
 

@@ -25,6 +25,7 @@ def test_autotune_choices_are_measured_candidates():
     assert params["spmv_block"] in (64, 128, 256)
     assert params["gmres_prefix"] in (0, 2, 4, 6, 8)
     assert params["sweep_nbuf"] in (0, 2, 3)
+    assert params["gmres_body"] in (1, 2)
     assert all(times[k] > 0 for k in ("fdjac_64", "fdjac_128", "spmv_64", "spmv_128", "spmv_256", "stage_prefix0"))
     assert autotune.get(m) == params
 
@@ -37,7 +38,8 @@ def test_tuned_parameters_do_not_change_results(tmp_path, monkeypatch):
     from dac_vtsa_b200.solver import TRBDF2
     monkeypatch.setenv("DVTSA_TUNE_CACHE", str(tmp_path / "tune.json"))
     runs = []
-    for params in (None, {"gmres_prefix": 0, "sweep_nbuf": 2, "spmv_block": 256, "fdjac_block": 64}):
+    for params in (None, {"gmres_prefix": 0, "sweep_nbuf": 2, "spmv_block": 256, "fdjac_block": 64,
+                          "gmres_body": 1}):
         d, m, cfg, meta = _c0()
         if params:
             autotune.apply(m, params)
