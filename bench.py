@@ -92,7 +92,7 @@ class Window:
         tmp = model_cls(self.cfg, self.grid, self.props, self.step, st)
         c, q, e, Tw = tmp.unpack(self.y)
         st.c, st.q, st.Tw = c.copy(), q.copy(), Tw.copy()
-        st.T = tmp.to_state(self.y, st, 0.0, "heating").T
+        st.T = tmp.temperature(e, c, q)
         self.state = st
         self.h_max = self.cfg.solver.h_max_fraction * float(self.step["duration"])
 

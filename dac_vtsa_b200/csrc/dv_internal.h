@@ -15,6 +15,12 @@ inline int launch_ok(const char* what) {
     return e == cudaSuccess ? DV_OK : cuda_fail(e, what);
 }
 
+// Dynamic shared memory above 48 KB for kernel `func`: its attribute is raised once per device, to
+// the most the kernel can take, under a lock.  Models of different sizes launch the same kernel with
+// different amounts from several host threads (an ensemble); setting the attribute to each launch's
+// own amount would let one thread lower it under another's launch.
+cudaError_t allow_dyn_smem(const void* func);
+
 // Launch accounting: every kernel launch of the library goes through DV_LAUNCH, which counts it per
 // kind and, when profiling is on (dv_profile_enable), brackets it with CUDA events on its stream.
 enum KernelKind { K_RESIDUAL = 0, K_MATVEC = 1, K_FDJAC = 2, K_PC_FACTOR = 3, K_PC_APPLY = 4, K_VECTOR = 5,

@@ -1609,13 +1609,13 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
     g.zs = pc_twist_zs(g, pc_tsize(m), factor_smem);
     if (factor_smem && g.zs > 0) {
         if (dyn > 48 * 1024)
-            DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            DV_CUDA(allow_dyn_smem((const void*)k_pc_factor_smem<true>));
         DV_LAUNCH(dv::K_PC_FACTOR, s,
                   DV_CUDA(launch_pair(k_pc_factor_smem<true>, 2u * g.nparts, 256u, dyn, s, g, m->d_pc, m->d_pc_info,
                                       lds)));
     } else if (factor_smem) {
         if (dyn > 48 * 1024)
-            DV_CUDA(cudaFuncSetAttribute(k_pc_factor_smem<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            DV_CUDA(allow_dyn_smem((const void*)k_pc_factor_smem<false>));
         DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_smem<false><<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_info, lds));
     } else {
         const size_t static_smem = (2 * 1024 + 256) * sizeof(double) + 256 * sizeof(int);
@@ -1623,7 +1623,7 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
         int use_smem = (need + static_smem) <= (size_t)optin ? 1 : 0;
         size_t dyn = use_smem ? need : 0;
         if (use_smem && dyn > 48 * 1024)
-            DV_CUDA(cudaFuncSetAttribute(k_pc_factor_glob, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            DV_CUDA(allow_dyn_smem((const void*)k_pc_factor_glob));
         DV_LAUNCH(dv::K_PC_FACTOR, s, k_pc_factor_glob<<<g.nparts, 256, dyn, s>>>(g, m->d_pc, m->d_pc_work, m->d_pc_info, use_smem));
     }
     if (m->pc_fp32) {               // the sweep streams an FP32 copy of the factors
@@ -1658,7 +1658,7 @@ static void launch_apply_tw(const PcGeom& g, dv_model* m, const TS* A, const dou
                             cudaStream_t s, const PaFuse& F, bool count) {
     const size_t dyn = apply_smem(g, NBUF, sizeof(TS));
     auto kern = k_pc_apply<NJ, NBUF, TS, TW>;
-    if (count && dyn > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (dyn > 48 * 1024) allow_dyn_smem((const void*)kern);
     if (count) prof_begin(dv::K_PC_APPLY, s);
     if (TW) launch_pair(kern, 2u * g.nparts, PA_THREADS, dyn, s, g, A, b, sc, x, m->d_err, F);
     else kern<<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F);

@@ -230,11 +230,7 @@ __global__ void __launch_bounds__(128) k_gemm(GemmP g) {
 }
 
 static int gemm(const GemmP& g, int grid, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM_ALLOC);
-        attr = true;
-    }
+    DV_CUDA(dv::allow_dyn_smem((const void*)k_gemm));
     DV_LAUNCH(dv::K_MLP, s, k_gemm<<<grid, 128, GEMM_SMEM_ALLOC, s>>>(g));
     return launch_ok("k_gemm");
 }

@@ -4,6 +4,7 @@
 // (dv_kernels.cu, dv_linalg.cu and the vector kernels below) and the host reads back a few
 // scalars per Krylov iteration to take the same branch decisions.
 #include <atomic>
+#include <mutex>
 #include <chrono>
 #include <thread>
 #include <cmath>
@@ -21,6 +22,25 @@
 namespace dv {
 
 static thread_local std::string g_err;
+
+cudaError_t allow_dyn_smem(const void* func) {
+    static std::mutex mu;
+    static std::vector<std::pair<int, const void*>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto& d : done)
+        if (d.first == dev && d.second == func) return cudaSuccess;
+    int optin = 0;
+    cudaFuncAttributes fa;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess ||
+        (e = cudaFuncGetAttributes(&fa, func)) != cudaSuccess)
+        return e;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    if (e == cudaSuccess) done.emplace_back(dev, func);
+    return e;
+}
 void set_error(const std::string& m) { g_err = m; }
 
 // ---------------------------------------------------------------- launch accounting / profiler

@@ -33,8 +33,9 @@ def test_network_starts_closer_to_the_stage_solutions():
     O = np.concatenate([net.forward(X[i:i + 65536]) for i in range(0, len(X), 65536)])
     err = T[:, :6] - O[:, :6] * nrm[13:19]
     rms = lambda a: float(np.sqrt(np.mean(np.asarray(a, dtype=np.float64) ** 2)))
-    for v in range(6):
-        assert rms(err[:, v]) < 0.97 * rms(T[:, v]), (v, rms(err[:, v]), rms(T[:, v]))
+    ratios = [rms(err[:, v]) / rms(T[:, v]) for v in range(6)]
+    assert max(ratios) < 1.0, ratios                        # closer for every unknown
+    assert float(np.exp(np.mean(np.log(ratios)))) < 0.9, ratios   # by 10 % or more on (geometric) average
 
 
 def test_cycle_with_the_network_reaches_the_plain_states():

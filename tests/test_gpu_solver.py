@@ -268,21 +268,25 @@ def test_replay_step_end_states_within_1e8():
     assert np.allclose(acc_gpu, acc_cpu, rtol=1e-8, atol=1e-20)
 
 
-def test_mixed_precision_replay_matches_fp64_within_1e6():
-    """Mixed-precision Krylov (GMRES on the FP32 assembled Jacobian with FP32 factors; FP64 residual and
-    Newton update) replaying the reference's first accepted steps of the 4x4x16 adsorption with every
-    stage solved tightly: the step-end states agree with the FP64 path's to <= 1e-6 relative per
-    entry (the stated mixed-mode tolerance; FP64 refinement makes the agreement far closer)."""
+@pytest.mark.parametrize("precision", ["fp32_factors", "fp32"])
+def test_mixed_precision_replay_matches_fp64_within_1e6(precision):
+    """Mixed precision (FP32 factors; and GMRES on the FP32 assembled Jacobian with FP32 factors) with
+    the FP64 residual and Newton update, replaying the reference's first accepted steps of the
+    4x4x16 adsorption with every stage solved tightly: the step-end states agree with the FP64
+    path's to <= 1e-6 relative per entry (the stated mixed-mode tolerance).  The FP32 operator's
+    Newton iteration contracts linearly, so its stages are solved to 1e-9 of the error scale in up
+    to 60 iterations (the FP64 path: 1e-11)."""
     from dac_vtsa_b200.model import TVSAModel
     from dac_vtsa_b200.replay import fixed_step_run as gpu_run
     d, m64, cfg, meta = _c0_model(TVSAModel)
     _, m32, _, _ = _c0_model(TVSAModel)
-    m32.set_krylov_precision("fp32")
+    m32.set_krylov_precision(precision)
     ts = np.concatenate([[0.0], d["s0_t_accepted"]])
     hs = np.diff(ts)[:12]
     y0 = d["s0_y0"]
     ys64, acc64 = gpu_run(m64, y0, hs, scheme="trbdf2")
-    ys32, acc32 = gpu_run(m32, y0, hs, scheme="trbdf2")
+    kw = {"kappa": 1e-9, "max_iter": 60} if precision == "fp32" else {}
+    ys32, acc32 = gpu_run(m32, y0, hs, scheme="trbdf2", **kw)
     worst = max(float((np.abs(a - b) / (np.abs(b) + m64.atol)).max()) for a, b in zip(ys32, ys64))
     assert worst <= 1e-6, worst
     assert np.allclose(acc32, acc64, rtol=1e-6, atol=1e-20)
@@ -368,10 +372,13 @@ def test_fp32_factors_solve_to_single_precision(Nz):
     assert 0.0 < rel < 1e-5, rel
 
 
-def test_mixed_precision_adsorption_stays_within_solver_tolerance():
-    """Free-running 200 s adsorption of the 4x4x16 bed with gpu.krylov_precision = fp32: the end
-    state matches the FP64 run within the solver's own error scale (atol + rtol |y|) and the
-    step count stays close; only the preconditioner changes, the Newton tolerance judges."""
+@pytest.mark.parametrize("precision,step_slack", [("fp32_factors", 0.15), ("fp32", 0.5)])
+def test_mixed_precision_adsorption_stays_within_solver_tolerance(precision, step_slack):
+    """Free-running 200 s adsorption of the 4x4x16 bed with gpu.krylov_precision = fp32_factors /
+    fp32: the end state matches the FP64 run within the solver's own error scale (atol + rtol |y|);
+    the Newton tolerance judges every stage.  The step count stays within 15 % with FP32 factors;
+    the FP32 operator (an inexact Newton with the step start's Jacobian, in FP32) needs up to 50 %
+    more steps (measured 128 against 97)."""
     from dac_vtsa_b200.config import load_config
     from dac_vtsa_b200.model import TVSAModel
     from dac_vtsa_b200.solver import TRBDF2
@@ -379,7 +386,7 @@ def test_mixed_precision_adsorption_stays_within_solver_tolerance():
     dur = meta["duration"]
     r64 = TRBDF2(m, cfg, h_max=cfg.solver.h_max_fraction * dur).integrate(d["s0_y0"], dur, [dur])
     over = json.loads(str(d["over"]))
-    over["gpu.krylov_precision"] = "fp32"
+    over["gpu.krylov_precision"] = precision
     d2, m2, cfg2, _ = _c0_model(TVSAModel)
     cfg32 = load_config(override_dict=over)
     integ = TRBDF2(m2, cfg32, h_max=cfg32.solver.h_max_fraction * dur)
@@ -387,7 +394,7 @@ def test_mixed_precision_adsorption_stays_within_solver_tolerance():
     sc = m.atol + cfg.solver.rtol * np.abs(r64.y)
     err = np.sqrt(np.mean(((r32.y - r64.y) / sc) ** 2))
     assert err < 1.0, err
-    assert abs(r32.n_steps - r64.n_steps) <= max(5, 0.15 * r64.n_steps), (r32.n_steps, r64.n_steps)
+    assert abs(r32.n_steps - r64.n_steps) <= max(5, step_slack * r64.n_steps), (r32.n_steps, r64.n_steps)
 
 
 _GRAPH_FORM_RUN = r"""
