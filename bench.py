@@ -92,7 +92,8 @@ class Window:
         tmp = model_cls(self.cfg, self.grid, self.props, self.step, st)
         c, q, e, Tw = tmp.unpack(self.y)
         st.c, st.q, st.Tw = c.copy(), q.copy(), Tw.copy()
-        st.T = tmp.temperature(e, c, q)
+        thermo = getattr(tmp, "thermo", tmp)          # the GPU model keeps e -> T in its thermo helper
+        st.T = thermo.temperature(e, c, q)
         self.state = st
         self.h_max = self.cfg.solver.h_max_fraction * float(self.step["duration"])
 

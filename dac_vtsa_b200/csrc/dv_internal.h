@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <mutex>
 #include <string>
 #include "dacvtsa.h"
 
@@ -20,6 +21,11 @@ inline int launch_ok(const char* what) {
 // different amounts from several host threads (an ensemble); setting the attribute to each launch's
 // own amount would let one thread lower it under another's launch.
 cudaError_t allow_dyn_smem(const void* func);
+
+// Held while a GMRES graph is captured and while handles are created or destroyed (device memory
+// allocated or freed, device-wide synchronisations): models driven from several host threads then
+// never allocate, free or synchronise the device in the middle of another thread's stream capture.
+std::recursive_mutex& capture_mutex();
 
 // Launch accounting: every kernel launch of the library goes through DV_LAUNCH, which counts it per
 // kind and, when profiling is on (dv_profile_enable), brackets it with CUDA events on its stream.

@@ -583,6 +583,7 @@ void bf16_round_host(const float* x, int64_t n, std::vector<uint16_t>& out) {
 extern "C" {
 
 int dv_mlp_create(int64_t sample_capacity, uint64_t seed, dv_mlp** out) {
+    std::lock_guard<std::recursive_mutex> lk_(dv::capture_mutex());
     if (!out || sample_capacity < 0) { set_error("dv_mlp_create: bad argument"); return DV_ERR_ARG; }
     dv_mlp* n = new dv_mlp();
     n->cap = (sample_capacity + NB - 1) / NB * NB;
@@ -627,6 +628,7 @@ int dv_mlp_create(int64_t sample_capacity, uint64_t seed, dv_mlp** out) {
 }
 
 int dv_mlp_destroy(dv_mlp* n) {
+    std::lock_guard<std::recursive_mutex> lk_(dv::capture_mutex());
     if (!n) return DV_OK;
     void* ptrs[] = {n->P, n->G, n->Mo, n->Vo, n->W1, n->W2, n->W3, n->W4, n->W2t, n->W3t, n->W4t, n->norm, n->Xs, n->Ts,
                     n->Xb, n->Xbt, n->H1, n->H2, n->H3, n->H1t, n->H2t, n->H3t, n->D4, n->D4t, n->D3, n->D2, n->D1,

@@ -23,6 +23,11 @@ namespace dv {
 
 static thread_local std::string g_err;
 
+std::recursive_mutex& capture_mutex() {
+    static std::recursive_mutex mu;
+    return mu;
+}
+
 cudaError_t allow_dyn_smem(const void* func) {
     static std::mutex mu;
     static std::vector<std::pair<int, const void*>> done;
@@ -1455,6 +1460,7 @@ static int gm_build_once(dv_model* m, Work& W, int kdim) {
 }
 
 static int gm_build(dv_model* m, Work& W, int kdim) {
+    std::lock_guard<std::recursive_mutex> lk(capture_mutex());
     for (int attempt = 0; attempt < 16; ++attempt) {
         const int rc = gm_build_once(m, W, kdim);
         if (rc != GM_CAPTURE_RETRY) return rc;
@@ -2279,6 +2285,7 @@ int dv_model_get_tuning(const dv_model* m, dv_tuning* t) {
 
 int dv_autotune(dv_model* m, double t, const double* y, double dh, int32_t reps, dv_tuning* best, double* times_us,
                 int32_t ntimes, void* stream) {
+    std::lock_guard<std::recursive_mutex> lk_(capture_mutex());
     if (!m || !y || !best || reps < 1 || dh <= 0.0) { set_error("dv_autotune: bad argument"); return DV_ERR_ARG; }
     cudaStream_t st = (cudaStream_t)stream;
     Work& W = *m->W;
@@ -2427,6 +2434,7 @@ int dv_model_set_krylov_fp32(dv_model* m, int32_t mask) {
 }
 
 int dv_model_destroy(dv_model* m) {
+    std::lock_guard<std::recursive_mutex> lk_(capture_mutex());
     if (!m) return DV_OK;
     void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_diag, m->d_acc, m->d_pc, m->d_pc32, m->d_J32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
                     m->d_err};
@@ -2442,6 +2450,7 @@ int dv_model_destroy(dv_model* m) {
 
 int dv_model_create(const dv_step_params* p, const double* feed_flux, const double* n_nom, const double* coverage,
                     dv_model** out) {
+    std::lock_guard<std::recursive_mutex> lk_(capture_mutex());
     if (!p || !out || !feed_flux || !n_nom || !coverage) { set_error("null argument"); return DV_ERR_ARG; }
     if (p->Nr < 1 || p->Nth < 1 || p->Nz < 1 || p->Nr > DV_MAX_NR || p->Nth == 2) {
         set_error("grid dimensions outside the supported range (1 <= Nr <= 64, Ntheta != 2)");
@@ -2631,6 +2640,7 @@ int dv_newton_stage(dv_model* m, double t, const double* z0, const double* rhs_k
 
 // ------------------------------------------------------------------ integrator
 int dv_integrator_destroy(dv_integrator* g) {
+    std::lock_guard<std::recursive_mutex> lk_(capture_mutex());
     if (!g) return DV_OK;
     double* ptrs[] = {g->y, g->fn, g->slope, g->z1, g->z2, g->f1, g->f2, g->rhs1, g->rhs2, g->pred, g->ev, g->es, g->d_g,
                       g->yprev, g->zext};
@@ -2645,6 +2655,7 @@ int dv_integrator_destroy(dv_integrator* g) {
 }
 
 int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** out) {
+    std::lock_guard<std::recursive_mutex> lk_(capture_mutex());
     if (!m || !o || !out) { set_error("null argument"); return DV_ERR_ARG; }
     if (o->scheme != 0 && o->scheme != 1) { set_error("scheme must be 0 (sdirk2) or 1 (trbdf2)"); return DV_ERR_ARG; }
     dv_integrator* g = new dv_integrator();
