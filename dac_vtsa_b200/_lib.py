@@ -110,11 +110,15 @@ class DvStepReport(C.Structure):
                 ("balance_projected", I64)]
 
 
+STRUCT_MIRRORS = {"dv_newton_opts": DvNewtonOpts, "dv_newton_result": DvNewtonResult, "dv_solver_opts": DvSolverOpts,
+                  "dv_step_report": DvStepReport, "dv_tuning": DvTuning}
+
 P = C.c_void_p
 # (name, restype, argtypes) of every entry point declared in include/dacvtsa.h
 SIGNATURES = [
     ("dv_abi_version", C.c_int, []),
     ("dv_step_params_size", C.c_size_t, []),
+    ("dv_struct_size", C.c_size_t, [C.c_char_p]),
     ("dv_last_error", C.c_char_p, []),
     ("dv_device_count", C.c_int, [C.POINTER(C.c_int)]),
     ("dv_profile_enable", C.c_int, [I32]),
@@ -185,6 +189,9 @@ def load(path: str = LIB_PATH):
         fn.argtypes = args
     if lib.dv_step_params_size() != C.sizeof(DvStepParams):
         raise LibraryError("dv_step_params layout mismatch between include/dacvtsa.h and the ctypes mirror")
+    for cname, mirror in STRUCT_MIRRORS.items():
+        if lib.dv_struct_size(cname.encode()) != C.sizeof(mirror):
+            raise LibraryError(f"{cname} layout mismatch between include/dacvtsa.h and the ctypes mirror")
     _lib = lib
     return lib
 

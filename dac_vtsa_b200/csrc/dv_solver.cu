@@ -2410,6 +2410,17 @@ int dv_profile_read(int32_t kind, int64_t* launches, int64_t* timed, double* tot
 
 int64_t dv_launch_count(void) { return g_launches.load(); }
 size_t dv_step_params_size(void) { return sizeof(dv_step_params); }
+
+size_t dv_struct_size(const char* name) {
+    if (!name) return 0;
+    const std::string n(name);
+    if (n == "dv_newton_opts") return sizeof(dv_newton_opts);
+    if (n == "dv_newton_result") return sizeof(dv_newton_result);
+    if (n == "dv_solver_opts") return sizeof(dv_solver_opts);
+    if (n == "dv_step_report") return sizeof(dv_step_report);
+    if (n == "dv_tuning") return sizeof(dv_tuning);
+    return 0;
+}
 const char* dv_last_error(void) { return g_err.c_str(); }
 
 int dv_device_count(int* n) {

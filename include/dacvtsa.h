@@ -123,6 +123,9 @@ typedef struct dv_integrator dv_integrator;
 /* ------------------------------------------------------------------ library */
 int dv_abi_version(void);
 size_t dv_step_params_size(void);
+/* sizeof of the ABI's other structs, by name ("dv_newton_opts", "dv_newton_result", "dv_solver_opts",
+ * "dv_step_report", "dv_tuning"); 0 for an unknown name.  Lets a binding check its mirrors. */
+size_t dv_struct_size(const char* name);
 const char* dv_last_error(void);
 int dv_device_count(int* n);
 

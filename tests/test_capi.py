@@ -29,6 +29,9 @@ def test_library_exports_every_declared_symbol():
     assert {n for n, _, _ in _lib.SIGNATURES} == set(names)
     assert lib.dv_abi_version() == 1
     assert lib.dv_step_params_size() == ctypes.sizeof(_lib.DvStepParams)
+    for cname, mirror in _lib.STRUCT_MIRRORS.items():
+        assert lib.dv_struct_size(cname.encode()) == ctypes.sizeof(mirror), cname
+    assert lib.dv_struct_size(b"no_such_struct") == 0
 
 
 def test_colouring_bit_identical_to_reference():
