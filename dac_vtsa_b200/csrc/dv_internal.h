@@ -85,6 +85,14 @@ struct Work {
 int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
 
 #ifdef __CUDACC__
+// Programmatic dependent launch (sm_90+): a kernel launched with programmatic stream serialisation
+// may start while its predecessor in the stream is still running; pdl_wait() blocks until that
+// predecessor has completed and its writes are visible, so it comes before the kernel's first read
+// of anything its predecessors wrote.  pdl_trigger() lets this kernel's own programmatic dependent
+// be scheduled now (its blocks then wait in pdl_wait()).  Both return at once in a kernel launched
+// without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 // sum of p[b * stride], b < nb, in index order: the deterministic finish of per-block partials
 // written by other SMs (volatile loads: never served from this SM's L1)
 __device__ __forceinline__ double sum_partials(const double* p, int nb, int64_t stride) {
@@ -191,7 +199,11 @@ struct PaFuse {
     double* out = nullptr;
     int64_t n = 0;
     const int* stop = nullptr;        // when *stop != 0 at launch: write *out = 0 and do nothing else
+    bool pdl = false;                 // launch with programmatic stream serialisation (inside the GMRES graph)
 };
+// Programmatic dependent launches inside the GMRES graph: off unless DVTSA_PDL=1 (read once;
+// measured 2 % slower on the 8x8x32 heating window, bit-identical results).
+bool pdl_enabled();
 bool precond_apply_fusable(dv_model* m);
 // bounded-wait self-test: one sweep-style mbarrier wait that nothing completes (bit 1 of *err)
 int selftest_mbar_timeout(int polls, int* err, cudaStream_t s);

@@ -4,6 +4,7 @@
 #include "dv_residual.cuh"
 
 #include <mutex>
+#include <utility>
 
 namespace dv {
 
@@ -339,6 +340,8 @@ template <int MODE>
 __global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
                                                const double* __restrict__ u, const double* __restrict__ sc,
                                                const double* __restrict__ scal) {
+    pdl_wait();                             // (launched programmatically inside the GMRES graph)
+    pdl_trigger();
     const int64_t nc = S.nc;
     const int64_t c = (int64_t)blockIdx.x * 32 + (threadIdx.x & 31);
     const bool half = (threadIdx.x >> 5) != 0;             // warp-uniform
@@ -404,6 +407,8 @@ static __device__ __forceinline__ void sp_slope(const dv_step_params& p, const S
 template <bool REC>
 __global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S, Rec rec, double t,
                                               const double* __restrict__ scal, const double* __restrict__ dargs) {
+    pdl_wait();
+    pdl_trigger();
     if (scal && scal[0] == 0.0) return;
     if (dargs) t = dargs[0];
     const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
@@ -490,6 +495,7 @@ __global__ void __launch_bounds__(64) k_assemble(dv_step_params p, Aux aux, Spli
                                                  const double* __restrict__ sc, const double* __restrict__ f0,
                                                  const double* __restrict__ scal, double gh,
                                                  double* __restrict__ out, const double* __restrict__ dargs) {
+    pdl_wait();
     const int64_t nc = S.nc;
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
@@ -619,6 +625,22 @@ int launch_matvec(dv_model* m, double t, const double* z, const double* u, const
     return split_residual<M_MATVEC, false>(m, rec, t, z, u, sc, f0, scal, dh, out, s, dv::K_MATVEC);
 }
 
+// Launch with programmatic stream serialisation (the kernel must begin with pdl_wait()).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 int matvec_capture(dv_model* m, const double* dargs, const double* z, const double* u, const double* sc,
                    const double* f0, const double* scal, double* out, cudaStream_t s) {
     const dv_step_params& p = m->p;
@@ -626,6 +648,13 @@ int matvec_capture(dv_model* m, const double* dargs, const double* z, const doub
     const Rec rec = make_rec(m->rl, m->d_rec);
     const int64_t ncol = (int64_t)p.Nr * p.Nth;
     const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
+    if (pdl_enabled()) {       // each kernel may start while its predecessor drains (pdl_wait in the kernel)
+        DV_CUDA(launch_pdl(k_cprops<M_MATVEC>, nblk(m->nc, 32), 64, s, p, S, z, u, sc, scal));
+        DV_CUDA(launch_pdl(k_faces<false>, nblk(nfaces, 64), 64, s, p, aux_of(m), S, rec, 0.0, scal, dargs));
+        DV_CUDA(launch_pdl(k_assemble<M_MATVEC, false>, nblk(m->nc, 64), 64, s, p, aux_of(m), S, rec, 0.0, z, u, sc, f0,
+                           scal, 0.0, out, dargs));
+        return DV_OK;
+    }
     k_cprops<M_MATVEC><<<nblk(m->nc, 32), 64, 0, s>>>(p, S, z, u, sc, scal);
     k_faces<false><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, scal, dargs);
     k_assemble<M_MATVEC, false><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, z, u, sc, f0, scal, 0.0,

@@ -1041,6 +1041,8 @@ template <int NJ, int NBUF, typename TS, bool TW>
 __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* __restrict__ A,
                                                          const double* __restrict__ b, const double* __restrict__ sc,
                                                          double* __restrict__ x, int* __restrict__ err, PaFuse F) {
+    pdl_wait();                                // (launched programmatically inside the GMRES graph)
+    pdl_trigger();
     if (F.stop && *F.stop) {                   // an Arnoldi step after the solve stopped: a zero direction
         if (blockIdx.x == 0 && threadIdx.x == 0 && F.out) *F.out = 0.0;
         return;                                // (every CTA of the grid returns here: no barrier is left open)
@@ -1556,19 +1558,21 @@ int64_t precond_work_doubles(int nb, int nparts, int Nz) {
 // a launch of `kern` as clusters of two CTAs (grid = 2 x partitions)
 template <typename... KArgs, typename... Args>
 static cudaError_t launch_pair(void (*kern)(KArgs...), unsigned grid, unsigned block, size_t dyn, cudaStream_t s,
-                               Args&&... args) {
+                               bool pdl, Args&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = dyn;
     cfg.stream = s;
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = 2;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl ? 2 : 1;
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
@@ -1611,7 +1615,7 @@ int precond_factor(dv_model* m, const double* J, double dh, int mode, cudaStream
         if (dyn > 48 * 1024)
             DV_CUDA(allow_dyn_smem((const void*)k_pc_factor_smem<true>));
         DV_LAUNCH(dv::K_PC_FACTOR, s,
-                  DV_CUDA(launch_pair(k_pc_factor_smem<true>, 2u * g.nparts, 256u, dyn, s, g, m->d_pc, m->d_pc_info,
+                  DV_CUDA(launch_pair(k_pc_factor_smem<true>, 2u * g.nparts, 256u, dyn, s, false, g, m->d_pc, m->d_pc_info,
                                       lds)));
     } else if (factor_smem) {
         if (dyn > 48 * 1024)
@@ -1660,7 +1664,7 @@ static void launch_apply_tw(const PcGeom& g, dv_model* m, const TS* A, const dou
     auto kern = k_pc_apply<NJ, NBUF, TS, TW>;
     if (dyn > 48 * 1024) allow_dyn_smem((const void*)kern);
     if (count) prof_begin(dv::K_PC_APPLY, s);
-    if (TW) launch_pair(kern, 2u * g.nparts, PA_THREADS, dyn, s, g, A, b, sc, x, m->d_err, F);
+    if (TW) launch_pair(kern, 2u * g.nparts, PA_THREADS, dyn, s, F.pdl, g, A, b, sc, x, m->d_err, F);
     else kern<<<g.nparts, PA_THREADS, dyn, s>>>(g, A, b, sc, x, m->d_err, F);
     if (count) prof_end(dv::K_PC_APPLY, s);
 }

@@ -23,6 +23,15 @@ namespace dv {
 
 static thread_local std::string g_err;
 
+bool pdl_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("DVTSA_PDL");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1;
+}
+
 std::recursive_mutex& capture_mutex() {
     static std::recursive_mutex mu;
     return mu;
@@ -1310,6 +1319,7 @@ static int gm_build_once(dv_model* m, Work& W, int kdim) {
         F.out = W.scal + 0;
         F.n = n;
         F.stop = &st->done;
+        F.pdl = pdl_enabled();
         int rc = precond_apply_capture(m, W.vin, W.s, W.u, c, F);
         if (rc == DV_OK) rc = op_capture(m, W, dargs, W.wout, c);
         if (coop) {                          // CGS2 as one cooperative launch (co-resident blocks)
@@ -1408,6 +1418,7 @@ static int gm_build_once(dv_model* m, Work& W, int kdim) {
             F.ticket = W.tickets + 4;
             F.out = W.scal + 0;
             F.n = n;
+            F.pdl = pdl_enabled();
             rc = precond_apply_capture(m, W.x, W.s, W.u, cs, F);
         } else {
             rc = precond_apply_capture(m, W.x, W.s, W.u, cs);
