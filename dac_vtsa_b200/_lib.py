@@ -119,6 +119,8 @@ SIGNATURES = [
     ("dv_abi_version", C.c_int, []),
     ("dv_step_params_size", C.c_size_t, []),
     ("dv_struct_size", C.c_size_t, [C.c_char_p]),
+    ("dv_pool_cached_bytes", C.c_int64, []),
+    ("dv_pool_release", C.c_int, []),
     ("dv_last_error", C.c_char_p, []),
     ("dv_device_count", C.c_int, [C.POINTER(C.c_int)]),
     ("dv_profile_enable", C.c_int, [I32]),
@@ -225,6 +227,16 @@ def profile_read():
         check(lib.dv_profile_read(k, C.byref(a), C.byref(b), C.byref(ms)), "dv_profile_read")
         out[name] = (a.value, b.value, ms.value)
     return out
+
+
+def pool_cached_bytes() -> int:
+    """Device and pinned memory of destroyed handles that the library keeps for the next ones."""
+    return int(load().dv_pool_cached_bytes())
+
+
+def pool_release():
+    """Free the memory the library keeps for future handles."""
+    check(load().dv_pool_release(), "dv_pool_release")
 
 
 def launch_count() -> int:

@@ -27,6 +27,16 @@ cudaError_t allow_dyn_smem(const void* func);
 // never allocate, free or synchronise the device in the middle of another thread's stream capture.
 std::recursive_mutex& capture_mutex();
 
+// Buffer pool of the handles' device and pinned host memory: a destroyed handle's buffers are kept
+// per (device, size) and handed to the next handle that asks for the same size, so the reference's
+// pattern of one model and one integrator per cycle step allocates once per shape instead of every
+// step.  pool_free / pool_free_host take only memory from pool_malloc / pool_malloc_host; the
+// caller makes sure no work in flight still uses it (handle destruction synchronises the device).
+cudaError_t pool_malloc(void** p, size_t bytes);
+cudaError_t pool_malloc_host(void** p, size_t bytes);
+void pool_free(void* p);
+void pool_free_host(void* p);
+
 // Launch accounting: every kernel launch of the library goes through DV_LAUNCH, which counts it per
 // kind and, when profiling is on (dv_profile_enable), brackets it with CUDA events on its stream.
 enum KernelKind { K_RESIDUAL = 0, K_MATVEC = 1, K_FDJAC = 2, K_PC_FACTOR = 3, K_PC_APPLY = 4, K_VECTOR = 5,

@@ -4,7 +4,9 @@
 // (dv_kernels.cu, dv_linalg.cu and the vector kernels below) and the host reads back a few
 // scalars per Krylov iteration to take the same branch decisions.
 #include <atomic>
+#include <map>
 #include <mutex>
+#include <unordered_map>
 #include <chrono>
 #include <thread>
 #include <cmath>
@@ -22,6 +24,63 @@
 namespace dv {
 
 static thread_local std::string g_err;
+
+// ---------------------------------------------------------------- buffer pool
+namespace {
+struct PoolKey {
+    int dev;          // -1: pinned host memory
+    size_t bytes;
+    bool operator<(const PoolKey& o) const { return dev != o.dev ? dev < o.dev : bytes < o.bytes; }
+};
+std::mutex g_pool_mu;
+std::map<PoolKey, std::vector<void*>> g_pool_free;
+std::unordered_map<void*, PoolKey> g_pool_live;
+int64_t g_pool_cached = 0;
+
+cudaError_t pool_get(void** p, size_t bytes, bool host) {
+    *p = nullptr;
+    int dev = -1;
+    if (!host) {
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+    }
+    const PoolKey k{dev, bytes};
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        auto it = g_pool_free.find(k);
+        if (it != g_pool_free.end() && !it->second.empty()) {
+            *p = it->second.back();
+            it->second.pop_back();
+            g_pool_cached -= (int64_t)bytes;
+            g_pool_live[*p] = k;
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = host ? cudaMallocHost(p, bytes) : cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return e;
+    }
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    g_pool_live[*p] = k;
+    return cudaSuccess;
+}
+
+void pool_put(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    auto it = g_pool_live.find(p);
+    if (it == g_pool_live.end()) return;       // not pool memory: never happens for handle buffers
+    g_pool_free[it->second].push_back(p);
+    g_pool_cached += (int64_t)it->second.bytes;
+    g_pool_live.erase(it);
+}
+}  // namespace
+
+cudaError_t pool_malloc(void** p, size_t bytes) { return pool_get(p, bytes, false); }
+cudaError_t pool_malloc_host(void** p, size_t bytes) { return pool_get(p, bytes, true); }
+void pool_free(void* p) { pool_put(p); }
+void pool_free_host(void* p) { pool_put(p); }
 
 bool pdl_enabled() {
     static int v = -1;
@@ -507,16 +566,16 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles) {
     W.n = n;
     W.kdim = kdim;
     W.nparts = 1024;
-    auto A = [&](double** p, int64_t cnt) { return cudaMalloc((void**)p, sizeof(double) * (size_t)cnt); };
+    auto A = [&](double** p, int64_t cnt) { return pool_malloc((void**)p, sizeof(double) * (size_t)cnt); };
     if (A(&W.V, (kdim + 1) * n) || A(&W.w, n) || A(&W.u, n) || A(&W.x, n) || A(&W.r, n) || A(&W.b, n) ||
         A(&W.s, n) || A(&W.z, n) || A(&W.f, n) || A(&W.R, n) || A(&W.dz, n) || A(&W.zt, n) || A(&W.ft, n) ||
         A(&W.Rt, n) || A(&W.tmp, n) || A(&W.best, n) || A(&W.part, (int64_t)W.nparts * (kdim + 2)) ||
         A(&W.scal, 32) || A(&W.hbuf, 4 * (kdim + 2)) || A(&W.ybuf, kdim + 2) || A(&W.J, jac_doubles) ||
-        A(&W.vin, n) || A(&W.wout, n) || A(&W.apart, 4096) || cudaMalloc(&W.gm, gm_state_bytes()) != cudaSuccess ||
-        cudaMalloc((void**)&W.tickets, 16 * sizeof(unsigned)) != cudaSuccess)
+        A(&W.vin, n) || A(&W.wout, n) || A(&W.apart, 4096) || pool_malloc(&W.gm, gm_state_bytes()) != cudaSuccess ||
+        pool_malloc((void**)&W.tickets, 16 * sizeof(unsigned)) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMalloc(Krylov workspace)");
-    if (cudaMallocHost(&W.gm_host, 256) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaMallocHost");
-    if (cudaMallocHost((void**)&W.hpin, sizeof(double) * 4 * (kdim + 8)) != cudaSuccess)
+    if (pool_malloc_host(&W.gm_host, 256) != cudaSuccess) return cuda_fail(cudaGetLastError(), "cudaMallocHost");
+    if (pool_malloc_host((void**)&W.hpin, sizeof(double) * 4 * (kdim + 8)) != cudaSuccess)
         return cuda_fail(cudaGetLastError(), "cudaMallocHost");
     {
         const size_t d = sizeof(double);
@@ -543,12 +602,11 @@ void work_free(Work& W) {
     if (W.gm_cs) cudaStreamDestroy(W.gm_cs);
     double* ptrs[] = {W.V, W.w, W.u, W.x, W.r, W.b, W.s, W.z, W.f, W.R, W.dz, W.zt, W.ft, W.Rt, W.tmp, W.best,
                       W.part, W.scal, W.hbuf, W.ybuf, W.J, W.vin, W.wout, W.apart};
-    for (double* p : ptrs)
-        if (p) cudaFree(p);
-    if (W.gm) cudaFree(W.gm);
-    if (W.tickets) cudaFree(W.tickets);
-    if (W.hpin) cudaFreeHost(W.hpin);
-    if (W.gm_host) cudaFreeHost(W.gm_host);
+    for (double* p : ptrs) pool_free(p);
+    pool_free(W.gm);
+    pool_free(W.tickets);
+    pool_free_host(W.hpin);
+    pool_free_host(W.gm_host);
     W = Work();
 }
 
@@ -2422,6 +2480,29 @@ int dv_profile_read(int32_t kind, int64_t* launches, int64_t* timed, double* tot
 int64_t dv_launch_count(void) { return g_launches.load(); }
 size_t dv_step_params_size(void) { return sizeof(dv_step_params); }
 
+int64_t dv_pool_cached_bytes(void) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    return g_pool_cached;
+}
+
+int dv_pool_release(void) {
+    std::lock_guard<std::recursive_mutex> lk_(capture_mutex());
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (auto& kv : g_pool_free) {
+        if (kv.first.dev >= 0) cudaSetDevice(kv.first.dev);
+        for (void* q : kv.second) {
+            if (kv.first.dev < 0) cudaFreeHost(q);
+            else cudaFree(q);
+        }
+    }
+    cudaSetDevice(cur);
+    g_pool_free.clear();
+    g_pool_cached = 0;
+    return launch_ok("dv_pool_release");
+}
+
 size_t dv_struct_size(const char* name) {
     if (!name) return 0;
     const std::string n(name);
@@ -2460,8 +2541,8 @@ int dv_model_destroy(dv_model* m) {
     if (!m) return DV_OK;
     void* ptrs[] = {m->d_aux, m->d_rec, m->d_split, m->d_diag, m->d_acc, m->d_pc, m->d_pc32, m->d_J32, m->d_pc_work, m->d_pc_piv, m->d_pc_info, m->d_atol7,
                     m->d_err};
-    for (void* q : ptrs)
-        if (q) cudaFree(q);
+    cudaDeviceSynchronize();              // no work in flight still uses the buffers the pool keeps
+    for (void* q : ptrs) pool_free(q);
     if (m->W) {
         work_free(*m->W);
         delete m->W;
@@ -2509,19 +2590,19 @@ int dv_model_create(const dv_step_params* p, const double* feed_flux, const doub
     int64_t work_need = precond_work_doubles(m->pc_cap_nb, m->pc_cap_parts, p->Nz);
     m->pc_doubles = pc_need;
     const int64_t rec_n = std::max<int64_t>(m->rl.total, m->n);
-    bool fail = cudaMalloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_split, sizeof(double) * split_doubles(*p)) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_diag, sizeof(double) * m->rl.total) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_pc32, sizeof(float) * pc_need) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_J32, sizeof(float) * m->jac_doubles) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_atol7, sizeof(double) * DV_NB) != cudaSuccess ||
-                cudaMalloc((void**)&m->d_err, sizeof(int)) != cudaSuccess;
+    bool fail = pool_malloc((void**)&m->d_aux, sizeof(double) * (2 * nf + nwall)) != cudaSuccess ||
+                pool_malloc((void**)&m->d_rec, sizeof(double) * rec_n) != cudaSuccess ||
+                pool_malloc((void**)&m->d_split, sizeof(double) * split_doubles(*p)) != cudaSuccess ||
+                pool_malloc((void**)&m->d_diag, sizeof(double) * m->rl.total) != cudaSuccess ||
+                pool_malloc((void**)&m->d_acc, sizeof(double) * DV_NACC) != cudaSuccess ||
+                pool_malloc((void**)&m->d_pc, sizeof(double) * pc_need) != cudaSuccess ||
+                pool_malloc((void**)&m->d_pc32, sizeof(float) * pc_need) != cudaSuccess ||
+                pool_malloc((void**)&m->d_J32, sizeof(float) * m->jac_doubles) != cudaSuccess ||
+                pool_malloc((void**)&m->d_pc_work, sizeof(double) * work_need) != cudaSuccess ||
+                pool_malloc((void**)&m->d_pc_piv, sizeof(int) * (size_t)m->pc_cap_parts * m->pc_cap_nb) != cudaSuccess ||
+                pool_malloc((void**)&m->d_pc_info, sizeof(int) * (size_t)m->pc_cap_parts) != cudaSuccess ||
+                pool_malloc((void**)&m->d_atol7, sizeof(double) * DV_NB) != cudaSuccess ||
+                pool_malloc((void**)&m->d_err, sizeof(int)) != cudaSuccess;
     if (fail) {
         int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(model workspace)");
         dv_model_destroy(m);
@@ -2666,12 +2747,12 @@ int dv_integrator_destroy(dv_integrator* g) {
     if (!g) return DV_OK;
     double* ptrs[] = {g->y, g->fn, g->slope, g->z1, g->z2, g->f1, g->f2, g->rhs1, g->rhs2, g->pred, g->ev, g->es, g->d_g,
                       g->yprev, g->zext};
-    for (double* q : ptrs)
-        if (q) cudaFree(q);
-    if (g->d_pick) cudaFree(g->d_pick);
-    if (g->h_pick) cudaFreeHost(g->h_pick);
-    if (g->h_g) cudaFreeHost(g->h_g);
-    if (g->h_err) cudaFreeHost(g->h_err);
+    cudaDeviceSynchronize();              // no work in flight still uses the buffers the pool keeps
+    for (double* q : ptrs) pool_free(q);
+    pool_free(g->d_pick);
+    pool_free_host(g->h_pick);
+    pool_free_host(g->h_g);
+    pool_free_host(g->h_err);
     delete g;
     return DV_OK;
 }
@@ -2701,15 +2782,15 @@ int dv_integrator_create(dv_model* m, const dv_solver_opts* o, dv_integrator** o
     }
     double** vecs[] = {&g->y, &g->fn, &g->slope, &g->z1, &g->z2, &g->f1, &g->f2, &g->rhs1, &g->rhs2, &g->pred, &g->ev, &g->es};
     for (double** v : vecs) {
-        if (cudaMalloc((void**)v, sizeof(double) * g->n) != cudaSuccess) {
+        if (pool_malloc((void**)v, sizeof(double) * g->n) != cudaSuccess) {
             int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(integrator)");
             dv_integrator_destroy(g);
             return rc;
         }
     }
-    if (cudaMalloc((void**)&g->d_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
-        cudaMallocHost((void**)&g->h_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
-        cudaMallocHost((void**)&g->h_err, sizeof(int)) != cudaSuccess) {
+    if (pool_malloc((void**)&g->d_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
+        pool_malloc_host((void**)&g->h_g, sizeof(double) * 3 * DV_NACC) != cudaSuccess ||
+        pool_malloc_host((void**)&g->h_err, sizeof(int)) != cudaSuccess) {
         int rc = cuda_fail(cudaGetLastError(), "cudaMalloc(integrator)");
         dv_integrator_destroy(g);
         return rc;
@@ -2771,10 +2852,10 @@ int dv_integrator_set_predictor(dv_integrator* g, dv_mlp* net, int32_t predict, 
     }
     DV_TRY(dv_mlp_reserve(net, g->m->nc));
     if (!g->yprev) {
-        if (cudaMalloc((void**)&g->yprev, sizeof(double) * g->n) != cudaSuccess ||
-            cudaMalloc((void**)&g->zext, sizeof(double) * g->n) != cudaSuccess ||
-            cudaMalloc((void**)&g->d_pick, 2 * sizeof(int64_t)) != cudaSuccess ||
-            cudaMallocHost((void**)&g->h_pick, 2 * sizeof(int64_t)) != cudaSuccess)
+        if (pool_malloc((void**)&g->yprev, sizeof(double) * g->n) != cudaSuccess ||
+            pool_malloc((void**)&g->zext, sizeof(double) * g->n) != cudaSuccess ||
+            pool_malloc((void**)&g->d_pick, 2 * sizeof(int64_t)) != cudaSuccess ||
+            pool_malloc_host((void**)&g->h_pick, 2 * sizeof(int64_t)) != cudaSuccess)
             return cuda_fail(cudaGetLastError(), "cudaMalloc(predictor)");
         DV_CUDA(cudaMemset(g->d_pick, 0, 2 * sizeof(int64_t)));
         g->h_pick[0] = g->h_pick[1] = 0;

@@ -74,33 +74,49 @@ def block_pattern(Nr, Nth, Nz, wall):
     return B, R.astype(np.int32), indptr.astype(np.int32), n
 
 
+@lru_cache(maxsize=16)
+def _colouring(Nr, Nth, Nz, wall):
+    c, nc = colour_columns(Nr, Nth, Nz, wall)
+    c.setflags(write=False)
+    return c, nc
+
+
+@lru_cache(maxsize=16)
+def _pattern_views(Nr, Nth, Nz, wall, cut):
+    """Boolean pattern matrix, entry columns and the theta-block reduction (core/jacobian.py:50-69:
+    same sector, or both in the innermost `cut + 1` rings) of a grid shape, built once per shape
+    (the reference's runner builds one Jacobian per cycle step)."""
+    _, indices, indptr, n = block_pattern(Nr, Nth, Nz, wall)
+    P = sp.csc_matrix((np.ones(len(indices), dtype=bool), indices, indptr), shape=(n, n))
+    entry_col = np.repeat(np.arange(n), np.diff(indptr))
+    nc = Nr * Nth * Nz
+    idx = np.arange(n)
+    cellpart = idx < DV_NV * nc
+    sector = np.where(cellpart, ((idx % nc) // Nz) % Nth, (idx - DV_NV * nc) // max(Nz, 1))
+    ring = np.where(cellpart, (idx % nc) // (Nth * Nz), Nr - 1)
+    er, ec = indices, entry_col
+    keep = (sector[er] == sector[ec]) | ((ring[er] <= cut) & (ring[ec] <= cut))
+    keep_theta = np.where(keep)[0]
+    red_indptr = np.concatenate([[0], np.cumsum(np.bincount(ec[keep_theta], minlength=n))])
+    for a in (entry_col, keep_theta, red_indptr):
+        a.setflags(write=False)
+    return P, entry_col, keep_theta, er[keep_theta], red_indptr
+
+
 class FDJacobian:
     """Coloured forward-difference Jacobian of a GPU TVSAModel."""
 
     def __init__(self, model):
         g = model.grid
+        wall = model.n_w > 0
         self.model = model
-        self.color, self.ngroups = colour_columns(g.Nr, g.Nth, g.Nz, model.n_w > 0)
-        self._blk, self.indices, self.indptr, self.n = block_pattern(g.Nr, g.Nth, g.Nz, model.n_w > 0)
-        self.P = sp.csc_matrix((np.ones(len(self.indices), dtype=bool), self.indices, self.indptr),
-                               shape=(self.n, self.n))
-        self.entry_col = np.repeat(np.arange(self.n), np.diff(self.indptr))
+        self.color, self.ngroups = _colouring(g.Nr, g.Nth, g.Nz, wall)
+        self._blk, self.indices, self.indptr, self.n = block_pattern(g.Nr, g.Nth, g.Nz, wall)
         self.entry_row = self.indices
         self.nevals = 0
         self._J = None
-        # theta-block reduction (core/jacobian.py:50-69): same sector, or both in the inner rings
-        n = g.ncell
-        nv = DV_NV
-        idx = np.arange(self.n)
-        cellpart = idx < nv * n
-        sector = np.where(cellpart, ((idx % n) // g.Nz) % g.Nth, (idx - nv * n) // max(g.Nz, 1))
-        ring = np.where(cellpart, (idx % n) // (g.Nth * g.Nz), g.Nr - 1)
-        cut = model.cfg.solver.precond_theta_rings - 1
-        er, ec = self.entry_row, self.entry_col
-        keep = (sector[er] == sector[ec]) | ((ring[er] <= cut) & (ring[ec] <= cut))
-        self.keep_theta = np.where(keep)[0]
-        self.red_indices = er[self.keep_theta]
-        self.red_indptr = np.concatenate([[0], np.cumsum(np.bincount(ec[self.keep_theta], minlength=self.n))])
+        (self.P, self.entry_col, self.keep_theta, self.red_indices,
+         self.red_indptr) = _pattern_views(g.Nr, g.Nth, g.Nz, wall, model.cfg.solver.precond_theta_rings - 1)
 
     def block(self, t, y, f0=None):
         """J on the device in the block layout (float64 tensor of jac_doubles)."""

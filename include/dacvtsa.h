@@ -126,6 +126,12 @@ size_t dv_step_params_size(void);
 /* sizeof of the ABI's other structs, by name ("dv_newton_opts", "dv_newton_result", "dv_solver_opts",
  * "dv_step_report", "dv_tuning"); 0 for an unknown name.  Lets a binding check its mirrors. */
 size_t dv_struct_size(const char* name);
+/* No reference counterpart.  The device and pinned host memory of destroyed models and integrators
+ * is kept by the library and handed to the next handle of the same sizes (the reference creates one
+ * model and one integrator per cycle step).  dv_pool_cached_bytes: bytes kept now; dv_pool_release:
+ * frees them all (handles alive are not affected). */
+int64_t dv_pool_cached_bytes(void);
+int dv_pool_release(void);
 const char* dv_last_error(void);
 int dv_device_count(int* n);
 
