@@ -1150,6 +1150,9 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
     const int lane = tid % PA_LANES;
     const int grp = tid / PA_LANES;            // 8 lanes per group, two rows per group: r0 and r0 + rh
     const int rh = (nb + 1) >> 1;
+    // the thread that issues the ring's refills: the first of the last warp when that warp has no
+    // rows (nb <= 56), so the copy issue is off the row warps' path to the next barrier
+    const int issuer = (rh <= PA_THREADS / PA_LANES - 32 / PA_LANES) ? PA_THREADS - 32 : 0;
     const int r0 = grp, r1 = grp + rh;
     const bool act0 = r0 < rh, act1 = act0 && r1 < nb;
     int issued = (S < NBUF) ? S : NBUF;        // stages whose copies have been issued
@@ -1196,7 +1199,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             return false;
         }
         if (s >= 1 && s - 1 + NBUF < S) {        // the previous stage's buffer is free: refill it
-            if (tid == 0) {
+            if (tid == issuer) {
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 issue(s - 1 + NBUF, smem_u32(buf0 + (int64_t)pb * 3 * bs), smem_u32(&bars[pb]));
             }
