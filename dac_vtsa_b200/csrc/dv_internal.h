@@ -103,6 +103,32 @@ int work_alloc(Work& W, int64_t n, int kdim, int64_t jac_doubles);
 // without the attribute.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Grid-wide barrier of a cooperative launch: one thread per block arrives on *cnt, the last one
+// resets it and advances *gen; the others poll *gen at most `limit` times and then set bit 4 of
+// *err and go on (the host reports the error; no thread waits forever).
+__device__ __forceinline__ void grid_sync_bounded(unsigned* cnt, unsigned* gen, int* err, int limit = 1 << 24) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vg = gen;
+        const unsigned g0 = *vg;
+        __threadfence();
+        if (atomicAdd(cnt, 1u) == gridDim.x - 1) {
+            *cnt = 0u;
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            for (int it = 0; *vg == g0; ++it) {
+                if (it > limit) {
+                    atomicOr(err, 4);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
 // sum of p[b * stride], b < nb, in index order: the deterministic finish of per-block partials
 // written by other SMs (volatile loads: never served from this SM's L1)
 __device__ __forceinline__ double sum_partials(const double* p, int nb, int64_t stride) {
@@ -222,6 +248,9 @@ int selftest_mbar_timeout(int polls, int* err, cudaStream_t s);
 int precond_apply_capture(dv_model* m, const double* b, const double* sc, double* x, cudaStream_t s,
                           const PaFuse& F = PaFuse());
 // FD matvec of the split residual for stream capture: t and gh are read from dargs[0..1] (device).
+// With `bar` (two zeroed barrier words) the three phases run as one cooperative launch.
 int matvec_capture(dv_model* m, const double* dargs, const double* z, const double* u, const double* sc,
-                   const double* f0, const double* scal, double* out, cudaStream_t s);
+                   const double* f0, const double* scal, double* out, cudaStream_t s, unsigned* bar = nullptr);
+// Kernels one matvec_capture with `bar` launched (1 cooperative, or the 3 of the split residual).
+int matvec_capture_kernels();
 }  // namespace dv

@@ -3,6 +3,7 @@
 #include "dv_internal.h"
 #include "dv_residual.cuh"
 
+#include <algorithm>
 #include <mutex>
 #include <utility>
 
@@ -336,14 +337,13 @@ static __device__ __forceinline__ double matvec_sig(const double* scal) {
 // Two warps per 32 cells: warp 0 evaluates the transport properties of its cells, warp 1 the
 // temperature, isotherms and LDF rates of the same cells (the two halves of the per-cell chain run
 // side by side; uptake reads only the clipped temperature of the properties).
+// The work of one 64-thread block `vb` (cells vb*32 .. vb*32 + 31).
 template <int MODE>
-__global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
-                                               const double* __restrict__ u, const double* __restrict__ sc,
-                                               const double* __restrict__ scal) {
-    pdl_wait();                             // (launched programmatically inside the GMRES graph)
-    pdl_trigger();
+__device__ __forceinline__ void cprops_block(const dv_step_params& p, const Split& S, const double* __restrict__ y,
+                                             const double* __restrict__ u, const double* __restrict__ sc,
+                                             const double* __restrict__ scal, int64_t vb) {
     const int64_t nc = S.nc;
-    const int64_t c = (int64_t)blockIdx.x * 32 + (threadIdx.x & 31);
+    const int64_t c = vb * 32 + (threadIdx.x & 31);
     const bool half = (threadIdx.x >> 5) != 0;             // warp-uniform
     if (c >= nc) return;
     Cell s;
@@ -386,6 +386,15 @@ __global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const 
     }
 }
 
+template <int MODE>
+__global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
+                                               const double* __restrict__ u, const double* __restrict__ sc,
+                                               const double* __restrict__ scal) {
+    pdl_wait();                             // (launched programmatically inside the GMRES graph)
+    pdl_trigger();
+    cprops_block<MODE>(p, S, y, u, sc, scal, blockIdx.x);
+}
+
 // MUSCL slope of cell kk of a column starting at cell index base (zero next to the ends).
 static __device__ __forceinline__ void sp_slope(const dv_step_params& p, const Split& S, int64_t base, int kk,
                                                 bool muscl, double s[4]) {
@@ -404,11 +413,11 @@ static __device__ __forceinline__ void sp_slope(const dv_step_params& p, const S
 
 // One thread per face: interior z faces, r faces, theta faces, then the two end faces of every
 // column (kept last so the warps of each range run one kind of face).
+// The face of index g (all kinds in the order above).
 template <bool REC>
-__global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S, Rec rec, double t,
-                                              const double* __restrict__ scal, const double* __restrict__ dargs) {
-    pdl_wait();
-    pdl_trigger();
+__device__ __forceinline__ void faces_at(const dv_step_params& p, const Aux& aux, const Split& S, const Rec& rec,
+                                         double t, const double* __restrict__ scal,
+                                         const double* __restrict__ dargs, int64_t g) {
     if (scal && scal[0] == 0.0) return;
     if (dargs) t = dargs[0];
     const int Nr = p.Nr, Nth = p.Nth, Nz = p.Nz;
@@ -416,7 +425,6 @@ __global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S
     const int64_t nzi = ncol * (Nz - 1);
     const int64_t nr = (Nr > 1) ? S.nrf : 0;
     const int64_t nt = (Nth > 1) ? S.ntf : 0;
-    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g < nzi) {
         const int64_t col = g / (Nz - 1);
         const int k = (int)(g % (Nz - 1));
@@ -489,15 +497,22 @@ __global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S
     }
 }
 
-template <int MODE, bool REC>
-__global__ void __launch_bounds__(64) k_assemble(dv_step_params p, Aux aux, Split S, Rec rec, double t,
-                                                 const double* __restrict__ y, const double* __restrict__ u,
-                                                 const double* __restrict__ sc, const double* __restrict__ f0,
-                                                 const double* __restrict__ scal, double gh,
-                                                 double* __restrict__ out, const double* __restrict__ dargs) {
+template <bool REC>
+__global__ void __launch_bounds__(64) k_faces(dv_step_params p, Aux aux, Split S, Rec rec, double t,
+                                              const double* __restrict__ scal, const double* __restrict__ dargs) {
     pdl_wait();
+    pdl_trigger();
+    faces_at<REC>(p, aux, S, rec, t, scal, dargs, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The assembly of cell c.
+template <int MODE, bool REC>
+__device__ __forceinline__ void assemble_at(const dv_step_params& p, const Aux& aux, const Split& S, const Rec& rec,
+                                            double t, const double* __restrict__ y, const double* __restrict__ u,
+                                            const double* __restrict__ sc, const double* __restrict__ f0,
+                                            const double* __restrict__ scal, double gh, double* __restrict__ out,
+                                            const double* __restrict__ dargs, int64_t c) {
     const int64_t nc = S.nc;
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= nc) return;
     if (dargs) {                  // launched from a CUDA graph: time and step factor live on the device
         t = dargs[0];
@@ -571,6 +586,37 @@ __global__ void __launch_bounds__(64) k_assemble(dv_step_params p, Aux aux, Spli
     }
 }
 
+template <int MODE, bool REC>
+__global__ void __launch_bounds__(64) k_assemble(dv_step_params p, Aux aux, Split S, Rec rec, double t,
+                                                 const double* __restrict__ y, const double* __restrict__ u,
+                                                 const double* __restrict__ sc, const double* __restrict__ f0,
+                                                 const double* __restrict__ scal, double gh,
+                                                 double* __restrict__ out, const double* __restrict__ dargs) {
+    pdl_wait();
+    assemble_at<MODE, REC>(p, aux, S, rec, t, y, u, sc, f0, scal, gh, out, dargs,
+                           (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The FD matvec of the GMRES graph in one cooperative launch: the blocks of k_cprops, k_faces and
+// k_assemble (the same per-block / per-index code, in the same 64-thread blocks) taken in grid-
+// stride order, the three phases separated by two bounded grid barriers (bar[0..1]; bit 4 of *err
+// on a timeout).  Saves two kernel boundaries per Arnoldi step; results are bit-identical.
+__global__ void __launch_bounds__(64) k_matvec_coop(dv_step_params p, Aux aux, Split S, Rec rec,
+                                                    const double* __restrict__ z, const double* __restrict__ u,
+                                                    const double* __restrict__ sc, const double* __restrict__ f0,
+                                                    const double* __restrict__ scal, double* __restrict__ out,
+                                                    const double* __restrict__ dargs, unsigned* bar, int* err,
+                                                    int64_t nb_props, int64_t nb_faces, int64_t nb_cells) {
+    for (int64_t vb = blockIdx.x; vb < nb_props; vb += gridDim.x)
+        cprops_block<M_MATVEC>(p, S, z, u, sc, scal, vb);
+    grid_sync_bounded(bar, bar + 1, err);
+    for (int64_t vb = blockIdx.x; vb < nb_faces; vb += gridDim.x)
+        faces_at<false>(p, aux, S, rec, 0.0, scal, dargs, vb * 64 + threadIdx.x);
+    grid_sync_bounded(bar, bar + 1, err);
+    for (int64_t vb = blockIdx.x; vb < nb_cells; vb += gridDim.x)
+        assemble_at<M_MATVEC, false>(p, aux, S, rec, 0.0, z, u, sc, f0, scal, 0.0, out, dargs, vb * 64 + threadIdx.x);
+}
+
 static Aux aux_of(const dv_model* m) { return Aux{m->aux.feed_flux, m->aux.n_nom, m->aux.cov}; }
 
 static unsigned nblk(int64_t n, int b) { return (unsigned)((n + b - 1) / b); }
@@ -641,13 +687,57 @@ static cudaError_t launch_pdl(void (*kern)(KArgs...), unsigned grid, unsigned bl
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+// co-resident 64-thread blocks of k_matvec_coop (-1: not asked yet; 0: refused)
+static int g_matvec_coop_cap = -1;
+
+// DVTSA_MATVEC_COOP=1 runs the FD matvec inside the GMRES graph as one cooperative launch (read
+// once; off by default: bit-identical, but measured 5 % slower on the 8x8x32 heating window, the
+// two grid barriers costing more than the two kernel boundaries they replace).
+static bool matvec_coop_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("DVTSA_MATVEC_COOP");
+        v = (e && e[0] == '1') ? 1 : 0;
+    }
+    return v == 1;
+}
+
+int matvec_capture_kernels() { return (g_matvec_coop_cap > 0 && matvec_coop_enabled()) ? 1 : 3; }
+
 int matvec_capture(dv_model* m, const double* dargs, const double* z, const double* u, const double* sc,
-                   const double* f0, const double* scal, double* out, cudaStream_t s) {
+                   const double* f0, const double* scal, double* out, cudaStream_t s, unsigned* bar) {
     const dv_step_params& p = m->p;
     const Split S = split_of(p, m->d_split);
     const Rec rec = make_rec(m->rl, m->d_rec);
     const int64_t ncol = (int64_t)p.Nr * p.Nth;
     const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
+    int& coop_cap = g_matvec_coop_cap;
+    if (coop_cap < 0) {
+        int dev = 0, nsm = 0, bps = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_matvec_coop, 64, 0) != cudaSuccess) bps = 0;
+        coop_cap = bps * nsm;
+        cudaGetLastError();
+    }
+    if (bar && coop_cap > 0 && matvec_coop_enabled()) {
+        const int64_t nbp = nblk(m->nc, 32), nbf = nblk(nfaces, 64), nbc = nblk(m->nc, 64);
+        const int64_t want = std::max(nbp, std::max(nbf, nbc));
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)std::min<int64_t>(want, coop_cap));
+        cfg.blockDim = dim3(64);
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (cudaLaunchKernelEx(&cfg, k_matvec_coop, p, aux_of(m), S, rec, z, u, sc, f0, scal, out, dargs, bar,
+                               m->d_err, nbp, nbf, nbc) == cudaSuccess)
+            return DV_OK;
+        cudaGetLastError();                   // a driver that refuses the cooperative node: three kernels
+        coop_cap = 0;
+    }
     if (pdl_enabled()) {       // each kernel may start while its predecessor drains (pdl_wait in the kernel)
         DV_CUDA(launch_pdl(k_cprops<M_MATVEC>, nblk(m->nc, 32), 64, s, p, S, z, u, sc, scal));
         DV_CUDA(launch_pdl(k_faces<false>, nblk(nfaces, 64), 64, s, p, aux_of(m), S, rec, 0.0, scal, dargs));

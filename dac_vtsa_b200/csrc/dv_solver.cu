@@ -793,7 +793,7 @@ static int check_device_error(dv_model* m);
 static void clear_device_error(dv_model* m);
 
 // the model's device error word: bit 1 a preconditioner sweep's bulk-copy wait timed out, bit 4 a
-// grid barrier of the cooperative Gram-Schmidt kernel timed out
+// grid barrier of a cooperative kernel (Gram-Schmidt, the FD matvec) timed out
 static const char* device_error_text(int e) {
     if (e & 32) return "a preconditioner index fell outside its storage (the access was skipped)";
     if (e & 1) return "a bounded device wait (preconditioner bulk copy) timed out";
@@ -1089,32 +1089,7 @@ __global__ void __launch_bounds__(VB) k_cgs_orth_norm(int64_t n, GmDev* st, cons
     }
 }
 
-// ---- CGS2 of one Arnoldi step in a single cooperative launch
-// Barrier of a cooperative launch (all blocks co-resident): arrival counter + generation word in
-// global memory.  The wait is bounded: after ~2^24 polls the kernel records bit 4 in *err and
-// carries on (the step's results are then void, and the host sees the error).
-__device__ __forceinline__ void grid_sync_bounded(unsigned* cnt, unsigned* gen, int* err, int limit = 1 << 24) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* vg = gen;
-        const unsigned g0 = *vg;
-        __threadfence();
-        if (atomicAdd(cnt, 1u) == gridDim.x - 1) {
-            *cnt = 0u;
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            for (int it = 0; *vg == g0; ++it) {
-                if (it > limit) {
-                    atomicOr(err, 4);
-                    break;
-                }
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-}
+// ---- CGS2 of one Arnoldi step in a single cooperative launch (grid_sync_bounded: dv_internal.h)
 
 // this block's sums of the first cnt entries of acc into part[blockIdx.x * GM_PS + q]
 __device__ __forceinline__ void gm_store_partials(const double (&acc)[GM_KMAX + 1], int cnt, double* part) {
@@ -1316,11 +1291,11 @@ static bool gmres_coop_enabled() {
 // kernels) or, with the mixed-precision operator, one FP32 assembled-Jacobian product.
 static int op_capture(dv_model* m, Work& W, const double* dargs, double* out, cudaStream_t c) {
     if (m->op32) return launch_spmv32(m, W.u, W.s, 0.0, dargs, out, c, false);
-    return matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, out, c);
+    return matvec_capture(m, dargs, W.z, W.u, W.s, W.f, W.scal, out, c, W.tickets + 11);
 }
 static void op_count(const dv_model* m, int64_t* cnt) {
     if (m->op32) cnt[K_SPMV] += 1;
-    else cnt[K_MATVEC] += 3;
+    else cnt[K_MATVEC] += matvec_capture_kernels();
 }
 
 // A capture that another host thread invalidated (for instance by the first launch of a kernel,

@@ -416,8 +416,8 @@ print(json.dumps({{"y": hashlib.sha256(np.ascontiguousarray(r.y).tobytes()).hexd
 
 def test_gmres_graph_forms_give_identical_results():
     """The GMRES graph's Arnoldi steps ahead of its WHILE node (DVTSA_GMRES_PREFIX), its steps per
-    WHILE pass (DVTSA_GMRES_BODY), its programmatic dependent launches (DVTSA_PDL) and its CGS2 as
-    one cooperative launch (DVTSA_GMRES_COOP) change
+    WHILE pass (DVTSA_GMRES_BODY), its programmatic dependent launches (DVTSA_PDL), its FD matvec
+    (DVTSA_MATVEC_COOP) and its CGS2 as one cooperative launch each (DVTSA_GMRES_COOP) change
     where the same kernels' arithmetic runs, not the arithmetic: a 200 s adsorption of the 4x4x16 bed
     ends in the bit-identical state with the same step and GMRES counts in every form."""
     import os
@@ -428,10 +428,10 @@ def test_gmres_graph_forms_give_identical_results():
     out = {}
     for name, env in {"default": {}, "three_kernel_cgs": {"DVTSA_GMRES_COOP": "0"},
                       "no_prefix": {"DVTSA_GMRES_PREFIX": "0"}, "one_step_body": {"DVTSA_GMRES_BODY": "1"},
-                      "pdl": {"DVTSA_PDL": "1"}}.items():
+                      "pdl": {"DVTSA_PDL": "1"}, "coop_matvec": {"DVTSA_MATVEC_COOP": "1"}}.items():
         e = dict(os.environ, **env)
         r = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True, text=True, timeout=600,
                            cwd=os.path.dirname(tests))
         assert r.returncode == 0, r.stderr[-2000:]
         out[name] = json.loads(r.stdout.strip().splitlines()[-1])
-    assert out["default"] == out["three_kernel_cgs"] == out["no_prefix"] == out["one_step_body"] == out["pdl"], out
+    assert out["default"] == out["three_kernel_cgs"] == out["no_prefix"] == out["one_step_body"] == out["pdl"] == out["coop_matvec"], out
