@@ -386,13 +386,115 @@ __device__ __forceinline__ void cprops_block(const dv_step_params& p, const Spli
     }
 }
 
+// Eight warps per 32 cells.  The transcendental terms of a cell's properties and uptake that do not
+// depend on one another (each power is a called routine, so one thread evaluates them strictly one
+// after another) are spread over the warps of its block, then combined after one barrier:
+//   warp 0: viscosities and the CO2-air Fuller diffusivity     warps 1-3: conductivity of gas 0-2
+//   warp 4: the CO2-water Fuller diffusivity                    warp 5: water saturation and GAB loading
+//   warp 6: the dry CO2 Toth term                               warp 7: the wet CO2 Toth term (wadst)
+// then warp 0 mixes the transport properties and warp 1 finishes the loadings and LDF rates.  Every
+// value is the same expression on the same operands as in cell_props / uptake, so the results are
+// bit-identical to the one-thread-per-cell evaluation.
+#define CP_WARPS 8
+static_assert(DV_NG == 3 && CP_WARPS == 8, "the warp roles assume three gases");
 template <int MODE>
-__global__ void __launch_bounds__(64) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
-                                               const double* __restrict__ u, const double* __restrict__ sc,
-                                               const double* __restrict__ scal) {
+__device__ __forceinline__ void cprops_split(const dv_step_params& p, const Split& S, const double* __restrict__ y,
+                                             const double* __restrict__ u, const double* __restrict__ sc,
+                                             const double* __restrict__ scal, int64_t vb) {
+    __shared__ double xk[DV_NG][32], xdcw[32], xqw[32], xqd[32], xqwet[32];
+    const int64_t nc = S.nc;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t c = vb * 32 + lane;
+    const bool in = c < nc;
+    if (MODE == M_MATVEC && scal[0] == 0.0) return;    // zero direction (grid-uniform): k_assemble writes zeros
+    Cell s;
+    if (in) {
+        if (MODE == M_MATVEC) {
+            LoadDir ld{y, u, sc, matvec_sig(scal)};
+            load_cell(ld, nc, c, s);
+        } else {
+            LoadPlain ld{y};
+            load_cell(ld, nc, c, s);
+        }
+    } else {
+        s = Cell{};
+    }
+    Props o;
+    double ycl[DV_NG];
+    props_state(p, s, o, ycl);
+    const double T = o.Tp, T3 = T / 300.0;
+    const double pp = npmax(s.c[0] * DV_R * o.Tp, 0.0);
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    double mu[DV_NG], sq[DV_NG], D_ca = 0.0;
+    if (w == 0) {
+#pragma unroll
+        for (int s2 = 0; s2 < DV_NG; ++s2) {
+            mu[s2] = gas_mu(p, s2, T);
+            sq[s2] = sqrt(mu[s2]);
+        }
+        D_ca = fuller(p, 0, T, npmax(o.P, 1.0));
+    } else if (w <= DV_NG) {
+        xk[w - 1][lane] = gas_k(p, w - 1, T3);
+    } else if (w == 4) {
+        xdcw[lane] = fuller(p, 1, T, npmax(o.P, 1.0));
+    } else if (w == 5) {
+        xqw[lane] = q_h2o(p, s.c[1] * DV_R * o.Tp, o.Tp, psat_h2o(o.Tp));
+    } else if (w == 6) {
+        xqd[lane] = co2_needs_qw(p) ? nan : co2_toth_dry(p, pp, o.Tp);
+    } else {
+        xqwet[lane] = (p.coads == DV_COADS_WADST) ? co2_toth_wet(p, pp, o.Tp) : nan;
+    }
+    __syncthreads();
+    if (!in || w > 1) return;
+    double* a = S.cell;
+    if (w == 0) {
+        double kk[DV_NG];
+#pragma unroll
+        for (int s2 = 0; s2 < DV_NG; ++s2) kk[s2] = xk[s2][lane];
+        double mu_m, k_m;
+        wilke_mix(p, ycl, mu, kk, sq, mu_m, k_m);
+        o.mu = mu_m;
+        o.kg = k_m;
+        o.rho = o.Cpos * wsum3(p.M, ycl);
+        o.cpm = wsum3(p.cpg, ycl);
+        o.Dm = blanc_Dm(ycl, D_ca, xdcw[lane]);
+        o.lam0 = stagnant(p, o.kg);
+#pragma unroll
+        for (int q = 0; q < DV_NG; ++q) {
+            a[(SP_C0 + q) * nc + c] = s.c[q];
+            a[(SP_Y0 + q) * nc + c] = o.y[q];
+        }
+        a[SP_T * nc + c] = o.T;
+        a[SP_P * nc + c] = o.P;
+        a[SP_CPOS * nc + c] = o.Cpos;
+        a[SP_MU * nc + c] = o.mu;
+        a[SP_KG * nc + c] = o.kg;
+        a[SP_RHO * nc + c] = o.rho;
+        a[SP_CPM * nc + c] = o.cpm;
+        a[SP_DM * nc + c] = o.Dm;
+        a[SP_LAM0 * nc + c] = o.lam0;
+    } else {
+        double rate[DV_NA], qstar[DV_NA];
+        const double qw_eq = xqw[lane];
+        const double basis = p.basis_state ? s.q[1] : qw_eq;
+        qstar[0] = q_co2_raw(p, pp, o.Tp, basis, xqd[lane], xqwet[lane]) * (pp / (pp + p.p_reg));
+        qstar[1] = qw_eq;
+        ldf_rates(p, s, o.Tp, qstar, rate);
+#pragma unroll
+        for (int q = 0; q < DV_NA; ++q) {
+            a[(SP_RATE0 + q) * nc + c] = rate[q];
+            a[(SP_QS0 + q) * nc + c] = qstar[q];
+        }
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(CP_WARPS * 32) k_cprops(dv_step_params p, Split S, const double* __restrict__ y,
+                                                          const double* __restrict__ u, const double* __restrict__ sc,
+                                                          const double* __restrict__ scal) {
     pdl_wait();                             // (launched programmatically inside the GMRES graph)
     pdl_trigger();
-    cprops_block<MODE>(p, S, y, u, sc, scal, blockIdx.x);
+    cprops_split<MODE>(p, S, y, u, sc, scal, blockIdx.x);
 }
 
 // MUSCL slope of cell kk of a column starting at cell index base (zero next to the ends).
@@ -629,7 +731,7 @@ static int split_residual(dv_model* m, const Rec& rec, double t, const double* y
     const Split S = split_of(p, m->d_split);
     const int64_t ncol = (int64_t)p.Nr * p.Nth;
     const int64_t nfaces = ncol * (p.Nz - 1) + (p.Nr > 1 ? S.nrf : 0) + (p.Nth > 1 ? S.ntf : 0) + 2 * ncol;
-    DV_LAUNCH(kind, s, k_cprops<MODE><<<nblk(m->nc, 32), 64, 0, s>>>(p, S, y, u, sc, scal));
+    DV_LAUNCH(kind, s, k_cprops<MODE><<<nblk(m->nc, 32), CP_WARPS * 32, 0, s>>>(p, S, y, u, sc, scal));
     DV_LAUNCH(kind, s, k_faces<REC><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t,
                                                                   MODE == M_MATVEC ? scal : nullptr, nullptr));
     DV_LAUNCH(kind, s, k_assemble<MODE, REC><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, t, y, u, sc, f0,
@@ -739,13 +841,13 @@ int matvec_capture(dv_model* m, const double* dargs, const double* z, const doub
         coop_cap = 0;
     }
     if (pdl_enabled()) {       // each kernel may start while its predecessor drains (pdl_wait in the kernel)
-        DV_CUDA(launch_pdl(k_cprops<M_MATVEC>, nblk(m->nc, 32), 64, s, p, S, z, u, sc, scal));
+        DV_CUDA(launch_pdl(k_cprops<M_MATVEC>, nblk(m->nc, 32), CP_WARPS * 32, s, p, S, z, u, sc, scal));
         DV_CUDA(launch_pdl(k_faces<false>, nblk(nfaces, 64), 64, s, p, aux_of(m), S, rec, 0.0, scal, dargs));
         DV_CUDA(launch_pdl(k_assemble<M_MATVEC, false>, nblk(m->nc, 64), 64, s, p, aux_of(m), S, rec, 0.0, z, u, sc, f0,
                            scal, 0.0, out, dargs));
         return DV_OK;
     }
-    k_cprops<M_MATVEC><<<nblk(m->nc, 32), 64, 0, s>>>(p, S, z, u, sc, scal);
+    k_cprops<M_MATVEC><<<nblk(m->nc, 32), CP_WARPS * 32, 0, s>>>(p, S, z, u, sc, scal);
     k_faces<false><<<nblk(nfaces, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, scal, dargs);
     k_assemble<M_MATVEC, false><<<nblk(m->nc, 64), 64, 0, s>>>(p, aux_of(m), S, rec, 0.0, z, u, sc, f0, scal, 0.0,
                                                              out, dargs);

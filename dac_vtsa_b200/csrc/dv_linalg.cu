@@ -1150,9 +1150,11 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
     const int lane = tid % PA_LANES;
     const int grp = tid / PA_LANES;            // 8 lanes per group, two rows per group: r0 and r0 + rh
     const int rh = (nb + 1) >> 1;
-    // the thread that issues the ring's refills: the first of the last warp when that warp has no
-    // rows (nb <= 56), so the copy issue is off the row warps' path to the next barrier
+    // the thread that issues the ring's refills and the warp that polls the copies' mbarriers: the
+    // last warp when it has no rows (nb <= 56), so neither the copy issue nor the poll is on the row
+    // warps' path to the next barrier
     const int issuer = (rh <= PA_THREADS / PA_LANES - 32 / PA_LANES) ? PA_THREADS - 32 : 0;
+    const int pollw = issuer / 32;
     const int r0 = grp, r1 = grp + rh;
     const bool act0 = r0 < rh, act1 = act0 && r1 < nb;
     int issued = (S < NBUF) ? S : NBUF;        // stages whose copies have been issued
@@ -1181,19 +1183,19 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             acc1 += __shfl_xor_sync(0xffffffffu, acc1, off, PA_LANES);
         }
     };
-    auto put = [&](double* row, double a0, double a1, bool sub) {
+    auto put = [&](double* row, double a0, double a1) {
         if (lane == 0 && act0) {
-            row[r0] = sub ? row[r0] - a0 : a0;
-            if (act1) row[r1] = sub ? row[r1] - a1 : a1;
+            row[r0] = a0;
+            if (act1) row[r1] = a1;
         }
     };
     // One barrier per stage: it publishes the previous stage's rows and frees its buffer, which is
     // refilled right after it.  Forward rows overwrite b_t by z_t in xs (each row reads and writes
-    // only its own entry of plane t); backward rows go to xb, as every row reads all of z_t.  Warp 0
-    // alone polls the copy's mbarrier; the barrier carries its answer to the others.
+    // only its own entry of plane t); backward rows go to xb, as every row reads all of z_t.  Warp
+    // `pollw` alone polls the copy's mbarrier; the barrier carries its answer to the others.
     auto stage = [&](int s) -> bool {
         TS* buf = buf0 + (int64_t)bi * 3 * bs;
-        const bool arrived = (tid < 32) ? mbar_wait(smem_u32(&bars[bi]), par) : true;
+        const bool arrived = ((tid >> 5) == pollw) ? mbar_wait(smem_u32(&bars[bi]), par) : true;
         if (!__syncthreads_and(arrived)) {       // uniform decision: no thread is left at a barrier
             if (tid == 0) atomicOr(err, 1);
             return false;
@@ -1209,12 +1211,21 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         double a0 = 0.0, a1 = 0.0;
         if (s < n - 1) {                                       // F(t)
             const int t = s + 1;
+            double* row = xs + (int64_t)t * LD;
+            double b0 = 0.0, b1 = 0.0;                         // this plane's b, read ahead of the products
+            if (lane == 0 && act0) {
+                b0 = row[r0];
+                if (act1) b1 = row[r1];
+            }
             if (act0) {
                 dot2(buf + oL1, xs + (int64_t)(t - 1) * LD, a0, a1);
                 if (t >= 2) dot2(buf + oL2, xs + (int64_t)(t - 2) * LD, a0, a1);
             }
             reduce(a0, a1);
-            put(xs + (int64_t)t * LD, a0, a1, true);
+            if (lane == 0 && act0) {
+                row[r0] = b0 - a0;
+                if (act1) row[r1] = b1 - a1;
+            }
         } else if (TW && s == n - 1) {                         // X: partial right-hand sides of the separator
             if (act0) {
                 dot2(buf + oL1, xs + (int64_t)(n - 1) * LD, a0, a1);
@@ -1240,7 +1251,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
                 dot2(buf + bs, xs + (int64_t)(2 * n + 1 - lz0) * LD, a0, a1);
             }
             reduce(a0, a1);
-            put(xb + (int64_t)t * LD, a0, a1, false);
+            put(xb + (int64_t)t * LD, a0, a1);
         } else {                                               // B(t)
             const int t = TW ? n - 1 - (s - (n + 2)) : Nz - 1 - (s - (Nz - 1));
             const int lim = TW ? n + 2 : Nz;
@@ -1251,7 +1262,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
                 if (t + 2 < lim) dot2(buf + oW2, xb + (int64_t)(t + 2) * LD, a0, a1);
             }
             reduce(a0, a1);
-            put(xb + (int64_t)t * LD, a0, a1, false);
+            put(xb + (int64_t)t * LD, a0, a1);
         }
         pb = bi;
         if (++bi == NBUF) {

@@ -85,31 +85,36 @@ static __device__ __forceinline__ double stagnant(const dv_step_params& p, doubl
     return lam_g * (1.0 - s + s * kc);
 }
 
-static __device__ void cell_props(const dv_step_params& p, const Cell& s, Props& o) {
+// The state part of the cell properties: T, P, clipped T, positive total concentration, mole
+// fractions and their clipped copies.
+static __device__ __forceinline__ void props_state(const dv_step_params& p, const Cell& s, Props& o, double ycl[DV_NG]) {
     double Ctot = s.c[0] + s.c[1] + s.c[2];
     o.T = cell_T(p, s);
     o.P = Ctot * DV_R * o.T;
     o.Tp = npclip(o.T, 150.0, 1500.0);
     o.Cpos = npmax(Ctot, 1e-9);
-    double ycl[DV_NG];
 #pragma unroll
     for (int k = 0; k < DV_NG; ++k) {
         o.y[k] = s.c[k] / o.Cpos;
         ycl[k] = npclip(o.y[k], 0.0, 1.0);
     }
-    // pure-gas viscosity / conductivity, Wilke & Mason-Saxena mixing (ideal_gas_backend.py:94-113,148-166)
-    const double T = o.Tp;
-    double mu[DV_NG], kk[DV_NG], sq[DV_NG];
-    const double T3 = T / 300.0;
-#pragma unroll
-    for (int s2 = 0; s2 < DV_NG; ++s2) {
-        if (p.mu_nt[s2] == 1) mu[s2] = p.mu_D[s2][0] * T + p.mu_E[s2][0];
-        else mu[s2] = p.mu_w[s2][0] * (p.mu_D[s2][0] * T + p.mu_E[s2][0]) + p.mu_w[s2][1] * (p.mu_D[s2][1] * T + p.mu_E[s2][1]);
-        if (p.k_nt[s2] == 1) kk[s2] = p.k_0[s2][0] * pow(T3, p.k_n[s2][0]);
-        else kk[s2] = p.k_w[s2][0] * p.k_0[s2][0] * pow(T3, p.k_n[s2][0]) + p.k_w[s2][1] * p.k_0[s2][1] * pow(T3, p.k_n[s2][1]);
-        sq[s2] = sqrt(mu[s2]);
-    }
-    double mu_m = 0.0, k_m = 0.0;
+}
+
+// pure-gas viscosity and conductivity of gas s2 (ideal_gas_backend.py:94-113,148-166); T3 = T / 300
+static __device__ __forceinline__ double gas_mu(const dv_step_params& p, int s2, double T) {
+    if (p.mu_nt[s2] == 1) return p.mu_D[s2][0] * T + p.mu_E[s2][0];
+    return p.mu_w[s2][0] * (p.mu_D[s2][0] * T + p.mu_E[s2][0]) + p.mu_w[s2][1] * (p.mu_D[s2][1] * T + p.mu_E[s2][1]);
+}
+static __device__ __forceinline__ double gas_k(const dv_step_params& p, int s2, double T3) {
+    if (p.k_nt[s2] == 1) return p.k_0[s2][0] * pow(T3, p.k_n[s2][0]);
+    return p.k_w[s2][0] * p.k_0[s2][0] * pow(T3, p.k_n[s2][0]) + p.k_w[s2][1] * p.k_0[s2][1] * pow(T3, p.k_n[s2][1]);
+}
+
+// Wilke & Mason-Saxena mixing of the pure-gas viscosities and conductivities
+static __device__ __forceinline__ void wilke_mix(const dv_step_params& p, const double ycl[DV_NG], const double mu[DV_NG],
+                                                 const double kk[DV_NG], const double sq[DV_NG], double& mu_m, double& k_m) {
+    mu_m = 0.0;
+    k_m = 0.0;
 #pragma unroll
     for (int i = 0; i < DV_NG; ++i) {
         double den = 0.0;
@@ -126,16 +131,34 @@ static __device__ void cell_props(const dv_step_params& p, const Cell& s, Props&
         mu_m = mu_m + ycl[i] * mu[i] / den;
         k_m = k_m + ycl[i] * kk[i] / den;
     }
+}
+
+// Blanc CO2 diffusivity over air and water (ideal_gas_backend.py:127-137) from the two Fuller values
+static __device__ __forceinline__ double blanc_Dm(const double ycl[DV_NG], double D_ca, double D_cw) {
+    double yi = ycl[2], yw = ycl[1];
+    return (yi + yw + 1e-9) / (yi / D_ca + yw / D_cw + 1e-9 / D_ca);
+}
+
+static __device__ void cell_props(const dv_step_params& p, const Cell& s, Props& o) {
+    double ycl[DV_NG];
+    props_state(p, s, o, ycl);
+    const double T = o.Tp;
+    double mu[DV_NG], kk[DV_NG], sq[DV_NG];
+    const double T3 = T / 300.0;
+#pragma unroll
+    for (int s2 = 0; s2 < DV_NG; ++s2) {
+        mu[s2] = gas_mu(p, s2, T);
+        kk[s2] = gas_k(p, s2, T3);
+        sq[s2] = sqrt(mu[s2]);
+    }
+    double mu_m, k_m;
+    wilke_mix(p, ycl, mu, kk, sq, mu_m, k_m);
     o.mu = mu_m;
     o.kg = k_m;
     o.rho = o.Cpos * wsum3(p.M, ycl);
     o.cpm = wsum3(p.cpg, ycl);
-    // Blanc CO2 diffusivity over air and water (ideal_gas_backend.py:127-137)
     double Pc = npmax(o.P, 1.0);
-    double D_ca = fuller(p, 0, T, Pc);
-    double D_cw = fuller(p, 1, T, Pc);
-    double yi = ycl[2], yw = ycl[1];
-    o.Dm = (yi + yw + 1e-9) / (yi / D_ca + yw / D_cw + 1e-9 / D_ca);
+    o.Dm = blanc_Dm(ycl, fuller(p, 0, T, Pc), fuller(p, 1, T, Pc));
     o.lam0 = stagnant(p, o.kg);
 }
 
@@ -171,47 +194,63 @@ static __device__ __forceinline__ double q_h2o(const dv_step_params& p, double p
     return p.h2o_q_m * c * kx / ((1.0 - kx) * (1.0 + (c - 1.0) * kx));
 }
 
-static __device__ double q_co2(const dv_step_params& p, double pc, double T, double qw) {   // isotherms.py:108-143
-    double pp = npmax(pc, 0.0);
-    double raw;
-    if (p.coads == DV_COADS_NONE) {
-        raw = toth(pp, T, p.co2_q_inf0, p.co2_chi, p.co2_b0, p.co2_dH0, p.co2_tau0, p.co2_alpha, p.co2_T0);
-    } else {
-        qw = npmax(qw, 1e-12);
-        if (p.coads == DV_COADS_WADST) {
-            double w = exp(-p.wadst_A / qw);
-            double q_wet = toth(pp, T, p.wadst_q_inf0, p.wadst_chi, p.wadst_b0, p.wadst_dH, p.wadst_tau0,
-                                p.wadst_alpha, p.co2_T0);
-            double q_dry = toth(pp, T, p.co2_q_inf0, p.co2_chi, p.co2_b0, p.co2_dH0, p.co2_tau0, p.co2_alpha, p.co2_T0);
-            raw = (1.0 - w) * q_dry + w * q_wet;
-        } else if (p.coads == DV_COADS_MECHANISTIC) {
-            double w = exp(-p.mech_A / qw);
-            double f_bl = p.mech_f_blocked_max * (1.0 - exp(-pow(p.mech_k * qw, p.mech_n)));
-            double phi_av = 1.0 - f_bl;
-            double phi = p.mech_phi_dry + (phi_av - p.mech_phi_dry) * w;
-            double dH_ave = (1.0 - w) * p.co2_dH0 + w * p.mech_dH_wet;
-            raw = (phi / p.mech_phi_dry) * toth(pp, T, p.co2_q_inf0, p.co2_chi, p.co2_b0, dH_ave, p.co2_tau0,
-                                                 p.co2_alpha, p.co2_T0);
-        } else {
-            double qi = p.co2_q_inf0 / (1.0 - p.sb_gamma * qw);
-            double b0 = p.co2_b0 * (1.0 + p.sb_beta * qw);
-            raw = toth(pp, T, qi, p.co2_chi, b0, p.co2_dH0, p.co2_tau0, p.co2_alpha, p.co2_T0);
-        }
-    }
-    return raw * (pp / (pp + p.p_reg));
+// The Toth terms of the CO2 isotherm that do not depend on the water loading: the dry one (models
+// none and wadst) and the wet one (wadst); pp = max(p_CO2, 0).
+static __device__ __forceinline__ double co2_toth_dry(const dv_step_params& p, double pp, double T) {
+    return toth(pp, T, p.co2_q_inf0, p.co2_chi, p.co2_b0, p.co2_dH0, p.co2_tau0, p.co2_alpha, p.co2_T0);
+}
+static __device__ __forceinline__ double co2_toth_wet(const dv_step_params& p, double pp, double T) {
+    return toth(pp, T, p.wadst_q_inf0, p.wadst_chi, p.wadst_b0, p.wadst_dH, p.wadst_tau0, p.wadst_alpha, p.co2_T0);
+}
+// WADST blend of the two Toth terms by the water loading qw (already floored at 1e-12)
+static __device__ __forceinline__ double wadst_blend(const dv_step_params& p, double qw, double q_dry, double q_wet) {
+    double w = exp(-p.wadst_A / qw);
+    return (1.0 - w) * q_dry + w * q_wet;
+}
+// the co-adsorption models whose Toth terms need the water loading first
+static __device__ __forceinline__ bool co2_needs_qw(const dv_step_params& p) {
+    return p.coads != DV_COADS_NONE && p.coads != DV_COADS_WADST;
 }
 
-// LDF rates (na) and equilibrium loadings of one cell (core/residual.py:232-238)
-static __device__ void uptake(const dv_step_params& p, const Cell& s, const Props& o, double rate[DV_NA], double qstar[DV_NA]) {
-    const double Tp = o.Tp;
-    double pk0 = s.c[0] * DV_R * Tp;
-    double pk1 = s.c[1] * DV_R * Tp;
+// CO2 loading before the low-pressure regularisation (isotherms.py:108-143); pp = max(p_CO2, 0).
+// q_dry / q_wet: the Toth terms when already evaluated (models none and wadst), else NaN.
+static __device__ double q_co2_raw(const dv_step_params& p, double pp, double T, double qw, double q_dry, double q_wet) {
+    if (p.coads == DV_COADS_NONE) return (q_dry == q_dry) ? q_dry : co2_toth_dry(p, pp, T);
+    qw = npmax(qw, 1e-12);
+    if (p.coads == DV_COADS_WADST) {
+        if (q_wet != q_wet) q_wet = co2_toth_wet(p, pp, T);
+        if (q_dry != q_dry) q_dry = co2_toth_dry(p, pp, T);
+        return wadst_blend(p, qw, q_dry, q_wet);
+    }
+    if (p.coads == DV_COADS_MECHANISTIC) {
+        double w = exp(-p.mech_A / qw);
+        double f_bl = p.mech_f_blocked_max * (1.0 - exp(-pow(p.mech_k * qw, p.mech_n)));
+        double phi_av = 1.0 - f_bl;
+        double phi = p.mech_phi_dry + (phi_av - p.mech_phi_dry) * w;
+        double dH_ave = (1.0 - w) * p.co2_dH0 + w * p.mech_dH_wet;
+        return (phi / p.mech_phi_dry) * toth(pp, T, p.co2_q_inf0, p.co2_chi, p.co2_b0, dH_ave, p.co2_tau0,
+                                             p.co2_alpha, p.co2_T0);
+    }
+    double qi = p.co2_q_inf0 / (1.0 - p.sb_gamma * qw);
+    double b0 = p.co2_b0 * (1.0 + p.sb_beta * qw);
+    return toth(pp, T, qi, p.co2_chi, b0, p.co2_dH0, p.co2_tau0, p.co2_alpha, p.co2_T0);
+}
+
+static __device__ __forceinline__ double q_co2(const dv_step_params& p, double pc, double T, double qw) {
+    double pp = npmax(pc, 0.0);
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    return q_co2_raw(p, pp, T, qw, nan, nan) * (pp / (pp + p.p_reg));
+}
+
+// saturation pressure of water (Arden Buck) at the clipped temperature
+static __device__ __forceinline__ double psat_h2o(double Tp) {
     double Tc = Tp - 273.15;
-    double psat = 611.21 * exp((18.678 - Tc / 234.5) * (Tc / (257.14 + Tc)));
-    double qw_eq = q_h2o(p, pk1, Tp, psat);
-    double basis = p.basis_state ? s.q[1] : qw_eq;
-    qstar[0] = q_co2(p, pk0, Tp, basis);
-    qstar[1] = qw_eq;
+    return 611.21 * exp((18.678 - Tc / 234.5) * (Tc / (257.14 + Tc)));
+}
+
+// LDF rates from the equilibrium loadings (core/residual.py:232-238)
+static __device__ __forceinline__ void ldf_rates(const dv_step_params& p, const Cell& s, double Tp,
+                                                 const double qstar[DV_NA], double rate[DV_NA]) {
 #pragma unroll
     for (int j = 0; j < DV_NA; ++j) {
         double k = p.k_ldf[j];
@@ -219,6 +258,19 @@ static __device__ void uptake(const dv_step_params& p, const Cell& s, const Prop
         else k = k * 1.0;
         rate[j] = k * (qstar[j] - s.q[j]);
     }
+}
+
+// LDF rates (na) and equilibrium loadings of one cell (core/residual.py:232-238)
+static __device__ void uptake(const dv_step_params& p, const Cell& s, const Props& o, double rate[DV_NA], double qstar[DV_NA]) {
+    const double Tp = o.Tp;
+    double pk0 = s.c[0] * DV_R * Tp;
+    double pk1 = s.c[1] * DV_R * Tp;
+    double psat = psat_h2o(Tp);
+    double qw_eq = q_h2o(p, pk1, Tp, psat);
+    double basis = p.basis_state ? s.q[1] : qw_eq;
+    qstar[0] = q_co2(p, pk0, Tp, basis);
+    qstar[1] = qw_eq;
+    ldf_rates(p, s, Tp, qstar, rate);
 }
 
 // ---------------------------------------------------------------- faces

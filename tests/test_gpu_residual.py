@@ -123,3 +123,32 @@ def test_outlet_records_match_reference():
         for k in ("cycle", "step", "t_step_s", "t_cycle_s", "t_total_s"):
             row.pop(k)
         _same_row(row, meta["row"], rtol=1e-10, atol=1e-18)
+
+
+def test_split_residual_is_bit_identical_to_the_thread_per_cell_evaluation():
+    """The split residual (per-cell properties with their independent transcendental terms spread
+    over the warps of a block, every face once, per-cell assembly) and the thread-per-cell kernel
+    behind dv_rhs_acc_noalloc evaluate the same expressions on the same operands: f and the 36
+    accumulator rates agree bit for bit on every golden case (every closure and co-adsorption
+    model)."""
+    import ctypes as C
+    from dac_vtsa_b200 import _lib
+    from dac_vtsa_b200.model import TVSAModel
+    from dac_vtsa_b200.params import build_params
+    lib = _lib.load()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for meta, data in CASES:
+        m, _ = build(TVSAModel, meta["over"], meta["step"], data["P0"], meta["T_jacket_prev"])
+        f, acc = m.rhs(meta["t"], data["y"])
+        params, feed_h, nnom_h, cov_h, _ = build_params(m.cfg, m.grid, m.props, m.step, m.P_start,
+                                                        meta["T_jacket_prev"])
+        put = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(m.device)  # noqa: E731
+        feed, nnom, cov, y = put(feed_h), put(nnom_h), put(cov_h), put(data["y"])
+        f2 = torch.full_like(y, np.nan)
+        acc2 = torch.full((36,), np.nan, dtype=torch.float64, device=m.device)
+        rc = lib.dv_rhs_acc_noalloc(C.byref(params), feed.data_ptr(), nnom.data_ptr(), cov.data_ptr(), meta["t"],
+                                    y.data_ptr(), f2.data_ptr(), acc2.data_ptr(), stream)
+        assert rc == 0, lib.dv_last_error()
+        torch.cuda.synchronize()
+        assert np.array_equal(f, f2.cpu().numpy()), meta["name"]
+        assert np.array_equal(acc, acc2.cpu().numpy()), meta["name"]
