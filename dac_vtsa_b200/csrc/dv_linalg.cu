@@ -1105,19 +1105,26 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0)                                // the first NBUF stages are in flight from the start
+    const int rh = (nb + 1) >> 1;              // rows per half: a group of 8 lanes takes rows r0 and r0 + rh
+    // the thread that issues the ring's copies and the warp that polls their mbarriers: the last warp
+    // when it has no rows (nb <= 56), so neither the copy issue nor the poll is on the row warps' path
+    // to the next barrier; that warp then takes no part in the prologue either
+    const int issuer = (rh <= PA_THREADS / PA_LANES - 32 / PA_LANES) ? PA_THREADS - 32 : 0;
+    const int pollw = issuer / 32;
+    const int nthr = issuer ? issuer : PA_THREADS;   // threads that load b and clear xb
+    if (tid == issuer)                           // the first NBUF stages are in flight from the start
         for (int q = 0; q < NBUF && q < S; ++q) issue(q, smem_u32(buf0 + (int64_t)q * 3 * bs), smem_u32(&bars[q]));
     const int fcol = F.V ? *F.col : 0;
     const double fscale = F.V ? *F.scale : 0.0;
     const double* __restrict__ src = F.V ? ((fcol == 0) ? F.src0 : F.src1) : b;
     // b (or the basis vector to normalise) into xs: PA_IO entries per thread at a time, all their
     // loads issued before the first use
-    for (int q0 = tid; q0 < Nz * LD; q0 += PA_IO * PA_THREADS) {
+    for (int q0 = (tid < nthr) ? tid : Nz * LD; q0 < Nz * LD; q0 += PA_IO * nthr) {
         int64_t gi[PA_IO];
         double bv[PA_IO], sv[PA_IO];
 #pragma unroll
         for (int u = 0; u < PA_IO; ++u) {
-            const int q = q0 + u * PA_THREADS;
+            const int q = q0 + u * nthr;
             const int t = q / LD, l = q - t * LD;
             bool in = q < Nz * LD && l < nb && t < nio;
             gi[u] = in ? pc_glob(g, part, fr.gp(t), l) : -1;
@@ -1131,7 +1138,7 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
         }
 #pragma unroll
         for (int u = 0; u < PA_IO; ++u) {
-            const int q = q0 + u * PA_THREADS;
+            const int q = q0 + u * nthr;
             if (q >= Nz * LD) break;
             double v = 0.0;
             if (gi[u] >= 0) {
@@ -1145,16 +1152,10 @@ __global__ void __launch_bounds__(PA_THREADS) k_pc_apply(PcGeom gin, const TS* _
             xs[q] = v;
         }
     }
-    for (int q = tid; q < Nz * LD; q += blockDim.x) xb[q] = 0.0;
+    for (int q = tid; q < Nz * LD && tid < nthr; q += nthr) xb[q] = 0.0;
     __syncthreads();
     const int lane = tid % PA_LANES;
-    const int grp = tid / PA_LANES;            // 8 lanes per group, two rows per group: r0 and r0 + rh
-    const int rh = (nb + 1) >> 1;
-    // the thread that issues the ring's refills and the warp that polls the copies' mbarriers: the
-    // last warp when it has no rows (nb <= 56), so neither the copy issue nor the poll is on the row
-    // warps' path to the next barrier
-    const int issuer = (rh <= PA_THREADS / PA_LANES - 32 / PA_LANES) ? PA_THREADS - 32 : 0;
-    const int pollw = issuer / 32;
+    const int grp = tid / PA_LANES;
     const int r0 = grp, r1 = grp + rh;
     const bool act0 = r0 < rh, act1 = act0 && r1 < nb;
     int issued = (S < NBUF) ? S : NBUF;        // stages whose copies have been issued
