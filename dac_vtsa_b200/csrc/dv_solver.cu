@@ -980,6 +980,28 @@ __global__ void k_gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, 
 }
 
 // ---- fused classical Gram-Schmidt of the graph body (three kernels per Arnoldi step)
+// Warp sums of the first cnt entries of acc into out[q] (lane 0).  Each entry is the same butterfly
+// over the 32 lanes; they run eight at a time, side by side (one uniform branch per eight), so the
+// sums wait on about five shuffle latencies per eight entries instead of five per entry.
+__device__ __forceinline__ void warp_sums(const double (&acc)[GM_KMAX + 1], int cnt, int lane, double* out) {
+#pragma unroll
+    for (int q0 = 0; q0 <= GM_KMAX; q0 += 8) {
+        if (q0 < cnt) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = (q0 + u <= GM_KMAX) ? acc[q0 + u] : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] += __shfl_xor_sync(0xffffffffu, v[u], off);
+            if (lane == 0)
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (q0 + u < cnt) out[q0 + u] = v[u];
+        }
+    }
+}
+
 // Block sums of the first cnt entries of acc (VB threads) into part[blockIdx.x * GM_PS + q];
 // returns true in the block that finished last (after the other blocks' partials are visible).
 constexpr int GM_PS = GM_KMAX + 2;      // partial stride per block
@@ -989,15 +1011,7 @@ __device__ __forceinline__ bool gm_block_partials(const double (&acc)[GM_KMAX + 
     __shared__ double sm[VB / 32][GM_PS];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q <= GM_KMAX; ++q) {
-        if (q < cnt) {
-            double v = acc[q];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (lane == 0) sm[wid][q] = v;
-        }
-    }
+    warp_sums(acc, cnt, lane, sm[wid]);
     __syncthreads();
     if ((int)threadIdx.x < cnt) {
         double t = 0.0;
@@ -1095,15 +1109,7 @@ __global__ void __launch_bounds__(VB) k_cgs_orth_norm(int64_t n, GmDev* st, cons
 __device__ __forceinline__ void gm_store_partials(const double (&acc)[GM_KMAX + 1], int cnt, double* part) {
     __shared__ double sm[VB / 32][GM_PS];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int q = 0; q <= GM_KMAX; ++q) {
-        if (q < cnt) {
-            double v = acc[q];
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            if (lane == 0) sm[wid][q] = v;
-        }
-    }
+    warp_sums(acc, cnt, lane, sm[wid]);
     __syncthreads();
     if ((int)threadIdx.x < cnt) {
         double t = 0.0;
