@@ -933,43 +933,44 @@ __global__ void k_orth_update_gm(int64_t n, const GmDev* __restrict__ st, const 
     }
 }
 
-// Hessenberg column, Givens rotations, residual estimate and the stopping test of gmres()
-__device__ void gm_givens(GmDev* st, const double* hh, int kdim, cudaGraphConditionalHandle hnd) {
+// Hessenberg column, Givens rotations, residual estimate and the stopping test of gmres().  One
+// thread.  The rotated entry k + 1 of the new column is carried to the next rotation in a register
+// and the loads (hh, the stored rotations) go through restrict pointers, so they run ahead of the
+// chain of rotations instead of each waiting behind the previous entry's store.
+__device__ void gm_givens(GmDev* st, const double* __restrict__ hh, int kdim, cudaGraphConditionalHandle hnd) {
     const double eps = 2.220446049250313e-16;                 // double epsilon
     const int col = st->col;
     const int m = col + 1;
-    double* H = st->H;
-    auto h = [&](int c, int k) -> double& { return H[c * (kdim + 1) + k]; };
+    double* __restrict__ Hc = st->H + (int64_t)col * (kdim + 1);      // column col of H
+    const double* __restrict__ gcs = st->gc;
+    const double* __restrict__ gss = st->gs;
     const double h0 = sqrt(hh[m]);
-    for (int k = 0; k <= col; ++k) h(col, k) = hh[k] + hh[(kdim + 2) + k];
     const double h1 = hh[2 * (kdim + 2)];
-    h(col, col + 1) = h1;
+    const double S_col = st->S[col], ptol = st->ptol;         // loaded with the column, ahead of their use
+    const int iters = st->iters;
     bool breakdown = false;
-    if (h1 <= eps * h0 || !(h1 == h1)) {
-        h(col, col + 1) = 0.0;
-        breakdown = true;
-    } else {
-        st->scale = 1.0 / h1;
-    }
+    if (h1 <= eps * h0 || !(h1 == h1)) breakdown = true;      // the subdiagonal entry is taken as 0
+    else st->scale = 1.0 / h1;
+    double carry = hh[0] + hh[(kdim + 2)];                     // entry k of the column, rotated by 0..k-1
     for (int k = 0; k < col; ++k) {
-        double c = st->gc[k], s2 = st->gs[k];
-        double n0 = h(col, k), n1 = h(col, k + 1);
-        h(col, k) = c * n0 + s2 * n1;
-        h(col, k + 1) = -s2 * n0 + c * n1;
+        const double c = gcs[k], s2 = gss[k];
+        const double n0 = carry, n1 = hh[k + 1] + hh[(kdim + 2) + k + 1];
+        Hc[k] = c * n0 + s2 * n1;
+        carry = -s2 * n0 + c * n1;
     }
     double c, s2, mag;
-    lartg_d(h(col, col), h(col, col + 1), c, s2, mag);
+    lartg_d(carry, breakdown ? 0.0 : h1, c, s2, mag);
     st->gc[col] = c;
     st->gs[col] = s2;
-    h(col, col) = mag;
-    h(col, col + 1) = 0.0;
-    double tmp = -s2 * st->S[col];
-    st->S[col] = c * st->S[col];
+    Hc[col] = mag;
+    Hc[col + 1] = 0.0;
+    double tmp = -s2 * S_col;
+    st->S[col] = c * S_col;
     st->S[col + 1] = tmp;
     const double presid = fabs(tmp);
     st->presid = presid;
-    st->iters += 1;
-    const bool stop = !(presid == presid) || presid <= st->ptol || breakdown || col + 1 == kdim;
+    st->iters = iters + 1;
+    const bool stop = !(presid == presid) || presid <= ptol || breakdown || col + 1 == kdim;
     if (!stop) st->col = col + 1;
     st->done = stop;
     cudaGraphSetConditional(hnd, stop ? 0u : 1u);
