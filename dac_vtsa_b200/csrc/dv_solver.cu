@@ -1119,6 +1119,26 @@ __device__ __forceinline__ void gm_store_partials(const double (&acc)[GM_KMAX + 
     }
 }
 
+// The grid's per-block partials of entries q < cnt, copied into this block's shared memory by all
+// its threads at once (one round of L2 loads), for a finish that then adds them in block order from
+// shared memory: the same additions in the same order as sum_partials, without one L2 round trip
+// per block.  Grids of more than CG_MAXB blocks finish with sum_partials.
+constexpr int CG_MAXB = 160;
+__device__ __forceinline__ void stage_partials(const double* part, int cnt, double (*ps)[GM_PS]) {
+    const int nb = (int)gridDim.x;
+    for (int i = threadIdx.x; i < nb * cnt; i += blockDim.x) {
+        const int b = i / cnt, q = i - b * cnt;
+        ps[b][q] = __ldcg(part + (int64_t)b * GM_PS + q);
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ double finish_partials(const double* part, int q, double (*ps)[GM_PS]) {
+    if (gridDim.x > CG_MAXB) return sum_partials(part + q, (int)gridDim.x, GM_PS);
+    double t = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) t += ps[b][q];
+    return t;
+}
+
 // k_cgs_dots + k_cgs_orth_dots + k_cgs_orth_norm in one launch, with the same block partition and
 // the same summation order (so the same results): the two global sums between the passes are
 // grid barriers instead of kernel boundaries, and every block sums the partials itself in block
@@ -1133,7 +1153,9 @@ __global__ void __launch_bounds__(VB) k_cgs_fused(int64_t n, GmDev* st, const do
     if (st->done) return;                  // a step after the solve stopped (uniform over the grid)
     const int m = st->col + 1;
     __shared__ double hs[GM_KMAX + 1];
+    __shared__ double ps[CG_MAXB][GM_PS];
     __shared__ bool last;
+    const bool staged = gridDim.x <= CG_MAXB;     // grid-uniform
     const int64_t pstride = (int64_t)gridDim.x * GM_PS;
     double* part1 = part;
     double* part2 = part + pstride;
@@ -1152,8 +1174,9 @@ __global__ void __launch_bounds__(VB) k_cgs_fused(int64_t n, GmDev* st, const do
     }
     gm_store_partials(acc, m + 1, part1);
     grid_sync_bounded(bar, bar + 1, err);
+    if (staged) stage_partials(part1, m + 1, ps);
     if ((int)threadIdx.x <= m) {
-        const double t = sum_partials(part1 + threadIdx.x, (int)gridDim.x, GM_PS);
+        const double t = finish_partials(part1, threadIdx.x, ps);
         hs[threadIdx.x] = t;
         if (blockIdx.x == 0) hh[threadIdx.x] = t;
     }
@@ -1172,8 +1195,9 @@ __global__ void __launch_bounds__(VB) k_cgs_fused(int64_t n, GmDev* st, const do
     }
     gm_store_partials(acc, m, part2);
     grid_sync_bounded(bar, bar + 1, err);
+    if (staged) stage_partials(part2, m, ps);
     if ((int)threadIdx.x < m) {
-        const double t = sum_partials(part2 + threadIdx.x, (int)gridDim.x, GM_PS);
+        const double t = finish_partials(part2, threadIdx.x, ps);
         hs[threadIdx.x] = t;
         if (blockIdx.x == 0) hh[(kdim + 2) + threadIdx.x] = t;
     }
@@ -1192,11 +1216,14 @@ __global__ void __launch_bounds__(VB) k_cgs_fused(int64_t n, GmDev* st, const do
     __syncthreads();
     if (threadIdx.x == 0) last = (atomicAdd(bar + 2, 1u) == gridDim.x - 1);
     __syncthreads();
-    if (last && threadIdx.x == 0) {
+    if (last) {                                 // block-uniform
         __threadfence();
-        hh[2 * (kdim + 2)] = sqrt(sum_partials(part3, (int)gridDim.x, GM_PS));
-        bar[2] = 0u;
-        gm_givens(st, hh, kdim, hnd);
+        if (staged) stage_partials(part3, 1, ps);
+        if (threadIdx.x == 0) {
+            hh[2 * (kdim + 2)] = sqrt(finish_partials(part3, 0, ps));
+            bar[2] = 0u;
+            gm_givens(st, hh, kdim, hnd);
+        }
     }
 }
 
