@@ -337,7 +337,9 @@ static __device__ __forceinline__ double matvec_sig(const double* scal) {
 // Two warps per 32 cells: warp 0 evaluates the transport properties of its cells, warp 1 the
 // temperature, isotherms and LDF rates of the same cells (the two halves of the per-cell chain run
 // side by side; uptake reads only the clipped temperature of the properties).
-// The work of one 64-thread block `vb` (cells vb*32 .. vb*32 + 31).
+// The work of one 64-thread block `vb` (cells vb*32 .. vb*32 + 31).  Used by the cooperative FD
+// matvec (k_matvec_coop, whose phases share 64-thread blocks); k_cprops runs the eight-warp form
+// below, which gives the same bits.
 template <int MODE>
 __device__ __forceinline__ void cprops_block(const dv_step_params& p, const Split& S, const double* __restrict__ y,
                                              const double* __restrict__ u, const double* __restrict__ sc,
